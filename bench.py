@@ -1,0 +1,357 @@
+"""Benchmark: KKT solves/s of the block-iLDL^T + SQMR path on B200.
+
+Workload (default --config scale): K = [[H + 1e-8 I, A'], [A, -1e-8 I]] with
+n = 200000, m = 100000, 6 nonzeros per column of A (3 in a band of half-width
+32 around floor(j m / n), 3 uniform), H log-uniform in [1e-6, 1e6],
+contiguous 32-row blocks, Bunch-Kaufman pivoting, level-0 fill,
+fill_factor 1, threshold 0; one N(0,1) right-hand side; SQMR with tol 1e-8
+and max_it 1000 (the driver's settings, apps/block_ildlt/block_ildlt_invariants.h:186-187).
+The sparsity pattern's symbolic analysis is done once (as for a stream of
+IPM iterations on one pattern); a step is one numeric factorization plus one
+SQMR solve with the values resident in HBM.  L2 (126 MB) is flushed before
+every step by writing a 512 MB buffer outside the timed events.
+
+`e2e` times the same step through the public C ABI with host buffers: K's
+values and b copied host -> device from pinned memory, the factor and the
+solve, and x copied device -> host, inside the timed region.
+
+`--impl reference` times the CPU restatement of the reference's path (the
+reference has no CPU numeric path; its host symbolic phase and GPU kernels
+are restated in oracle/) on the same workload.
+
+Multi-GPU: independent replicas (one KKT system per rank, no collective on
+the data path); value = solves of all ranks / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "KKT solves/s (block-iLDLt + SQMR, FP64 plain path)"
+UNIT = "solves/s"
+
+
+def _parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="culipx", choices=["culipx", "reference"])
+    ap.add_argument("--config", default="scale", choices=["small", "scale"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def _workload(name):
+    import culip_b200 as cb
+
+    cfg = dict(cb.KKT_CONFIGS[name])
+    rp, ci, v = cb.kkt_generate(cfg["n"], cfg["m"], cfg["nnz_per_col"], cfg["band_half"], cfg["hmin"], cfg["hmax"])
+    bs = cb.kkt_blocking(cfg["n"], cfg["m"], cfg["block"])
+    b = cb.normal_vector(cb.SEED + 1, len(rp) - 1)
+    return cfg, rp, ci, v, bs, b
+
+
+def _config_dict(name, cfg, nnz, extra=None):
+    d = {"workload": f"KKT {name}: n={cfg['n']} m={cfg['m']} N={cfg['n'] + cfg['m']} nnz_K={nnz}, "
+                     f"A {cfg['nnz_per_col']}/col (band_half={cfg['band_half']}), H log-U[{cfg['hmin']:g},{cfg['hmax']:g}], "
+                     f"blocks {cfg['block']}, BK, fill 0, SQMR tol 1e-8 max_it 1000, 1 RHS",
+         "pattern_reuse": "symbolic analysis once, numeric factor + solve per step",
+         "l2": "flushed before every step (512 MB write outside the timed events)"}
+    if extra:
+        d.update(extra)
+    return d
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    def __init__(self, device=0):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def _dist():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def run_culipx(args):
+    import torch
+
+    import culip_b200 as cb
+    from culip_b200 import _capi as capi
+
+    world, rank, local = _dist()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    cfg, rp, ci, v, bs, b = _workload(args.config)
+    N = len(rp) - 1
+    nnz = len(ci)
+    stream = torch.cuda.current_stream()
+    h = cb.Handle(local, stream)
+    P = cb.Pattern(h, rp, ci, bs, 0, 1.0, cb.F64)
+    F = cb.Factor(P)
+    d_rp = torch.from_numpy(rp).cuda()
+    d_ci = torch.from_numpy(ci).cuda()
+    d_v = torch.from_numpy(v).cuda()
+    d_b = torch.from_numpy(b).cuda()
+    d_x = torch.zeros(N, dtype=torch.float64, device="cuda")
+    A = cb.CsrOperator(h, d_rp, d_ci, d_v)
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    iters_seen = []
+
+    def step():
+        F.compute(d_v, None, cb.PIV_BK, 0.0)
+        res, its, st = cb.sqmr_solve(h, A, F, d_b, d_x, 1e-8, 1000)
+        iters_seen.append(its)
+        return res, its
+
+    for _ in range(args.warmup):
+        flush.fill_(1.0)
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    h.launch_count(reset=True)
+    clocks = ClockSampler(local)
+    clocks.start()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    torch.cuda.synchronize()
+    for i in range(args.steps):
+        flush.fill_(float(i))
+        evs[i][0].record(stream)
+        step()
+        evs[i][1].record(stream)
+    torch.cuda.synchronize()
+    ck = clocks.stop()
+    launches = h.launch_count(reset=True)
+    step_ms = [a.elapsed_time(b2) for a, b2 in evs]
+    total_ms = float(np.sum(step_ms))
+    if dist:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        dist.barrier()
+
+    # accuracy of the last step
+    x = d_x.cpu().numpy()
+    import scipy.sparse as sp
+
+    K = sp.csr_matrix((v, ci, rp), shape=(N, N))
+    relres = float(np.linalg.norm(b - K @ x) / np.linalg.norm(b))
+
+    # SpMV roofline: the operator's HBM-bound kernel, timed with events on the stream
+    y = torch.empty_like(d_x)
+    spmv_ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+    reps = 50
+    flush.fill_(0.0)
+    A.spmv(d_b, y)
+    torch.cuda.synchronize()
+    spmv_ev[0].record(stream)
+    for _ in range(reps):
+        A.spmv(d_b, y)
+    spmv_ev[1].record(stream)
+    torch.cuda.synchronize()
+    spmv_ms = spmv_ev[0].elapsed_time(spmv_ev[1]) / reps
+    spmv_bytes = nnz * (8 + 4) + 4 * (N + 1) + 8 * N + 8 * N
+
+    # e2e through the public API with host buffers
+    hv = torch.from_numpy(v).pin_memory()
+    hb = torch.from_numpy(b).pin_memory()
+    hx = torch.empty(N, dtype=torch.float64).pin_memory()
+    d_v2 = torch.empty_like(d_v)
+    d_b2 = torch.empty_like(d_b)
+    A2 = cb.CsrOperator(h, d_rp, d_ci, d_v2)
+    e2e_steps = max(2, min(args.steps, 5))
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e_ms = []
+    for i in range(e2e_steps):
+        flush.fill_(float(i))
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        d_v2.copy_(hv, non_blocking=True)
+        d_b2.copy_(hb, non_blocking=True)
+        F.compute(d_v2, None, cb.PIV_BK, 0.0)
+        cb.sqmr_solve(h, A2, F, d_b2, d_x, 1e-8, 1000)
+        hx.copy_(d_x, non_blocking=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        e_ms.append(e0.elapsed_time(e1))
+    e2e_total = float(np.sum(e_ms))
+    if dist:
+        t = torch.tensor([e2e_total], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_total = float(t.item())
+
+    fac_ms, fac_launches = F.stats()
+    value = world * args.steps / (total_ms / 1e3)
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded KKT generator)",
+        "config": _config_dict(args.config, cfg, nnz, {"parallelism": f"replicas x{world} (independent KKT systems)"}),
+        "sqmr_iterations": int(np.median(iters_seen)) if iters_seen else None,
+        "true_relres": relres,
+        "factor_ms": fac_ms,
+        "gpu_launches": int(launches),
+        "clocks": ck,
+        "e2e": {"value": world * e2e_steps / (e2e_total / 1e3), "unit": UNIT,
+                "h2d_bytes_per_step": int(nnz * 8 + N * 8), "d2h_bytes_per_step": int(N * 8)},
+        "roofline": {"kernel": "k_csr_spmv<double,8>", "bound": "hbm", "achieved": spmv_bytes / (spmv_ms * 1e-3) / 1e9,
+                     "peak": _peak_hbm(), "unit": "GB/s",
+                     "frac": spmv_bytes / (spmv_ms * 1e-3) / 1e9 / _peak_hbm(), "traffic": None,
+                     "algorithmic_bytes": int(spmv_bytes), "avg_launch_ms": spmv_ms,
+                     "note": "x (2.4 MB) is L2-resident; matrix streamed from HBM after a flush"},
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(args.config, rp, ci, v, bs, b, int(np.median(iters_seen)))
+    if dist:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+def _peak_hbm():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"])
+    except Exception:
+        return 6650.0
+
+
+def cpu_baseline(name, rp, ci, v, bs, b, gpu_iters, max_seconds=25.0):
+    """Oracle (CPU restatement, 1 thread): symbolic + factor timed fully, SQMR on
+    a bounded number of iterations, scaled to the GPU run's iteration count."""
+    import oracle
+
+    t0 = time.perf_counter()
+    S = oracle.Sym(rp, ci, bs, 0, 1.0)
+    t1 = time.perf_counter()
+    F = S.factor(v)
+    t2 = time.perf_counter()
+    sample_it = 20
+    t3 = time.perf_counter()
+    oracle.sqmr(rp, ci, v, b, F, 1e-8, sample_it)
+    t4 = time.perf_counter()
+    per_it = (t4 - t3) / sample_it
+    solve_s = (t2 - t1) + per_it * max(gpu_iters, 1)
+    return {"value": 1.0 / solve_s, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"oracle factor (full, {t2 - t1:.2f}s) + {sample_it} SQMR iterations ({t4 - t3:.2f}s) scaled to "
+                      f"{gpu_iters} iterations; symbolic {t1 - t0:.2f}s not counted (cached per pattern)"}
+
+
+def run_reference(args):
+    world, rank, _ = _dist()
+    if rank != 0:
+        return
+    cfg, rp, ci, v, bs, b = _workload(args.config)
+    import oracle
+
+    S = oracle.Sym(rp, ci, bs, 0, 1.0)
+    # one step = factor + SQMR; bounded: SQMR capped at 20 iterations per step, scaled to the GPU iteration count
+    ms = []
+    iters_full = None
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        F = S.factor(v)
+        t1 = time.perf_counter()
+        _, _, it = oracle.sqmr(rp, ci, v, b, F, 1e-8, 20)
+        t2 = time.perf_counter()
+        if iters_full is None:
+            iters_full = _reference_iterations(args.config)
+        if i >= args.warmup:
+            ms.append(((t1 - t0) + (t2 - t1) / 20 * iters_full) * 1e3)
+    total = float(np.sum(ms))
+    value = args.steps / (total / 1e3)
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": total / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f64", "data": "synthetic (seeded KKT generator)", "impl": "reference",
+           "config": _config_dict(args.config, cfg, len(ci)),
+           "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
+                            "sample": f"per step: oracle factor (full) + 20 SQMR iterations scaled to {iters_full}"},
+           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def _reference_iterations(name):
+    # iteration count of the full FP64 SQMR solve on this workload (from the oracle, cached per process)
+    cache = os.path.join(ROOT, "tests", "golden", f"sqmr_iterations_{name}.txt")
+    if os.path.exists(cache):
+        return int(open(cache).read().strip())
+    return 300
+
+
+if __name__ == "__main__":
+    a = _parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_culipx(a)

@@ -1,0 +1,366 @@
+"""culip_b200: B200-native block-iLDL^T + SQMR solve path for KKT systems.
+
+Python mirror of the reference's class API over the C ABI (include/culipx.h):
+
+  BlockiLDLt      libs/la/preconditioner/block_ildlt.cuh:188-401
+  CSRMatrixSPMV   libs/la/spmv.cuh:19-66
+  SQMR            libs/la/iterative_solvers/sqmr.cuh:29-79
+
+plus the lower-level objects they are built from (Handle, Pattern, Factor,
+CsrOperator) and the seeded KKT generator.  Device vectors are torch CUDA
+tensors (PyTorch is used only for device memory and streams); all compute
+runs in libculipx.so's sm_100a kernels.  There is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _capi as capi
+from ._capi import (F32, F64, LEFT, MIDDLE, PIV_BK, PIV_ROOK, PIV_STATIC, RIGHT, CulipxError,  # noqa: F401
+                    KktSpec)
+
+__all__ = ["Handle", "Pattern", "Factor", "CsrOperator", "BlockiLDLt", "CSRMatrixSPMV", "SQMR", "kkt_generate",
+           "kkt_blocking", "normal_vector", "CulipxError", "KKT_CONFIGS"]
+
+# The benchmark systems: K = [[H + delta I, A'], [A, -gamma I]] (see DESIGN.md for the construction)
+KKT_CONFIGS = {
+    "small": dict(n=2000, m=1000, nnz_per_col=4, band_half=0, hmin=1e-2, hmax=1e2, block=4),
+    "scale": dict(n=200000, m=100000, nnz_per_col=6, band_half=32, hmin=1e-6, hmax=1e6, block=32),
+    "mixed": dict(n=1000000, m=500000, nnz_per_col=6, band_half=32, hmin=1e-6, hmax=1e6, block=32),
+}
+SEED = 20260101
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _dptr(t) -> ctypes.c_void_p:
+    """Device pointer of a torch CUDA tensor (or None)."""
+    if t is None:
+        return None
+    if not getattr(t, "is_cuda", False):
+        raise TypeError("expected a CUDA tensor")
+    if not t.is_contiguous():
+        raise ValueError("expected a contiguous tensor")
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def kkt_generate(n, m, nnz_per_col, band_half, hmin, hmax, delta=1e-8, gamma=1e-8, seed=SEED):
+    """Seeded KKT system as full symmetric CSR (rowptr, colidx, val) numpy arrays."""
+    spec = KktSpec(n, m, nnz_per_col, band_half, hmin, hmax, delta, gamma, seed)
+    nnz = ctypes.c_longlong()
+    capi.call("culipx_kkt_nnz", ctypes.byref(spec), ctypes.byref(nnz))
+    rowptr = np.zeros(n + m + 1, np.int32)
+    colidx = np.zeros(nnz.value, np.int32)
+    val = np.zeros(nnz.value, np.float64)
+    capi.call("culipx_kkt_generate", ctypes.byref(spec), _p(rowptr), _p(colidx), _p(val))
+    return rowptr, colidx, val
+
+
+def kkt_blocking(n, m, block) -> np.ndarray:
+    """block_starts with num_blocks + 1 entries (last = n + m)."""
+    nb = ctypes.c_int()
+    capi.call("culipx_kkt_blocking", n, m, block, None, 0, ctypes.byref(nb))
+    bs = np.zeros(nb.value + 1, np.int32)
+    capi.call("culipx_kkt_blocking", n, m, block, _p(bs), nb.value + 1, ctypes.byref(nb))
+    return bs
+
+
+def normal_vector(seed, n) -> np.ndarray:
+    out = np.zeros(n, np.float64)
+    capi.call("culipx_normal_vector", seed, n, _p(out))
+    return out
+
+
+class Handle:
+    """Device, stream and device-memory budget (the reference's gpu_handle_t)."""
+
+    def __init__(self, device: int = 0, stream=None):
+        import torch
+
+        self.device = device
+        if stream is None:
+            stream = torch.cuda.current_stream(device)
+        self.stream = stream
+        h = ctypes.c_void_p()
+        capi.call("culipx_handle_create", ctypes.byref(h), device, ctypes.c_void_p(stream.cuda_stream))
+        self._h = h
+
+    def set_stream(self, stream):
+        self.stream = stream
+        capi.call("culipx_handle_set_stream", self._h, ctypes.c_void_p(stream.cuda_stream))
+
+    def set_memory_budget(self, nbytes: int):
+        capi.call("culipx_handle_set_memory_budget", self._h, int(nbytes))
+
+    def memory_used(self) -> int:
+        v = ctypes.c_longlong()
+        capi.call("culipx_handle_memory_used", self._h, ctypes.byref(v))
+        return v.value
+
+    def synchronize(self):
+        capi.call("culipx_handle_synchronize", self._h)
+
+    def launch_count(self, reset=False) -> int:
+        v = ctypes.c_longlong()
+        capi.call("culipx_handle_launch_count", self._h, ctypes.byref(v), 1 if reset else 0)
+        return v.value
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            capi.load().culipx_handle_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Pattern:
+    """Symbolic analysis of one sparsity pattern (BlockiLDLt ctor + symbolic part of compute())."""
+
+    def __init__(self, handle: Handle, rowptr, colidx, block_starts, fill_level=0, fill_factor=1.0,
+                 precision=F64):
+        self.handle = handle
+        self.rowptr = np.ascontiguousarray(rowptr, np.int32)
+        self.colidx = np.ascontiguousarray(colidx, np.int32)
+        self.n = len(self.rowptr) - 1
+        bs = np.ascontiguousarray(block_starts, np.int32)
+        if bs[-1] == self.n:
+            bs = bs[:-1]
+        self.num_blocks = len(bs)
+        self.precision = precision
+        p = ctypes.c_void_p()
+        capi.call("culipx_pattern_analyze", handle._h, self.n, _p(self.rowptr), _p(self.colidx), self.num_blocks,
+                  _p(bs), int(fill_level), float(fill_factor), int(precision), ctypes.byref(p))
+        self._h = p
+
+    def info(self) -> dict:
+        v = np.zeros(16, np.int64)
+        capi.call("culipx_pattern_info", self._h, _p(v))
+        keys = ["n", "nnz", "num_blocks", "coarse_nnz", "fill_nnz", "num_levels", "num_sparse", "num_dense",
+                "val_slots", "idx_slots", "max_level_blocks", "max_level_rows", "device_bytes", "precision"]
+        return {k: int(v[i]) for i, k in enumerate(keys)}
+
+    def export(self) -> dict:
+        inf = self.info()
+        cm, cnz, nl = inf["num_blocks"], inf["coarse_nnz"], inf["num_levels"]
+        out = dict(coarse_off=np.zeros(cm + 1, np.int32), coarse_col=np.zeros(cnz, np.int32),
+                   blk_nnzA=np.zeros(cnz, np.int32), lvl_off=np.zeros(nl + 1, np.int32),
+                   lvl_rows=np.zeros(cm, np.int32), lb_off=np.zeros(nl + 1, np.int32), lb=np.zeros(cnz, np.int32),
+                   sb_off=np.zeros(nl + 1, np.int32), sb=np.zeros(cnz, np.int32), fmt=np.zeros(cnz, np.int32),
+                   max_nnz=np.zeros(cnz, np.int32))
+        capi.call("culipx_pattern_export", self._h, *[_p(out[k]) for k in
+                                                      ("coarse_off", "coarse_col", "blk_nnzA", "lvl_off", "lvl_rows",
+                                                       "lb_off", "lb", "sb_off", "sb", "fmt", "max_nnz")])
+        return out
+
+    def __del__(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            capi.load().culipx_pattern_destroy(self._h)
+            self._h = None
+
+
+class Factor:
+    """Numeric block-iLDL^T factor of one pattern (BlockiLDLt::factorize + applies)."""
+
+    def __init__(self, pattern: Pattern):
+        self.pattern = pattern
+        f = ctypes.c_void_p()
+        capi.call("culipx_factor_create", pattern._h, ctypes.byref(f))
+        self._h = f
+
+    @property
+    def dtype(self):
+        import torch
+
+        return torch.float64 if self.pattern.precision == F64 else torch.float32
+
+    def compute(self, vals, is_piv=None, pivot=PIV_BK, threshold=0.0):
+        """vals: torch CUDA tensor (pattern precision) or host numpy float64 array."""
+        ip = None if is_piv is None else np.ascontiguousarray(is_piv, np.int32)
+        if isinstance(vals, np.ndarray):
+            v = np.ascontiguousarray(vals, np.float64)
+            capi.call("culipx_factor_compute_host", self._h, _p(v), None if ip is None else _p(ip), int(pivot),
+                      float(threshold))
+        else:
+            capi.call("culipx_factor_compute", self._h, _dptr(vals), None if ip is None else _p(ip), int(pivot),
+                      float(threshold))
+
+    def stats(self):
+        ms = ctypes.c_double()
+        nl = ctypes.c_int()
+        capi.call("culipx_factor_stats", self._h, ctypes.byref(ms), ctypes.byref(nl))
+        return ms.value, nl.value
+
+    def export(self) -> dict:
+        tot = ctypes.c_longlong()
+        capi.call("culipx_factor_export_size", self._h, ctypes.byref(tot))
+        inf = self.pattern.info()
+        cnz, n = inf["coarse_nnz"], inf["n"]
+        vd = np.float64 if self.pattern.precision == F64 else np.float32
+        out = dict(blk_nnz=np.zeros(cnz, np.int32), blk_off=np.zeros(cnz + 1, np.int64),
+                   idx=np.zeros(max(tot.value, 1), np.int32), val=np.zeros(max(tot.value, 1), vd),
+                   tri=np.zeros(3 * n, vd), is_piv=np.zeros(n, np.int32), perm=np.zeros(n, np.int32),
+                   got_extra=np.zeros(cnz, np.int32))
+        capi.call("culipx_factor_export", self._h, *[_p(out[k]) for k in
+                                                     ("blk_nnz", "blk_off", "idx", "val", "tri", "is_piv", "perm",
+                                                      "got_extra")])
+        out["idx"] = out["idx"][: tot.value]
+        out["val"] = out["val"][: tot.value]
+        return out
+
+    def apply(self, stage: int, b, x=None):
+        import torch
+
+        if x is None:
+            x = torch.empty_like(b)
+        capi.call("culipx_prec_apply", self._h, int(stage), _dptr(b), _dptr(x))
+        return x
+
+    def __del__(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            capi.load().culipx_factor_destroy(self._h)
+            self._h = None
+
+
+class CsrOperator:
+    """CSR operator over torch CUDA tensors (kept alive by this object)."""
+
+    def __init__(self, handle: Handle, rowptr, colidx, val, ncols=None, explicit_transpose=False):
+        self.handle = handle
+        self.rowptr, self.colidx, self.val = rowptr, colidx, val
+        self.m = rowptr.numel() - 1
+        self.n = self.m if ncols is None else ncols
+        import torch
+
+        prec = F64 if val.dtype == torch.float64 else F32
+        A = ctypes.c_void_p()
+        capi.call("culipx_csr_create", handle._h, self.m, self.n, colidx.numel(), _dptr(rowptr), _dptr(colidx),
+                  _dptr(val), prec, 1 if explicit_transpose else 0, ctypes.byref(A))
+        self._h = A
+
+    def spmv(self, x, y, alpha=1.0, beta=0.0, transpose=False):
+        capi.call("culipx_spmv", self._h, _dptr(x), _dptr(y), float(alpha), float(beta), 1 if transpose else 0)
+        return y
+
+    def __del__(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            capi.load().culipx_csr_destroy(self._h)
+            self._h = None
+
+
+def sqmr_solve(handle: Handle, A: CsrOperator, M: Factor | None, b, x, tol=1e-8, max_it=1000):
+    """Returns (residual, iterations, status); status is OK or MAXIT."""
+    res = ctypes.c_double()
+    its = ctypes.c_int()
+    st = capi.call("culipx_sqmr_solve", handle._h, A._h, M._h if M is not None else None, _dptr(b), _dptr(x),
+                   float(tol), int(max_it), ctypes.byref(res), ctypes.byref(its), allow=(capi.OK, capi.MAXIT))
+    return res.value, its.value, st
+
+
+# --------------------------------------------------------------------------
+# Reference-named facade (same names, argument meaning and return values)
+
+SOLVE_STRIPE, SOLVE_BLOCK, SOLVE_SCALAR, SOLVE_JACOBI = range(4)
+
+
+class BlockiLDLt:
+    """BlockiLDLt<T, BK, Rook>(handle, h_A, num_pivs, piv_starts, num_blocks, block_starts).
+
+    h_A is a host CSR triple (rowptr, colidx, val); piv_starts lists the rows
+    where a pivot starts (num_pivs entries, as apps/block_ildlt builds it from
+    the is_piv file); pivot is PIV_STATIC / PIV_BK / PIV_ROOK (the template
+    flags); precision F64 / F32 (T).
+    """
+
+    def __init__(self, handle: Handle, h_A, num_pivs, piv_starts, num_blocks, block_starts, pivot=PIV_BK,
+                 precision=F64):
+        self.handle = handle
+        self.rowptr, self.colidx, self.val = (np.ascontiguousarray(h_A[0], np.int32),
+                                              np.ascontiguousarray(h_A[1], np.int32),
+                                              np.ascontiguousarray(h_A[2], np.float64))
+        self.n_ = len(self.rowptr) - 1
+        self.block_starts = np.ascontiguousarray(block_starts[:num_blocks], np.int32)
+        self.is_piv = np.zeros(self.n_, np.int32)
+        self.is_piv[np.asarray(piv_starts[:num_pivs], dtype=np.int64)] = 1
+        self.pivot = pivot
+        self.precision = precision
+        self.pattern = None
+        self.factor = None
+        self.algorithm = SOLVE_BLOCK
+
+    def n(self):
+        return self.n_
+
+    def compute(self, fill_level, fill_factor, threshold):
+        self.pattern = Pattern(self.handle, self.rowptr, self.colidx, self.block_starts, fill_level,
+                               max(1.0, float(fill_factor)), self.precision)
+        self.factor = Factor(self.pattern)
+        self.factor.compute(self.val, self.is_piv, self.pivot, threshold)
+        return 0
+
+    def is_left(self):
+        return True
+
+    def is_middle(self):
+        return True
+
+    def is_right(self):
+        return True
+
+    def set_solve_algorithm(self, algorithm, num_jacobi_sweeps=0):
+        if algorithm != SOLVE_BLOCK:
+            raise CulipxError(capi.NOT_SUPPORTED, "only the level-scheduled block solve (SOLVE_BLOCK) is provided")
+        self.algorithm = algorithm
+
+    def solve_analysis(self):
+        # the sweep structures are built with the factor
+        return None
+
+    def solve_left(self, b, x, transpose=False):
+        return self.factor.apply(RIGHT if transpose else LEFT, b, x)
+
+    def solve_middle(self, b, x, transpose=False):
+        return self.factor.apply(MIDDLE, b, x)
+
+    def solve_right(self, b, x, transpose=False):
+        return self.factor.apply(LEFT if transpose else RIGHT, b, x)
+
+    def export_factorized(self) -> dict:
+        return self.factor.export()
+
+
+class CSRMatrixSPMV:
+    """CSRMatrixSPMV<T>(handle, A, explicit_At): b = alpha op(A) x + beta b."""
+
+    def __init__(self, handle: Handle, A: CsrOperator | tuple, explicit_At=False):
+        if isinstance(A, tuple):
+            A = CsrOperator(handle, *A, explicit_transpose=explicit_At)
+        self.A = A
+
+    def m(self):
+        return self.A.m
+
+    def n(self):
+        return self.A.n
+
+    def multiply(self, x, b, alpha=1.0, beta=0.0, transpose=False):
+        return self.A.spmv(x, b, alpha, beta, transpose)
+
+
+class SQMR:
+    """SQMR<T>(handle, spmv, tol, max_it, prec).solve(b, x) -> (residual, iterations)."""
+
+    def __init__(self, handle: Handle, spmv: CSRMatrixSPMV, tol, max_it, preconditioner: BlockiLDLt | None = None):
+        self.handle, self.spmv, self.tol, self.max_it, self.prec = handle, spmv, tol, max_it, preconditioner
+
+    def solve(self, b, x):
+        M = self.prec.factor if self.prec is not None else None
+        res, its, _ = sqmr_solve(self.handle, self.spmv.A, M, b, x, self.tol, self.max_it)
+        return res, its

@@ -1,0 +1,317 @@
+// extern "C" entry points of libculipx (declared in include/culipx.h).
+#include "factor.h"
+#include "pattern.h"
+#include "spmv.h"
+#include "sqmr.h"
+
+#include <cstring>
+#include <new>
+#include <vector>
+
+namespace culipx {
+const char* last_error();
+}
+
+using namespace culipx;
+
+#define GUARD_BEGIN try {
+#define GUARD_END                                                                            \
+    }                                                                                        \
+    catch (const std::bad_alloc&) { return fail(CULIPX_OOM, "host allocation failed"); }     \
+    catch (...) { return fail(CULIPX_CUDA_ERROR, "unexpected exception"); }
+
+namespace {
+int use_device(culipx_handle_t* h)
+{
+    if (h->device < 0) return CULIPX_OK;  // host-only handle
+    CULIPX_CUDA(cudaSetDevice(h->device));
+    return CULIPX_OK;
+}
+}  // namespace
+
+extern "C" {
+
+CULIPX_API const char* culipx_last_error(void) { return last_error(); }
+
+CULIPX_API int culipx_version(void) { return 10000; }
+
+CULIPX_API int culipx_handle_create(culipx_handle* out, int device, void* cuda_stream)
+{
+    if (!out) return fail(CULIPX_INVALID_ARG, "culipx_handle_create: null out");
+    GUARD_BEGIN
+    if (device == -1) {
+        // host-only handle: symbolic analysis without a device mirror
+        auto* h = new culipx_handle_t();
+        h->device = -1;
+        h->sqmr = new Sqmr();
+        *out = h;
+        return CULIPX_OK;
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(CULIPX_CUDA_ERROR, "culipx_handle_create: no CUDA device");
+    }
+    if (device < 0 || device >= ndev) return fail(CULIPX_INVALID_ARG, "culipx_handle_create: bad device %d", device);
+    auto* h = new culipx_handle_t();
+    h->device = device;
+    h->stream = static_cast<cudaStream_t>(cuda_stream);
+    if (cudaSetDevice(device) != cudaSuccess || cudaEventCreate(&h->ev_start) != cudaSuccess ||
+        cudaEventCreate(&h->ev_stop) != cudaSuccess) {
+        delete h;
+        return fail(CULIPX_CUDA_ERROR, "culipx_handle_create: CUDA initialization failed");
+    }
+    h->sqmr = new Sqmr();
+    *out = h;
+    return CULIPX_OK;
+    GUARD_END
+}
+
+CULIPX_API int culipx_handle_destroy(culipx_handle h)
+{
+    if (!h) return CULIPX_OK;
+    if (h->device >= 0) cudaSetDevice(h->device);
+    delete h->sqmr;
+    if (h->ev_start) cudaEventDestroy(h->ev_start);
+    if (h->ev_stop) cudaEventDestroy(h->ev_stop);
+    delete h;
+    return CULIPX_OK;
+}
+
+CULIPX_API int culipx_handle_set_stream(culipx_handle h, void* cuda_stream)
+{
+    if (!h) return fail(CULIPX_INVALID_ARG, "null handle");
+    h->stream = static_cast<cudaStream_t>(cuda_stream);
+    return CULIPX_OK;
+}
+
+CULIPX_API int culipx_handle_set_memory_budget(culipx_handle h, long long bytes)
+{
+    if (!h) return fail(CULIPX_INVALID_ARG, "null handle");
+    h->budget = bytes;
+    return CULIPX_OK;
+}
+
+CULIPX_API int culipx_handle_memory_used(culipx_handle h, long long* bytes)
+{
+    if (!h || !bytes) return fail(CULIPX_INVALID_ARG, "null argument");
+    *bytes = h->used.load();
+    return CULIPX_OK;
+}
+
+CULIPX_API int culipx_handle_launch_count(culipx_handle h, long long* count, int reset)
+{
+    if (!h || !count) return fail(CULIPX_INVALID_ARG, "null argument");
+    *count = h->launches;
+    if (reset) h->launches = 0;
+    return CULIPX_OK;
+}
+
+CULIPX_API int culipx_handle_synchronize(culipx_handle h)
+{
+    if (!h) return fail(CULIPX_INVALID_ARG, "null handle");
+    CULIPX_TRY(use_device(h));
+    CULIPX_CUDA(cudaStreamSynchronize(h->stream));
+    return CULIPX_OK;
+}
+
+CULIPX_API int culipx_pattern_analyze(culipx_handle h, int n, const int* h_rowptr, const int* h_colidx,
+                                      int num_blocks, const int* h_block_starts, int fill_level,
+                                      double fill_factor, int precision, culipx_pattern* out)
+{
+    if (!h) return fail(CULIPX_INVALID_ARG, "null handle");
+    GUARD_BEGIN
+    CULIPX_TRY(use_device(h));
+    Pattern* p = nullptr;
+    CULIPX_TRY(analyze_pattern(h, n, h_rowptr, h_colidx, num_blocks, h_block_starts, fill_level, fill_factor,
+                               precision, &p));
+    *out = static_cast<culipx_pattern>(p);
+    return CULIPX_OK;
+    GUARD_END
+}
+
+CULIPX_API int culipx_pattern_destroy(culipx_pattern p)
+{
+    if (p) {
+        if (p->handle->device >= 0) cudaSetDevice(p->handle->device);
+        delete p;
+    }
+    return CULIPX_OK;
+}
+
+CULIPX_API int culipx_pattern_info(culipx_pattern p, long long* info)
+{
+    if (!p || !info) return fail(CULIPX_INVALID_ARG, "null argument");
+    const long long v[16] = {p->n,          p->nnz,           p->num_blocks,     p->coarse_nnz,
+                             p->fill_nnz,   p->num_levels,    p->num_sparse,     p->num_dense,
+                             p->val_slots,  p->val_slots,     p->max_level_blocks, p->max_level_rows,
+                             p->device_bytes, p->precision,   0,                 0};
+    std::memcpy(info, v, sizeof(v));
+    return CULIPX_OK;
+}
+
+CULIPX_API int culipx_pattern_export(culipx_pattern p, int* coarse_off, int* coarse_col, int* blk_nnzA,
+                                     int* lvl_off, int* lvl_rows, int* lb_off, int* lb, int* sb_off, int* sb,
+                                     int* fmt, int* max_nnz)
+{
+    if (!p) return fail(CULIPX_INVALID_ARG, "null pattern");
+    auto cp = [](int* dst, const std::vector<int>& src) {
+        if (dst && !src.empty()) std::memcpy(dst, src.data(), src.size() * sizeof(int));
+    };
+    cp(coarse_off, p->cs_off);
+    cp(coarse_col, p->cs_col);
+    cp(blk_nnzA, p->blk_nnzA);
+    cp(lvl_off, p->lvl_off);
+    cp(lvl_rows, p->lvl_rows);
+    cp(lb_off, p->lb_off);
+    cp(lb, p->lb);
+    cp(sb_off, p->sb_off);
+    cp(sb, p->sb);
+    cp(fmt, p->fmt);
+    cp(max_nnz, p->max_nnz);
+    return CULIPX_OK;
+}
+
+CULIPX_API int culipx_factor_create(culipx_pattern p, culipx_factor* out)
+{
+    if (!p || !out) return fail(CULIPX_INVALID_ARG, "null argument");
+    if (p->handle->device < 0) return fail(CULIPX_INVALID_ARG, "culipx_factor_create: pattern was analyzed on a host-only handle");
+    GUARD_BEGIN
+    CULIPX_TRY(use_device(p->handle));
+    Factor* f = nullptr;
+    CULIPX_TRY(factor_create(p, &f));
+    *out = static_cast<culipx_factor>(f);
+    return CULIPX_OK;
+    GUARD_END
+}
+
+CULIPX_API int culipx_factor_destroy(culipx_factor f)
+{
+    if (f) {
+        cudaSetDevice(f->pat->handle->device);
+        delete f;
+    }
+    return CULIPX_OK;
+}
+
+CULIPX_API int culipx_factor_compute(culipx_factor f, const void* d_vals, const int* h_is_piv, int pivot,
+                                     double threshold)
+{
+    if (!f) return fail(CULIPX_INVALID_ARG, "null factor");
+    GUARD_BEGIN
+    CULIPX_TRY(use_device(f->pat->handle));
+    return factor_compute(f, d_vals, h_is_piv, pivot, threshold);
+    GUARD_END
+}
+
+CULIPX_API int culipx_factor_compute_host(culipx_factor f, const double* h_vals, const int* h_is_piv, int pivot,
+                                          double threshold)
+{
+    if (!f || !h_vals) return fail(CULIPX_INVALID_ARG, "null argument");
+    GUARD_BEGIN
+    culipx_handle_t* h = f->pat->handle;
+    CULIPX_TRY(use_device(h));
+    const long long nnz = f->pat->nnz;
+    DeviceBuffer tmp;
+    if (f->precision == CULIPX_F64) {
+        CULIPX_TRY(tmp.upload(h, h_vals, nnz * sizeof(double)));
+    } else {
+        std::vector<float> fv(h_vals, h_vals + nnz);
+        CULIPX_TRY(tmp.upload(h, fv.data(), nnz * sizeof(float)));
+    }
+    return factor_compute(f, tmp.get(), h_is_piv, pivot, threshold);
+    GUARD_END
+}
+
+CULIPX_API int culipx_factor_export_size(culipx_factor f, long long* entries)
+{
+    if (!f || !entries) return fail(CULIPX_INVALID_ARG, "null argument");
+    GUARD_BEGIN
+    CULIPX_TRY(use_device(f->pat->handle));
+    return factor_export(f, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, entries);
+    GUARD_END
+}
+
+CULIPX_API int culipx_factor_export(culipx_factor f, int* h_blk_nnz, long long* h_blk_off, int* h_idx, void* h_val,
+                                    void* h_tri, int* h_is_piv, int* h_perm, int* h_got_extra)
+{
+    if (!f) return fail(CULIPX_INVALID_ARG, "null factor");
+    GUARD_BEGIN
+    CULIPX_TRY(use_device(f->pat->handle));
+    return factor_export(f, h_blk_nnz, h_blk_off, h_idx, h_val, h_tri, h_is_piv, h_perm, h_got_extra, nullptr);
+    GUARD_END
+}
+
+CULIPX_API int culipx_factor_stats(culipx_factor f, double* ms, int* launches)
+{
+    if (!f) return fail(CULIPX_INVALID_ARG, "null factor");
+    if (ms) *ms = f->last_ms;
+    if (launches) *launches = f->last_launches;
+    return CULIPX_OK;
+}
+
+CULIPX_API int culipx_prec_apply(culipx_factor f, int stage, const void* d_b, void* d_x)
+{
+    if (!f) return fail(CULIPX_INVALID_ARG, "null factor");
+    GUARD_BEGIN
+    CULIPX_TRY(use_device(f->pat->handle));
+    return prec_apply(f, stage, d_b, d_x, f->pat->handle->stream);
+    GUARD_END
+}
+
+CULIPX_API int culipx_csr_create(culipx_handle h, int m, int n, long long nnz, const int* d_rowptr,
+                                 const int* d_colidx, const void* d_val, int precision, int explicit_transpose,
+                                 culipx_csr* out)
+{
+    if (!h || !out || m < 0 || n < 0 || nnz < 0 || (nnz > 0 && (!d_colidx || !d_val)) || !d_rowptr)
+        return fail(CULIPX_INVALID_ARG, "culipx_csr_create: bad arguments");
+    if (h->device < 0) return fail(CULIPX_INVALID_ARG, "culipx_csr_create: host-only handle");
+    if (precision != CULIPX_F64 && precision != CULIPX_F32)
+        return fail(CULIPX_INVALID_ARG, "culipx_csr_create: bad precision");
+    GUARD_BEGIN
+    CULIPX_TRY(use_device(h));
+    auto* A = new culipx_csr_t();
+    A->h = h;
+    A->m = m;
+    A->n = n;
+    A->nnz = nnz;
+    A->rowptr = d_rowptr;
+    A->colidx = d_colidx;
+    A->val = d_val;
+    A->precision = precision;
+    if (explicit_transpose) {
+        const int st = csr_build_transpose(A);
+        if (st) { delete A; return st; }
+    }
+    *out = A;
+    return CULIPX_OK;
+    GUARD_END
+}
+
+CULIPX_API int culipx_csr_destroy(culipx_csr A)
+{
+    delete A;
+    return CULIPX_OK;
+}
+
+CULIPX_API int culipx_spmv(culipx_csr A, const void* d_x, void* d_y, double alpha, double beta, int transpose)
+{
+    if (!A) return fail(CULIPX_INVALID_ARG, "null operator");
+    GUARD_BEGIN
+    CULIPX_TRY(use_device(A->h));
+    return csr_spmv(A, d_x, d_y, alpha, beta, transpose, A->h->stream);
+    GUARD_END
+}
+
+CULIPX_API int culipx_sqmr_solve(culipx_handle h, culipx_csr A, culipx_factor M, const double* d_b, double* d_x,
+                                 double tol, int max_it, double* residual, int* iterations)
+{
+    if (!h) return fail(CULIPX_INVALID_ARG, "null handle");
+    if (h->device < 0) return fail(CULIPX_INVALID_ARG, "culipx_sqmr_solve: host-only handle");
+    GUARD_BEGIN
+    CULIPX_TRY(use_device(h));
+    return sqmr_solve(h, A, M, d_b, d_x, tol, max_it, residual, iterations, h->sqmr);
+    GUARD_END
+}
+
+}  // extern "C"

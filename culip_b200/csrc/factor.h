@@ -1,0 +1,52 @@
+// Numeric block-iLDL^T factor on the device and the solve structures built
+// from it.
+#pragma once
+
+#include "pattern.h"
+
+namespace culipx {
+
+struct Factor {
+    Pattern* pat = nullptr;
+    int precision = CULIPX_F64;
+    size_t vbytes = 8;
+    bool computed = false;
+    int pivot = CULIPX_PIV_BK;
+    double threshold = 0.0;
+
+    // block storage (pattern layout + relocation arena for blocks that were
+    // granted extra slots by dual dropping)
+    DeviceBuffer val, idx;       // val_cap slots
+    long long val_cap = 0;
+    DeviceBuffer boff;           // per block: slot offset (int64)
+    DeviceBuffer nnz, cap;       // per block: stored entries (sparse), capacity after grants
+    DeviceBuffer got_extra;      // per block
+    DeviceBuffer tri;            // 3n values
+    DeviceBuffer is_piv, perm;   // n ints
+    DeviceBuffer rowflags;       // per block row: bit0 pivot tile is identity, bit1 D has a 2x2
+    DeviceBuffer state;          // device scalars (see factor.cu)
+    DeviceBuffer deferred;       // per level list of deferred blocks
+    DeviceBuffer norm_part;      // threshold > 0: row-norm partials
+    DeviceBuffer row_norm;       // n values
+
+    // sweep structures (fine-row CSR of the strictly off-diagonal block part)
+    DeviceBuffer u_off, u_col, u_val;    // rows of U
+    DeviceBuffer ut_off, ut_col, ut_val; // rows of U' (columns of U)
+    DeviceBuffer piv_off;                // per block row: value slot of its pivot tile
+    DeviceBuffer work;                   // n values of apply scratch
+    DeviceBuffer scan_tmp;               // scan partial sums
+    long long u_nnz = 0;
+
+    float last_ms = 0.f;
+    int last_launches = 0;
+};
+
+int factor_create(Pattern* p, Factor** out);
+int factor_compute(Factor* f, const void* d_vals, const int* h_is_piv, int pivot, double threshold);
+int factor_export(Factor* f, int* blk_nnz, long long* blk_off, int* idx, void* val, void* tri,
+                  int* is_piv, int* perm, int* got_extra, long long* total);
+int prec_apply(Factor* f, int stage, const void* d_b, void* d_x, cudaStream_t stream);
+
+}  // namespace culipx
+
+struct culipx_factor_t : culipx::Factor {};

@@ -1,0 +1,421 @@
+// Preconditioner applies for the block-iLDL^T factor: level-scheduled block
+// triangular sweeps, the 1x1/2x2 block-diagonal D solve and the pivot
+// permutation.
+//
+// Reference: solve_left / solve_middle / solve_right
+// (libs/la/preconditioner/block_ildlt.impl.cuh:183-246), solve_U_block /
+// solve_Ut_block (:2378-2426, :2557-2606) with k_solve_blocks_offdiagonal_atomic
+// and k_solve_blocks_diagonal_atomic (block_ildlt_kernels.impl.cuh:2353-2606),
+// k_solve_D and k_permute_P / k_permute_Pt (libs/la/helper_kernels.impl.cuh:720-816).
+//
+// Design: after the numeric factor, the strictly off-diagonal block part of
+// U is re-laid out once as two fine-row CSR arrays (rows of U for the U
+// sweep, rows of U' for the U' sweep), each row sorted by column.  A sweep
+// level is then one warp per block row, one lane per fine row: the lane
+// subtracts its row's terms in column order (no atomics, deterministic; the
+// reference adds them with atomicAdd) and the warp finishes with the
+// triangular solve on the dense pivot tile, skipped when the tile is exactly
+// the identity (then the reference's divide-by-1 / subtract-0 steps are
+// exact no-ops).
+#include "factor.h"
+#include "kernels_common.cuh"
+#include "block_io.cuh"
+
+namespace culipx {
+
+namespace {
+
+constexpr int kSweepWarps = 4;
+
+// ---------------------------------------------------------------------------
+// exclusive scan of n+1 int counts (in place), three passes
+constexpr int kScanThreads = 512;
+constexpr int kScanItems = 8;
+constexpr int kScanChunk = kScanThreads * kScanItems;
+
+__device__ int block_exclusive_scan(int v, int* warp_sums, int* total)
+{
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int incl = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    if (lane == 31) warp_sums[w] = incl;
+    __syncthreads();
+    if (w == 0) {
+        const int nw = blockDim.x >> 5;
+        int s = (lane < nw) ? warp_sums[lane] : 0;
+        int si = s;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, si, o);
+            if (lane >= o) si += t;
+        }
+        if (lane < nw) warp_sums[lane] = si - s;
+        if (lane == nw - 1) *total = si;
+    }
+    __syncthreads();
+    const int r = warp_sums[w] + incl - v;
+    __syncthreads();
+    return r;
+}
+
+__global__ void k_scan_chunks(int* data, int n, int* sums)
+{
+    __shared__ int ws[32];
+    __shared__ int tot;
+    const long long base = (long long)blockIdx.x * kScanChunk + threadIdx.x * kScanItems;
+    int loc[kScanItems];
+    int s = 0;
+    for (int k = 0; k < kScanItems; ++k) {
+        const long long i = base + k;
+        loc[k] = (i < n) ? data[i] : 0;
+        s += loc[k];
+    }
+    int off = block_exclusive_scan(s, ws, &tot);
+    for (int k = 0; k < kScanItems; ++k) {
+        const long long i = base + k;
+        if (i < n) data[i] = off;
+        off += loc[k];
+    }
+    if (threadIdx.x == 0) sums[blockIdx.x] = tot;
+}
+
+__global__ void k_scan_sums(int* sums, int m)
+{
+    __shared__ int ws[32];
+    __shared__ int tot;
+    int carry = 0;
+    for (int base = 0; base < m; base += blockDim.x) {
+        const int i = base + threadIdx.x;
+        const int v = (i < m) ? sums[i] : 0;
+        const int e = block_exclusive_scan(v, ws, &tot);
+        if (i < m) sums[i] = carry + e;
+        carry += tot;
+        __syncthreads();
+    }
+}
+
+__global__ void k_scan_add(int* data, int n, const int* sums)
+{
+    const long long base = (long long)blockIdx.x * kScanChunk;
+    const int add = sums[blockIdx.x];
+    for (int k = threadIdx.x; k < kScanChunk; k += blockDim.x) {
+        const long long i = base + k;
+        if (i < n) data[i] += add;
+    }
+}
+
+// ---------------------------------------------------------------------------
+struct SweepBuild {
+    const DevBlock* desc;
+    const int* bs;
+    const int* cs_off;
+    const int* csc_off;
+    const int* csc_blk;
+    const int* fmt;
+    const long long* boff;
+    const int* nnz;
+    const int* idx;
+};
+
+// per fine row of U and of U': number of non-zero off-diagonal entries
+template <class T>
+__global__ void k_count_offdiag(SweepBuild a, const T* val, int nblocks_total, int* cnt_u, int* cnt_ut)
+{
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    const int lane = lane_id();
+    for (int b = warp; b < nblocks_total; b += nwarps) {
+        const DevBlock d = a.desc[b];
+        if (d.row == d.col) continue;
+        const int fr = a.bs[d.row], h = a.bs[d.row + 1] - fr;
+        const int fc = a.bs[d.col], w = a.bs[d.col + 1] - fc;
+        const long long off = a.boff[b];
+        if (a.fmt[b] == 1) {
+            int colcount = 0;
+            for (int i = 0; i < h; ++i) {
+                const bool nz = lane < w && val[off + (long long)i * w + lane] != T(0);
+                const unsigned m = __ballot_sync(0xffffffffu, nz);
+                if (lane == 0 && m) atomicAdd(&cnt_u[fr + i], __popc(m));
+                colcount += nz;
+            }
+            if (lane < w && colcount) atomicAdd(&cnt_ut[fc + lane], colcount);
+        } else {
+            const int cnt = a.nnz[b];
+            for (int e = lane; e < cnt; e += 32) {
+                if (val[off + e] == T(0)) continue;
+                const int li = a.idx[off + e];
+                const int r = li / w, c = li - r * w;
+                atomicAdd(&cnt_u[fr + r], 1);
+                atomicAdd(&cnt_ut[fc + c], 1);
+            }
+        }
+    }
+}
+
+// rows of U: warp per block row, blocks in column order, each row in column order
+template <class T>
+__global__ void __launch_bounds__(32 * kSweepWarps) k_fill_u_rows(SweepBuild a, const T* val, int cm,
+                                                                   const int* u_off, int* u_col, T* u_val)
+{
+    __shared__ T tiles[kSweepWarps][kTileElems];
+    const int warp = threadIdx.x >> 5;
+    const int I = blockIdx.x * kSweepWarps + warp;
+    if (I >= cm) return;
+    const int lane = lane_id();
+    T* tile = tiles[warp];
+    for (int e = lane; e < kTileElems; e += 32) tile[e] = T(0);
+    __syncwarp();
+    const int fr = a.bs[I], h = a.bs[I + 1] - fr;
+    int run = 0;  // lane i: entries written so far in row fr + i
+    for (int q = a.cs_off[I] + 1; q < a.cs_off[I + 1]; ++q) {
+        const int J = a.desc[q].col;
+        const int fc = a.bs[J], w = a.bs[J + 1] - fc;
+        load_block(tile, q, a.desc, a.bs, a.boff, a.nnz, a.fmt, val, a.idx, false);
+        for (int i = 0; i < h; ++i) {
+            const T v = (lane < w) ? tile[i * kTileStride + lane] : T(0);
+            const bool nz = v != T(0);
+            const unsigned m = __ballot_sync(0xffffffffu, nz);
+            const int base = u_off[fr + i] + shfl(run, i);
+            if (nz) {
+                const int pos = base + __popc(m & ((1u << lane) - 1u));
+                u_col[pos] = fc + lane;
+                u_val[pos] = v;
+            }
+            if (lane == i) run += __popc(m);
+        }
+        unload_block(tile, q, a.desc, a.bs, a.boff, a.nnz, a.fmt, a.idx);
+    }
+}
+
+// rows of U' (columns of U): warp per block column, blocks in row order
+template <class T>
+__global__ void __launch_bounds__(32 * kSweepWarps) k_fill_ut_rows(SweepBuild a, const T* val, int cm,
+                                                                    const int* ut_off, int* ut_col, T* ut_val)
+{
+    __shared__ T tiles[kSweepWarps][kTileElems];
+    const int warp = threadIdx.x >> 5;
+    const int J = blockIdx.x * kSweepWarps + warp;
+    if (J >= cm) return;
+    const int lane = lane_id();
+    T* tile = tiles[warp];
+    for (int e = lane; e < kTileElems; e += 32) tile[e] = T(0);
+    __syncwarp();
+    const int fc = a.bs[J], w = a.bs[J + 1] - fc;
+    int run = 0;  // lane c: entries written so far in U' row fc + c
+    for (int q = a.csc_off[J]; q < a.csc_off[J + 1] - 1; ++q) {
+        const int b = a.csc_blk[q];
+        const int K = a.desc[b].row;
+        const int fr = a.bs[K], h = a.bs[K + 1] - fr;
+        load_block(tile, b, a.desc, a.bs, a.boff, a.nnz, a.fmt, val, a.idx, false);
+        for (int c = 0; c < w; ++c) {
+            const T v = (lane < h) ? tile[lane * kTileStride + c] : T(0);
+            const bool nz = v != T(0);
+            const unsigned m = __ballot_sync(0xffffffffu, nz);
+            const int base = ut_off[fc + c] + shfl(run, c);
+            if (nz) {
+                const int pos = base + __popc(m & ((1u << lane) - 1u));
+                ut_col[pos] = fr + lane;
+                ut_val[pos] = v;
+            }
+            if (lane == c) run += __popc(m);
+        }
+        unload_block(tile, b, a.desc, a.bs, a.boff, a.nnz, a.fmt, a.idx);
+    }
+}
+
+__global__ void k_pivot_offsets(int cm, const int* csc_off, const int* csc_blk, const long long* boff,
+                                long long* piv_off)
+{
+    for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < cm; I += gridDim.x * blockDim.x)
+        piv_off[I] = boff[csc_blk[csc_off[I + 1] - 1]];
+}
+
+// ---------------------------------------------------------------------------
+// one level of the U (UPPER) or U' sweep, in place on x
+template <class T, bool UPPER>
+__global__ void __launch_bounds__(32 * kSweepWarps)
+    k_sweep_level(const int* __restrict__ rows, int nrows, const int* __restrict__ bs,
+                  const int* __restrict__ off, const int* __restrict__ col, const T* __restrict__ vals,
+                  const long long* __restrict__ piv_off, const int* __restrict__ rowflags,
+                  const T* __restrict__ fval, T* __restrict__ x)
+{
+    __shared__ T tiles[kSweepWarps][kTileElems];
+    const int warp = threadIdx.x >> 5;
+    const int t = blockIdx.x * kSweepWarps + warp;
+    if (t >= nrows) return;
+    const int lane = lane_id();
+    const int I = rows[t];
+    const int fr = bs[I], h = bs[I + 1] - fr;
+    T acc = T(0);
+    if (lane < h) {
+        acc = x[fr + lane];
+        const int e1 = off[fr + lane + 1];
+        for (int k = off[fr + lane]; k < e1; ++k) acc = fma_rn(-vals[k], x[col[k]], acc);
+    }
+    if (!(rowflags[I] & 1)) {
+        T* tile = tiles[warp];
+        const T* P = fval + piv_off[I];
+        if (lane < h)
+            for (int i = 0; i < h; ++i) tile[i * kTileStride + lane] = P[i * h + lane];
+        __syncwarp();
+        if (UPPER) {
+            for (int c = h - 1; c >= 0; --c) {
+                if (lane == c) acc = acc / tile[c * kTileStride + c];
+                const T xc = shfl(acc, c);
+                if (lane < c) acc = fma_rn(-tile[lane * kTileStride + c], xc, acc);
+            }
+        } else {
+            for (int r = 0; r < h; ++r) {
+                if (lane == r) acc = acc / tile[r * kTileStride + r];
+                const T xr = shfl(acc, r);
+                if (lane > r && lane < h) acc = fma_rn(-tile[r * kTileStride + lane], xr, acc);
+            }
+        }
+    }
+    if (lane < h) x[fr + lane] = acc;
+}
+
+// k_solve_D: Givens-based 1x1 / 2x2 block-diagonal solve (out may equal in)
+template <class T>
+__global__ void k_solve_D(const T* __restrict__ tri, const int* __restrict__ is_piv, const T* in, T* out, int n)
+{
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < n; g += gridDim.x * blockDim.x) {
+        const int this_piv = is_piv[g];
+        const int next_piv = (g < n - 1) ? is_piv[g + 1] : 1;
+        const T p11 = tri[3 * (size_t)g + 1], p12 = tri[3 * (size_t)g + 2];
+        const T p22 = !next_piv ? tri[3 * (size_t)(g + 1) + 1] : T(1);
+        const T r1 = in[g], r2 = (g < n - 1) ? in[g + 1] : T(0);
+        const T gr = sqrt(fma_rn(p11, p11, p12 * p12));
+        const T gc = p11 / gr, gs = p12 / gr;
+        T g1 = fma_rn(gc, r1, gs * r2);
+        T g2 = fma_rn(-gs, r1, gc * r2);
+        const T tp12 = fma_rn(gc, p12, gs * p22);
+        const T tp22 = fma_rn(-gs, p12, gc * p22);
+        g2 = g2 / tp22;
+        g1 = fma_rn(-tp12, g2, g1) / gr;
+        if (this_piv) out[g] = g1;
+        if (!next_piv) out[g + 1] = g2;
+    }
+}
+
+template <class T>
+__global__ void k_perm_gather(const T* __restrict__ b, T* __restrict__ x, const int* __restrict__ perm, int n)
+{
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < n; g += gridDim.x * blockDim.x) x[g] = b[perm[g]];
+}
+
+template <class T>
+__global__ void k_perm_scatter(const T* __restrict__ b, T* __restrict__ x, const int* __restrict__ perm, int n)
+{
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < n; g += gridDim.x * blockDim.x) x[perm[g]] = b[g];
+}
+
+int exclusive_scan(int* d, int n, DeviceBuffer& tmp, culipx_handle_t* h, cudaStream_t s, int* launches)
+{
+    const int chunks = (n + kScanChunk - 1) / kScanChunk;
+    if ((size_t)chunks * sizeof(int) > tmp.bytes()) CULIPX_TRY(tmp.alloc(h, (size_t)chunks * sizeof(int)));
+    k_scan_chunks<<<chunks, kScanThreads, 0, s>>>(d, n, tmp.as<int>());
+    k_scan_sums<<<1, 1024, 0, s>>>(tmp.as<int>(), chunks);
+    k_scan_add<<<chunks, kScanThreads, 0, s>>>(d, n, tmp.as<int>());
+    *launches += 3;
+    return launch_check("exclusive_scan");
+}
+
+template <class T>
+int build_sweeps_t(Factor* f, cudaStream_t s, int* launches)
+{
+    Pattern& p = *f->pat;
+    const int n = p.n, cm = p.num_blocks;
+    SweepBuild a;
+    a.desc = p.d_desc.as<DevBlock>();
+    a.bs = p.d_bs.as<int>();
+    a.cs_off = p.d_cs_off.as<int>();
+    a.csc_off = p.d_csc_off.as<int>();
+    a.csc_blk = p.d_csc_blk.as<int>();
+    a.fmt = p.d_fmt.as<int>();
+    a.boff = f->boff.as<long long>();
+    a.nnz = f->nnz.as<int>();
+    a.idx = f->idx.as<int>();
+    const T* val = f->val.as<T>();
+    int* u_off = f->u_off.as<int>();
+    int* ut_off = f->ut_off.as<int>();
+    CULIPX_CUDA(cudaMemsetAsync(u_off, 0, (n + 1) * sizeof(int), s));
+    CULIPX_CUDA(cudaMemsetAsync(ut_off, 0, (n + 1) * sizeof(int), s));
+    k_count_offdiag<T><<<148 * 8, 256, 0, s>>>(a, val, p.coarse_nnz, u_off, ut_off);
+    ++*launches;
+    CULIPX_TRY(launch_check("k_count_offdiag"));
+    CULIPX_TRY(exclusive_scan(u_off, n + 1, f->scan_tmp, p.handle, s, launches));
+    CULIPX_TRY(exclusive_scan(ut_off, n + 1, f->scan_tmp, p.handle, s, launches));
+    const int grid = (cm + kSweepWarps - 1) / kSweepWarps;
+    k_fill_u_rows<T><<<grid, 32 * kSweepWarps, 0, s>>>(a, val, cm, u_off, f->u_col.as<int>(), f->u_val.as<T>());
+    k_fill_ut_rows<T><<<grid, 32 * kSweepWarps, 0, s>>>(a, val, cm, ut_off, f->ut_col.as<int>(), f->ut_val.as<T>());
+    k_pivot_offsets<<<(cm + 255) / 256, 256, 0, s>>>(cm, a.csc_off, a.csc_blk, a.boff, f->piv_off.as<long long>());
+    *launches += 3;
+    return launch_check("build_sweeps");
+}
+
+template <class T>
+int apply_t(Factor* f, int stage, const void* d_b, void* d_x, cudaStream_t s)
+{
+    Pattern& p = *f->pat;
+    const int n = p.n;
+    const T* b = static_cast<const T*>(d_b);
+    T* x = static_cast<T*>(d_x);
+    const int grid_n = (n + 255) / 256 < 148 * 8 ? (n + 255) / 256 : 148 * 8;
+    if (stage == CULIPX_MIDDLE) {
+        k_solve_D<T><<<grid_n, 256, 0, s>>>(f->tri.as<T>(), f->is_piv.as<int>(), b, x, n);
+        return launch_check("k_solve_D");
+    }
+    const T* fval = f->val.as<T>();
+    if (stage == CULIPX_LEFT) {
+        T* t = x;
+        if ((const void*)b == (void*)x) {
+            t = f->work.as<T>();
+            CULIPX_CUDA(cudaMemcpyAsync(t, b, n * sizeof(T), cudaMemcpyDeviceToDevice, s));
+            k_perm_gather<T><<<grid_n, 256, 0, s>>>(t, x, f->perm.as<int>(), n);
+        } else {
+            k_perm_gather<T><<<grid_n, 256, 0, s>>>(b, x, f->perm.as<int>(), n);
+        }
+        for (int L = 0; L < p.num_levels; ++L) {
+            const int nr = p.lvl_off[L + 1] - p.lvl_off[L];
+            k_sweep_level<T, false><<<(nr + kSweepWarps - 1) / kSweepWarps, 32 * kSweepWarps, 0, s>>>(
+                p.d_lvl_rows.as<int>() + p.lvl_off[L], nr, p.d_bs.as<int>(), f->ut_off.as<int>(),
+                f->ut_col.as<int>(), f->ut_val.as<T>(), f->piv_off.as<long long>(), f->rowflags.as<int>(), fval, x);
+        }
+        return launch_check("U' sweep");
+    }
+    // RIGHT: t = U^-1 b, x = P t
+    T* t = f->work.as<T>();
+    CULIPX_CUDA(cudaMemcpyAsync(t, b, n * sizeof(T), cudaMemcpyDeviceToDevice, s));
+    for (int L = p.num_levels - 1; L >= 0; --L) {
+        const int nr = p.lvl_off[L + 1] - p.lvl_off[L];
+        k_sweep_level<T, true><<<(nr + kSweepWarps - 1) / kSweepWarps, 32 * kSweepWarps, 0, s>>>(
+            p.d_lvl_rows.as<int>() + p.lvl_off[L], nr, p.d_bs.as<int>(), f->u_off.as<int>(), f->u_col.as<int>(),
+            f->u_val.as<T>(), f->piv_off.as<long long>(), f->rowflags.as<int>(), fval, t);
+    }
+    k_perm_scatter<T><<<grid_n, 256, 0, s>>>(t, x, f->perm.as<int>(), n);
+    return launch_check("U sweep");
+}
+
+}  // namespace
+
+int build_sweeps(Factor* f, cudaStream_t s, int* launches)
+{
+    if (f->precision == CULIPX_F64) return build_sweeps_t<double>(f, s, launches);
+    return build_sweeps_t<float>(f, s, launches);
+}
+
+int prec_apply(Factor* f, int stage, const void* d_b, void* d_x, cudaStream_t s)
+{
+    if (!f || !f->computed) return fail(CULIPX_INVALID_ARG, "culipx_prec_apply: factor not computed");
+    if (!d_b || !d_x) return fail(CULIPX_INVALID_ARG, "culipx_prec_apply: null vector");
+    if (stage < CULIPX_LEFT || stage > CULIPX_RIGHT) return fail(CULIPX_INVALID_ARG, "culipx_prec_apply: bad stage");
+    Pattern& p = *f->pat;
+    p.handle->launches += (stage == CULIPX_MIDDLE) ? 1 : p.num_levels + 1;
+    if (f->precision == CULIPX_F64) return apply_t<double>(f, stage, d_b, d_x, s);
+    return apply_t<float>(f, stage, d_b, d_x, s);
+}
+
+}  // namespace culipx

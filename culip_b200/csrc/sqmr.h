@@ -1,0 +1,26 @@
+// SQMR workspace and solver entry.
+#pragma once
+
+#include "device.h"
+#include "spmv.h"
+
+namespace culipx {
+
+struct Factor;
+
+// Work vectors (13 x n doubles), per-CTA partials and the device scalar block.
+struct Sqmr {
+    int n = -1;
+    DeviceBuffer vecs, partials, scal;
+    void* host_flags = nullptr;  // pinned
+    ~Sqmr()
+    {
+        if (host_flags) cudaFreeHost(host_flags);
+    }
+};
+
+int sqmr_workspace(Sqmr* w, culipx_handle_t* h, int n);
+int sqmr_solve(culipx_handle_t* h, Csr* A, Factor* M, const double* b, double* x, double tol, int max_it,
+               double* residual, int* iterations, Sqmr* w);
+
+}  // namespace culipx

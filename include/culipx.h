@@ -1,0 +1,178 @@
+/*
+ * culipx.h -- C ABI of the B200-native block-iLDL^T + SQMR KKT solve path.
+ *
+ * This boundary replaces the parts of culip's libs/la module that the
+ * apps/block_ildlt driver calls (paths relative to the culip repository):
+ *
+ *   gpu_handle_t                 libs/utils/types.cuh:441-482, types.cu:343-430
+ *   BlockiLDLt<T, BK, Rook>      libs/la/preconditioner/block_ildlt.cuh:188-401
+ *     ctor + compute()           libs/la/preconditioner/block_ildlt.impl.cuh:44-146
+ *     solve_analysis()           libs/la/preconditioner/block_ildlt.impl.cuh:1924-2150
+ *     solve_left/middle/right    libs/la/preconditioner/block_ildlt.impl.cuh:183-246
+ *     export_factorized()        libs/la/preconditioner/block_ildlt.impl.cuh:1700-1916
+ *   CSRMatrixSPMV<T>             libs/la/spmv.cuh:19-66, spmv.impl.cuh:29-113
+ *   SQMR<T>                      libs/la/iterative_solvers/sqmr.cuh:29-79,
+ *                                sqmr.impl.cuh:109-369
+ *
+ * Conventions: every entry point returns a culipx status (0 = OK) instead of
+ * raising SIGSEGV as the reference's CHECK_CUDA does (libs/utils/types.cuh:32);
+ * culipx_last_error() describes the last failure of the calling thread.
+ * Pointers named d_* are device pointers on the handle's device, h_* host
+ * pointers.  Indices are 0-based int32 as the reference's mat_int_t
+ * (libs/utils/defines.h:56-63).  Work is issued on the handle's stream.
+ */
+#ifndef CULIPX_H
+#define CULIPX_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define CULIPX_OK            0
+#define CULIPX_INVALID_ARG   1
+#define CULIPX_OOM           2  /* device-memory budget or cudaMalloc exhausted */
+#define CULIPX_BREAKDOWN     3  /* SQMR breakdown (division by zero / non-finite) */
+#define CULIPX_MAXIT         4  /* SQMR hit max_it without passing its test */
+#define CULIPX_TIMEOUT       5  /* a bounded device wait gave up */
+#define CULIPX_CUDA_ERROR    6
+#define CULIPX_NOT_SUPPORTED 7
+
+/* ---- value precision (the reference's T = double / float) ---- */
+#define CULIPX_F64 0
+#define CULIPX_F32 1
+
+/* ---- pivot method, as the driver's argument (apps/block_ildlt/block_ildlt.cc:33-35) ---- */
+#define CULIPX_PIV_STATIC 0
+#define CULIPX_PIV_BK     1
+#define CULIPX_PIV_ROOK   2
+
+/* ---- preconditioner stage (Preconditioner<T>, libs/la/preconditioner.cuh:18-40) ---- */
+#define CULIPX_LEFT   0   /* x = U'^-1 P' b   (solve_left)   */
+#define CULIPX_MIDDLE 1   /* x = D^-1 b       (solve_middle) */
+#define CULIPX_RIGHT  2   /* x = P U^-1 b     (solve_right)  */
+
+typedef struct culipx_handle_t  *culipx_handle;
+typedef struct culipx_pattern_t *culipx_pattern;
+typedef struct culipx_factor_t  *culipx_factor;
+typedef struct culipx_csr_t     *culipx_csr;
+
+const char *culipx_last_error(void);
+int culipx_version(void);
+
+/* ------------------------------------------------------------------------ */
+/* Seeded synthetic KKT systems (no counterpart in the reference, which reads
+ * its inputs from files: apps/block_ildlt/block_ildlt.cc:29-35).           */
+typedef struct culipx_kkt_spec {
+    int n, m;             /* H is n x n, A is m x n; K has order n + m      */
+    int nnz_per_col;      /* distinct nonzeros per column of A              */
+    int band_half;        /* > 0: half of each column within +-band_half of floor(j m / n) */
+    double hmin, hmax;    /* H diagonal, log-uniform                         */
+    double delta, gamma;  /* K = [[H + delta I, A'], [A, -gamma I]]          */
+    unsigned long long seed;
+} culipx_kkt_spec;
+
+int culipx_kkt_nnz(const culipx_kkt_spec *spec, long long *nnz_out);
+/* full symmetric CSR with sorted columns and an explicit diagonal */
+int culipx_kkt_generate(const culipx_kkt_spec *spec, int *h_rowptr, int *h_colidx, double *h_val);
+/* contiguous blocking that never straddles row n; block_starts gets
+ * num_blocks + 1 entries (NULL: only count) */
+int culipx_kkt_blocking(int n, int m, int block, int *h_block_starts, int capacity, int *num_blocks);
+int culipx_normal_vector(unsigned long long seed, long long len, double *h_out);
+
+/* ------------------------------------------------------------------------ */
+/* Handle: device, stream, device-memory budget (replaces gpu_handle_t).    */
+/* device = -1: host-only handle (symbolic analysis only, no CUDA calls) */
+int culipx_handle_create(culipx_handle *out, int device, void *cuda_stream);
+int culipx_handle_destroy(culipx_handle h);
+int culipx_handle_set_stream(culipx_handle h, void *cuda_stream);
+/* cap on the device bytes this handle's objects may hold (<= 0: unlimited) */
+int culipx_handle_set_memory_budget(culipx_handle h, long long bytes);
+int culipx_handle_memory_used(culipx_handle h, long long *bytes);
+int culipx_handle_synchronize(culipx_handle h);
+/* kernels this handle's objects launched (optionally reset to 0) */
+int culipx_handle_launch_count(culipx_handle h, long long *count, int reset);
+
+/* ------------------------------------------------------------------------ */
+/* Symbolic analysis of one sparsity pattern (host; cacheable across IPM
+ * iterations).  Replaces the BlockiLDLt constructor and the symbolic half of
+ * compute(): build_initial_coarse, determine_coarse_level_fill_and_diag,
+ * build_block_csc, find_level_sets, build_blocks
+ * (libs/la/preconditioner/block_ildlt.impl.cuh:352-1280) and
+ * solve_analysis_block (:2050-2150).
+ *   h_rowptr/h_colidx : full symmetric CSR of K (n x n), sorted columns
+ *   h_block_starts    : num_blocks entries (first row of each block), as the
+ *                       reference's constructor; n is appended internally
+ *   fill_level        : block level of fill (>= 0)
+ *   fill_factor       : >= 1, fine fill allowed inside a block
+ *   precision         : CULIPX_F64 / CULIPX_F32 (enters the block-format rule) */
+int culipx_pattern_analyze(culipx_handle h, int n, const int *h_rowptr, const int *h_colidx,
+                           int num_blocks, const int *h_block_starts, int fill_level,
+                           double fill_factor, int precision, culipx_pattern *out);
+int culipx_pattern_destroy(culipx_pattern p);
+/* info[0..15]: n, nnz, num_blocks, coarse_nnz, fill_nnz, num_levels, num_sparse,
+ * num_dense, val_slots, idx_slots, max_level_blocks, max_level_rows,
+ * device_bytes, precision, 0, 0 */
+int culipx_pattern_info(culipx_pattern p, long long *info16);
+/* canonical symbolic output for parity checks (host arrays sized by info):
+ * coarse CSR (num_blocks+1, coarse_nnz), A nnz per block, level offsets
+ * (num_levels+1) and rows (num_blocks, ascending per level), factor-order
+ * block lists (num_levels+1, coarse_nnz), U'-sweep block lists (same),
+ * format (0 sparse, 1 dense) and max_nnz per block.  Any pointer may be NULL. */
+int culipx_pattern_export(culipx_pattern p, int *coarse_off, int *coarse_col, int *blk_nnzA,
+                          int *lvl_off, int *lvl_rows, int *lb_off, int *lb, int *sb_off,
+                          int *sb, int *fmt, int *max_nnz);
+
+/* ------------------------------------------------------------------------ */
+/* Numeric factorization (device).  Replaces BlockiLDLt::factorize
+ * (block_ildlt.impl.cuh:1519-1671) and the kernels it launches.            */
+int culipx_factor_create(culipx_pattern p, culipx_factor *out);
+int culipx_factor_destroy(culipx_factor f);
+/* d_vals: K's values in the pattern's CSR order, in the pattern's precision.
+ * h_is_piv: n flags (1 = a pivot starts at this row), NULL = all ones; used
+ * as given by CULIPX_PIV_STATIC and overwritten by BK / Rook.
+ * threshold: relative dropping threshold (>= 0). */
+int culipx_factor_compute(culipx_factor f, const void *d_vals, const int *h_is_piv, int pivot,
+                          double threshold);
+/* same, with K's values (double) in host memory; converts to the pattern's precision */
+int culipx_factor_compute_host(culipx_factor f, const double *h_vals, const int *h_is_piv,
+                               int pivot, double threshold);
+/* factor export for parity (export_factorized, block_ildlt.impl.cuh:1700-1916):
+ * total entry count, then per block (block-id order) nnz, offsets
+ * (coarse_nnz + 1), entries (sparse: sorted local index row * width + col;
+ * dense: all r * c entries row-major), D as tridiagonal[3n], is_piv[n],
+ * permutation[n] and the extra slots granted by dual dropping.  Values are in
+ * the pattern's precision. */
+int culipx_factor_export_size(culipx_factor f, long long *entries);
+int culipx_factor_export(culipx_factor f, int *h_blk_nnz, long long *h_blk_off, int *h_idx,
+                         void *h_val, void *h_tri, int *h_is_piv, int *h_perm, int *h_got_extra);
+/* timing of the last culipx_factor_compute on the device (ms), and launches */
+int culipx_factor_stats(culipx_factor f, double *ms, int *launches);
+
+/* Preconditioner applies; b and x are device vectors of n values in the
+ * factor's precision (b == x allowed for MIDDLE). */
+int culipx_prec_apply(culipx_factor f, int stage, const void *d_b, void *d_x);
+
+/* ------------------------------------------------------------------------ */
+/* CSR operator (CSRMatrixSPMV<T>).  Device arrays are borrowed, not copied:
+ * they must outlive the operator, as the reference's raw pointer does. */
+int culipx_csr_create(culipx_handle h, int m, int n, long long nnz, const int *d_rowptr,
+                      const int *d_colidx, const void *d_val, int precision,
+                      int explicit_transpose, culipx_csr *out);
+int culipx_csr_destroy(culipx_csr A);
+/* y = alpha op(A) x + beta y (beta == 0: y is not read) */
+int culipx_spmv(culipx_csr A, const void *d_x, void *d_y, double alpha, double beta, int transpose);
+
+/* ------------------------------------------------------------------------ */
+/* SQMR with the factor as split preconditioner M = (P U') D (U P')
+ * (SQMR<double>::solve, sqmr.impl.cuh:109-355).  A must be FP64; M may be
+ * FP64, FP32 (mixed precision: applies in FP32, recurrence in FP64) or NULL.
+ * x is overwritten.  residual = the quasi-residual gamma / ||M_L^-1 b||, as
+ * the reference returns; iterations as the reference counts them. */
+int culipx_sqmr_solve(culipx_handle h, culipx_csr A, culipx_factor M, const double *d_b,
+                      double *d_x, double tol, int max_it, double *residual, int *iterations);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CULIPX_H */
