@@ -245,6 +245,12 @@ CULIPX_API int culipx_factor_export(culipx_factor f, int* h_blk_nnz, long long* 
 CULIPX_API int culipx_factor_stats(culipx_factor f, double* ms, int* launches)
 {
     if (!f) return fail(CULIPX_INVALID_ARG, "null factor");
+    if (!f->computed) return fail(CULIPX_INVALID_ARG, "culipx_factor_stats: factor not computed");
+    culipx_handle_t* h = f->pat->handle;
+    CULIPX_TRY(use_device(h));
+    // the last factorization's device time (its events bracket the launches)
+    CULIPX_CUDA(cudaEventSynchronize(h->ev_stop));
+    CULIPX_CUDA(cudaEventElapsedTime(&f->last_ms, h->ev_start, h->ev_stop));
     if (ms) *ms = f->last_ms;
     if (launches) *launches = f->last_launches;
     return CULIPX_OK;

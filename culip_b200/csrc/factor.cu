@@ -5,30 +5,30 @@
 // the execution model is this library's own:
 //
 //  * one warp per block, the block as a 32x32 tile in shared memory with a
-//    padded stride, up to four warps (blocks) per CTA;
-//  * Schur updates A_ij -= U_ki' D_k U_kj are enumerated sparsely: for every
-//    output row a the warp builds row a of U_ki' D_k with the reference's
-//    tridiagonal formula, ballots its non-zeros and accumulates only those
-//    terms, in ascending inner index, with explicit fma.  A term with a zero
-//    factor changes an fma-accumulated sum by at most the sign of a zero, so
-//    the result equals the reference's dense 32x32x32 product bit for bit
-//    (up to signed zeros).  Each update's product is rounded on its own and
-//    then subtracted, as the reference does (d_apply_left_right_update,
-//    :415-456);
+//    padded stride, four warps (blocks) per CTA;
+//  * Schur updates A_ij -= U_ki' D_k U_kj are enumerated sparsely
+//    (schur_update, pivot_tile.cuh): only non-zero terms are accumulated, in
+//    ascending inner index, with explicit fma, which equals the reference's
+//    dense 32x32x32 product bit for bit up to signed zeros; each update's
+//    product is rounded on its own and then subtracted, as the reference does;
 //  * Bunch-Kaufman / Rook / static 1x1-2x2 pivoting runs warp-parallel on the
-//    tile with lowest-index tie breaking, which is what the reference's
-//    shfl_down argmax tree produces (:761-781);
-//  * blocks are written straight to their final storage, sparse entries in
-//    row-major order, dropping |v| <= NZ_EPS (d_save_block, :85-173);
-//    there is no in-flight 32x32 staging buffer per level.
-//
-// All files are compiled with --fmad=false: every fused multiply-add is the
-// explicit fma_rn written here.
+//    tile;
+//  * blocks are written straight to their final storage (sparse entries in
+//    row-major order, |v| <= NZ_EPS dropped); there is no per-level in-flight
+//    32x32 staging buffer.  Blocks that need the reference's dual dropping
+//    (k_apply_block_dual_dropping, :1866-2074) -- more non-zeros than their
+//    fill cap, or any sparse block when a relative threshold is set -- are
+//    deferred: they are recomputed after a one-CTA scan has granted leftover
+//    slots in level-list order (the reference's CTAs race on one counter;
+//    this is the serialization by block order) and relocated to an arena
+//    when granted extra slots.
 #include "factor.h"
 #include "kernels_common.cuh"
 #include "block_io.cuh"
+#include "pivot_tile.cuh"
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -39,256 +39,34 @@ namespace {
 
 constexpr int kWarps = 4;  // blocks per CTA
 
-enum StateSlot { kStErr = 0, kStLeftover = 1 };
-enum ErrBits { kErrOverflow = 1 };
+// device scalars in Factor::state
+enum StateSlot { kStErr = 0, kStLeftover = 1, kStArena = 2, kStDeferred = 3, kStLevelAcc = 4 };
+enum ErrBits { kErrLeftoverNegative = 1 };
 
-template <class T>
-__device__ __forceinline__ T bk_alpha() { return (T)((1.0f + sqrtf(17.0f)) / 8.0f); }
-
-// Out[a][b] -= sum_r R[r][b] * (Q' D_k)[a][r] for a in colmask(Q), lanes b < rh.
-// Q: U_ki (bw x .), R: U_kj (bw x rh); D_k from tri at the rows of block k.
-// d_multiply_block_by_block_diagonal (:372-411) + d_apply_left_right_update.
-template <class T>
-__device__ void schur_update(T* out, const T* Q, const T* R, unsigned colmask, int bw, int rh,
-                             const T* tri_k)
-{
-    const int lane = lane_id();
-    T sup = T(0), dia = T(0), sub = T(0);
-    if (lane < bw) {
-        sup = tri_k[3 * lane];
-        dia = tri_k[3 * lane + 1];
-        sub = tri_k[3 * lane + 2];
-    }
-    while (colmask) {
-        const int a = __ffs(colmask) - 1;
-        colmask &= colmask - 1;
-        T lv = T(0);
-        if (lane < bw) {
-            const T left = (lane > 0) ? Q[(lane - 1) * kTileStride + a] : T(0);
-            const T mid = Q[lane * kTileStride + a];
-            const T right = (lane < 31) ? Q[(lane + 1) * kTileStride + a] : T(0);
-            lv = fma_rn(sub, right, fma_rn(sup, left, dia * mid));
-        }
-        unsigned m = __ballot_sync(0xffffffffu, lv != T(0));
-        T acc = T(0);
-        while (m) {
-            const int r = __ffs(m) - 1;
-            m &= m - 1;
-            const T la = shfl(lv, r);
-            acc = fma_rn(R[r * kTileStride + lane], la, acc);
-        }
-        if (lane < rh) out[a * kTileStride + lane] -= acc;
-    }
-    __syncwarp();
-}
-
-// ---- dense pivot-block factorization (d_factor_pivot_factorize, :956-1083) ----
-
-template <class T>
-__device__ void pivot_swap(T* Tt, int* perm, int p1, int p2, int len)
-{
-    const int l = lane_id();
-    int ia, ib;
-    if (l < p1) { ia = l * kTileStride + p1; ib = l * kTileStride + p2; }
-    else if (l == p1) { ia = p1 * kTileStride + p1; ib = p2 * kTileStride + p2; }
-    else if (l < p2) { ia = p1 * kTileStride + l; ib = l * kTileStride + p2; }
-    else if (l == p2) { ia = p1 * kTileStride + p2; ib = ia; }
-    else { ia = p1 * kTileStride + l; ib = p2 * kTileStride + l; }
-    T va = T(0), vb = T(0);
-    if (l < len) { va = Tt[ia]; vb = Tt[ib]; }
-    __syncwarp();
-    if (l < len) Tt[ia] = vb;
-    __syncwarp();
-    if (l < len) Tt[ib] = va;
-    if (l == 0) { const int t = perm[p1]; perm[p1] = perm[p2]; perm[p2] = t; }
-    __syncwarp();
-}
-
-// argmax of v over lanes, ties to the lowest index (value, index) = (v, i)
-template <class T>
-__device__ __forceinline__ void warp_argmax(T& v, int& i)
-{
-    for (int o = 16; o > 0; o >>= 1) {
-        const T ov = __shfl_xor_sync(0xffffffffu, v, o);
-        const int oi = __shfl_xor_sync(0xffffffffu, i, o);
-        if (ov > v || (ov == v && oi < i)) { v = ov; i = oi; }
-    }
-}
-
-template <class T>
-__device__ __forceinline__ T warp_max(T v)
-{
-    for (int o = 16; o > 0; o >>= 1) {
-        const T ov = __shfl_xor_sync(0xffffffffu, v, o);
-        v = (ov > v) ? ov : v;
-    }
-    return v;
-}
-
-template <class T>
-__device__ __forceinline__ T upper_abs(const T* Tt, int a, int b)
-{
-    return (a < b) ? fabs(Tt[a * kTileStride + b]) : fabs(Tt[b * kTileStride + a]);
-}
-
-template <class T>
-__device__ void select_bk(const T* Tt, int p, int len, int& order, int& p0, int& p1)
-{
-    const int l = lane_id();
-    const T alpha = bk_alpha<T>();
-    order = 1;
-    p0 = p;
-    int r = (l > p + 1) ? l : p + 1;
-    T w1 = (l > p && l < len) ? fabs(Tt[p * kTileStride + l]) : T(0);
-    warp_argmax(w1, r);
-    if (!(w1 > T(0))) return;
-    const T app = fabs(Tt[p * kTileStride + p]);
-    if (app >= alpha * w1) return;
-    T wr = (l < p || l == r || l >= len) ? T(0) : upper_abs(Tt, l, r);
-    wr = warp_max(wr);
-    if (app * wr >= alpha * w1 * w1) return;
-    if (fabs(Tt[r * kTileStride + r]) >= alpha * wr) { p0 = r; return; }
-    order = 2;
-    p0 = p;
-    p1 = r;
-}
-
-template <class T>
-__device__ void select_rook(const T* Tt, int p, int len, int& order, int& p0, int& p1)
-{
-    const int l = lane_id();
-    const T alpha = bk_alpha<T>();
-    order = 1;
-    p0 = p;
-    int r = (l > p + 1) ? l : p + 1;
-    T wi = (l > p && l < len) ? fabs(Tt[p * kTileStride + l]) : T(0);
-    warp_argmax(wi, r);
-    if (!(wi > T(0))) return;
-    int i = p;
-    if (fabs(Tt[p * kTileStride + p]) >= alpha * wi) return;
-    for (int guard = 0; guard < 64; ++guard) {  // values strictly grow: at most len rounds
-        int q = (l > p) ? l : p;
-        T wr = (l >= p && l < len && l != r) ? upper_abs(Tt, l, r) : T(0);
-        warp_argmax(wr, q);
-        if (fabs(Tt[r * kTileStride + r]) >= alpha * wr) { p0 = r; return; }
-        if (wi == wr) { order = 2; p0 = i; p1 = r; return; }
-        i = r;
-        r = q;
-        wi = wr;
-    }
-    p0 = p;  // unreachable for finite values
-}
-
-template <class T>
-__device__ void step_1x1(T* Tt, T* D, int row, int len)
-{
-    const int l = lane_id();
-    T d11 = Tt[row * kTileStride + row];
-    const bool modified = fabs(d11) < 1e-8;
-    if (modified) d11 = T(1e-6);
-    const T a = (l < row) ? T(0) : Tt[row * kTileStride + l];
-    const T u = a / d11;
-    __syncwarp();
-    Tt[row * kTileStride + l] = u;
-    const T ru = u * d11;
-    for (int i = row + 1; i < len; ++i) {
-        const T lv = shfl(ru, i);
-        if (l < len) Tt[i * kTileStride + l] = fma_rn(-lv, u, Tt[i * kTileStride + l]);
-    }
-    __syncwarp();
-    if (modified && l == 0) Tt[row * kTileStride + row] = T(1);
-    if (l < 3) D[3 * row + l] = (l != 1) ? T(0) : d11;
-    __syncwarp();
-}
-
-template <class T>
-__device__ void step_2x2(T* Tt, T* D, int row, int len)
-{
-    const int l = lane_id();
-    T d11 = Tt[row * kTileStride + row];
-    const T d12 = Tt[row * kTileStride + row + 1];
-    T d22 = Tt[(row + 1) * kTileStride + row + 1];
-    const bool modified = fabs(fma_rn(d11, d22, -(d12 * d12))) < 1e-8;
-    if (modified) { d11 = T(1e-6); d22 = T(1e-6); }
-    const T a1 = (l < row) ? T(0) : Tt[row * kTileStride + l];
-    const T a2 = (l < row) ? T(0) : ((l == row) ? d12 : Tt[(row + 1) * kTileStride + l]);
-    const T gr = sqrt(fma_rn(d11, d11, d12 * d12));
-    const T gc = d11 / gr, gs = d12 / gr;
-    T x1 = fma_rn(gc, a1, gs * a2);
-    T x2 = fma_rn(-gs, a1, gc * a2);
-    const T td11 = fma_rn(gc, d11, gs * d12);
-    const T td12 = fma_rn(gc, d12, gs * d22);
-    const T td22 = fma_rn(-gs, d12, gc * d22);
-    x2 = x2 / td22;
-    x1 = fma_rn(-td12, x2, x1) / td11;
-    __syncwarp();
-    Tt[row * kTileStride + l] = (l < row) ? T(0) : x1;
-    Tt[(row + 1) * kTileStride + l] = (l < row) ? T(0) : x2;
-    const T r1 = fma_rn(x1, d11, x2 * d12);
-    const T r2 = fma_rn(x1, d12, x2 * d22);
-    for (int i = row + 2; i < len; ++i) {
-        const T l1 = shfl(r1, i), l2 = shfl(r2, i);
-        Tt[i * kTileStride + l] -= fma_rn(l1, x1, l2 * x2);
-    }
-    __syncwarp();
-    if (modified && l == 0) {
-        Tt[row * kTileStride + row] = T(1);
-        Tt[row * kTileStride + row + 1] = T(0);
-        Tt[(row + 1) * kTileStride + row + 1] = T(1);
-    }
-    if (l < 3) {
-        D[3 * row + l] = (l == 0) ? T(0) : ((l == 1) ? d11 : d12);
-        D[3 * (row + 1) + l] = (l == 2) ? T(0) : ((l == 0) ? d12 : d22);
-    }
-    __syncwarp();
-}
-
-template <class T>
-__device__ void factorize_tile(T* Tt, int len, int* is_piv, T* D, int* perm, int method)
-{
-    const bool use_piv = method != CULIPX_PIV_STATIC;
-    int p = 0;
-    while (p < len) {
-        int order = 1, p0 = p, p1 = p + 1;
-        if (p < len - 1 && method == CULIPX_PIV_BK) select_bk(Tt, p, len, order, p0, p1);
-        else if (p < len - 1 && method == CULIPX_PIV_ROOK) select_rook(Tt, p, len, order, p0, p1);
-        else order = (p < len - 1 && !is_piv[p + 1]) ? 2 : 1;
-        __syncwarp();
-        if (order == 1) {
-            if (use_piv && p != p0) pivot_swap(Tt, perm, p, p0, len);
-            step_1x1(Tt, D, p, len);
-            if (use_piv && lane_id() == 0) is_piv[p] = 1;
-        } else {
-            if (use_piv) {
-                if (p0 != p) pivot_swap(Tt, perm, p, p0, len);
-                pivot_swap(Tt, perm, p + 1, p1, len);
-            }
-            step_2x2(Tt, D, p, len);
-            if (use_piv && lane_id() == 0) { is_piv[p] = 1; is_piv[p + 1] = 0; }
-        }
-        __syncwarp();
-        p += order;
-    }
-}
-
-// ------------------------------- kernels ----------------------------------
+enum OffdiagMode { kFirst = 0, kCount = 1, kWrite = 2 };
 
 struct FactorArgs {
     const DevBlock* desc;
     const int* bs;
+    const int* cs_off;
     const int* csc_off;
     const int* csc_blk;
     const int* fmt;
-    const int* lb;        // factor-order block list
+    const int* lb;  // factor-order block list
     const int* lvl_rows;
+    const int* row_offdiag_start;
+    const int* nnz_init;  // A's entries per sparse block (pattern)
     long long* boff;
     int* nnz;
     int* cap;
+    int* got_extra;
     int* idx;
     int* is_piv;
     int* perm;
     int* rowflags;
     long long* state;
+    int* deferred;
+    long long val_slots;  // first arena slot
 };
 
 template <class T>
@@ -309,22 +87,26 @@ __global__ void k_init_blocks(int cnz, const DevBlock* desc, long long* boff, in
     }
 }
 
-__global__ void k_init_rows(int n, int* perm, int* is_piv, const int* h_is_piv_dev, int use_given)
+__global__ void k_init_rows(int n, int* perm, int* is_piv, int use_given)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         perm[i] = i;
-        is_piv[i] = use_given ? h_is_piv_dev[i] : 1;
+        if (!use_given) is_piv[i] = 1;
     }
 }
 
 // Step 1 of a level: Schur updates + factorization of the pivot blocks
-// (k_factor_pivot_blocks, :1146-1283).
+// (k_factor_pivot_blocks, :1146-1283), row norms of the pivot rows (:1259-1269).
 template <class T>
-__global__ void __launch_bounds__(32 * kWarps) k_pivot_blocks(FactorArgs a, T* val, T* tri, int lb0,
+__global__ void __launch_bounds__(32 * kWarps) k_pivot_blocks(FactorArgs a, T* val, T* tri, T* row_norm, int lb0,
                                                               int npiv, int method)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* smem = reinterpret_cast<T*>(smem_raw);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        a.state[kStDeferred] = 0;
+        a.state[kStLevelAcc] = 0;
+    }
     const int warp = threadIdx.x >> 5;
     const int t = blockIdx.x * kWarps + warp;
     if (t >= npiv) return;
@@ -351,6 +133,12 @@ __global__ void __launch_bounds__(32 * kWarps) k_pivot_blocks(FactorArgs a, T* v
     __syncwarp();
     factorize_tile(Tt, len, a.is_piv + from, tri + 3 * (size_t)from, a.perm + from, method);
 
+    if (row_norm) {
+        T rs = T(0);
+        for (int j = 0; j < len; ++j) rs = fma_rn(Tt[lane * kTileStride + j], Tt[lane * kTileStride + j], rs);
+        if (lane < len) row_norm[from + lane] = rs;
+    }
+
     // write the dense pivot tile and the row flags
     const long long off = a.boff[b];
     bool ident = true;
@@ -368,34 +156,26 @@ __global__ void __launch_bounds__(32 * kWarps) k_pivot_blocks(FactorArgs a, T* v
     if (lane == 0) a.rowflags[I] = (ident ? 1 : 0) | (two ? 2 : 0);
 }
 
-// Step 2 of a level: fan-in updates, row permutation, D^-1 U'^-1 scaling and
-// compressed write of the off-diagonal blocks
-// (k_update_scale_offdiagonal_blocks :1628-1803 + k_apply_block_dual_dropping
-// :1866-2074 for the threshold-free case).
+// Off-diagonal block (I, J) up to its final values in Tt: fan-in updates over
+// the block columns I and J, the pivot block's row permutation and the left
+// solve with D^-1 U'^-1 (k_update_scale_offdiagonal_blocks, :1628-1778, with
+// d_left_solve_with_D_Ut :1489-1570).  Q and R must be zero on entry and are
+// zero on exit.
 template <class T>
-__global__ void __launch_bounds__(32 * kWarps) k_offdiag_blocks(FactorArgs a, T* val, const T* tri,
-                                                                int lb_first, int noff, int pivoting)
+__device__ void offdiag_tile(const FactorArgs& a, const T* val, const T* tri, int b, T* Tt, T* Q, T* R, int pivoting)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    T* smem = reinterpret_cast<T*>(smem_raw);
-    const int warp = threadIdx.x >> 5;
-    const int t = blockIdx.x * kWarps + warp;
-    if (t >= noff) return;
     const int lane = lane_id();
-    T* Tt = smem + (size_t)warp * 3 * kTileElems;
-    T* Q = Tt + kTileElems;
-    T* R = Q + kTileElems;
-
-    const int b = a.lb[lb_first + t];
     const DevBlock d = a.desc[b];
     const int I = d.row, J = d.col;
     const int from = a.bs[I], h = a.bs[I + 1] - from;
     const int w = a.bs[J + 1] - a.bs[J];
 
-    for (int e = lane; e < kTileElems; e += 32) { Q[e] = T(0); R[e] = T(0); }
-    load_block(Tt, b, a.desc, a.bs, a.boff, a.nnz, a.fmt, val, a.idx, true);
+    // the block's own input (A's entries) stays at its pattern slot until the
+    // block is written; a deferred block may already be relocated and its nnz
+    // hold the survivor count
+    const bool dense = a.fmt[b] == 1;
+    load_block_at(Tt, h, w, dense, (long long)d.val_off, dense ? 0 : a.nnz_init[b], val, a.idx, true);
 
-    // merge-walk the block columns I and J above the diagonal
     int ip = a.csc_off[I], jp = a.csc_off[J];
     const int ie = a.csc_off[I + 1] - 1, je = a.csc_off[J + 1] - 1;
     while (ip < ie && jp < je) {
@@ -414,7 +194,6 @@ __global__ void __launch_bounds__(32 * kWarps) k_offdiag_blocks(FactorArgs a, T*
     }
 
     if (pivoting) {
-        // rows of the block follow the pivot block's local permutation
         for (int i = 0; i < h; ++i) R[i * kTileStride + lane] = Tt[i * kTileStride + lane];
         __syncwarp();
         for (int i = 0; i < h; ++i) {
@@ -426,7 +205,6 @@ __global__ void __launch_bounds__(32 * kWarps) k_offdiag_blocks(FactorArgs a, T*
         __syncwarp();
     }
 
-    // left solve with D^-1 U'^-1 (d_left_solve_with_D_Ut, :1489-1570)
     const int flags = a.rowflags[I];
     const bool ident = flags & 1;
     const int pb = a.csc_blk[a.csc_off[I + 1] - 1];
@@ -435,14 +213,14 @@ __global__ void __launch_bounds__(32 * kWarps) k_offdiag_blocks(FactorArgs a, T*
         for (int i = 0; i < h; ++i) Q[i * kTileStride + lane] = val[poff + (long long)i * h + lane];
     __syncwarp();
     unsigned colmask = 0;
-    for (int i = 0; i < h; ++i) colmask |= __ballot_sync(0xffffffffu, lane < w && Tt[i * kTileStride + lane] != T(0));
+    for (int i = 0; i < h; ++i)
+        colmask |= __ballot_sync(0xffffffffu, lane < w && Tt[i * kTileStride + lane] != T(0));
     const T* D = tri + 3 * (size_t)from;
     const int* ip_row = a.is_piv + from;
     const T d11 = (lane < h) ? D[3 * lane + 1] : T(0);
     const T d12 = (lane < h) ? D[3 * lane + 2] : T(0);
     T d22 = shfl(d11, (lane < 31) ? lane + 1 : 31);
     if (lane == h) d22 = T(0);
-    if (lane == 31 && h == 32) d22 = d11;
     const bool piv1 = lane < h && ip_row[lane];
     const bool piv2 = (lane + 1) < h && !ip_row[lane + 1];
     const T gr = sqrt(fma_rn(d11, d11, d12 * d12));
@@ -471,35 +249,283 @@ __global__ void __launch_bounds__(32 * kWarps) k_offdiag_blocks(FactorArgs a, T*
         if (piv2) Tt[(lane + 1) * kTileStride + j] = x2;
         __syncwarp();
     }
+    if (!ident) {
+        if (lane < h)
+            for (int i = 0; i < h; ++i) Q[i * kTileStride + lane] = T(0);
+        __syncwarp();
+    }
+}
 
-    // compressed write (NZ_EPS dropping) or dense copy
-    const long long off = a.boff[b];
-    if (a.fmt[b] == 1) {
-        if (lane < w)
-            for (int i = 0; i < h; ++i) val[off + (long long)i * w + lane] = Tt[i * kTileStride + lane];
-        if (lane == 0) a.nnz[b] = 0;
-        return;
-    }
+// threshold dropping (:1923-1945): zero |v| < threshold * ||row|| (non-zeros
+// only) and count the survivors with |v| > NZ_EPS
+template <class T>
+__device__ int drop_and_count(T* Tt, int h, int w, const T* row_norm, int from, T threshold)
+{
+    const int lane = lane_id();
     int total = 0;
-    for (int i = 0; i < h; ++i)
-        total += __popc(__ballot_sync(0xffffffffu, lane < w && fabs(Tt[i * kTileStride + lane]) > T(kNzEps)));
-    if (total > a.cap[b]) {
-        if (lane == 0) atomicOr(reinterpret_cast<unsigned long long*>(&a.state[kStErr]), (unsigned long long)kErrOverflow);
-        return;
+    for (int i = 0; i < h; ++i) {
+        T v = (lane < w) ? Tt[i * kTileStride + lane] : T(0);
+        bool drop = false;
+        if (row_norm) {
+            const T nrm = (T)sqrtf((float)row_norm[from + i]);
+            drop = fabs(v) < threshold * nrm;
+            if (drop && fabs(v) > T(kNzEps) && lane < w) Tt[i * kTileStride + lane] = T(0);
+        }
+        total += __popc(__ballot_sync(0xffffffffu, lane < w && !drop && fabs(v) > T(kNzEps)));
     }
+    __syncwarp();
+    return total;
+}
+
+// row-major compressed write of the entries with |v| > NZ_EPS (d_save_block)
+// or, with keep != nullptr, of the tile positions flagged in keep
+template <class T>
+__device__ void write_sparse(const T* Tt, int h, int w, T* val, int* idx, long long off, const unsigned* keep)
+{
+    const int lane = lane_id();
     int o = 0;
     for (int i = 0; i < h; ++i) {
         const T v = (lane < w) ? Tt[i * kTileStride + lane] : T(0);
-        const bool nz = lane < w && fabs(v) > T(kNzEps);
+        const bool nz = lane < w && (keep ? ((keep[i] >> lane) & 1u) : (fabs(v) > T(kNzEps)));
         const unsigned m = __ballot_sync(0xffffffffu, nz);
         if (nz) {
             const int pos = o + __popc(m & ((1u << lane) - 1u));
             val[off + pos] = v;
-            a.idx[off + pos] = i * w + lane;
+            idx[off + pos] = i * w + lane;
         }
         o += __popc(m);
     }
-    if (lane == 0) a.nnz[b] = total;
+}
+
+// keep the `k` largest |v| (ties to the lower tile index, as CUB's stable
+// descending radix sort in :2016-2061), flagged per row in keep[32]; a
+// warp-level bitonic sort of (|v|, index) in the scratch tiles K, X
+template <class T>
+__device__ void select_largest(const T* Tt, int h, int w, int k, T* K, int* X, unsigned* keep)
+{
+    const int lane = lane_id();
+    for (int e = lane; e < 1024; e += 32) {
+        const int r = e >> 5, c = e & 31;
+        K[e] = (r < h && c < w) ? fabs(Tt[r * kTileStride + c]) : T(0);
+        X[e] = e;
+    }
+    __syncwarp();
+    // sort descending by key, ascending by index: "a before b" when ka > kb or (ka == kb and ia < ib)
+    for (int size = 2; size <= 1024; size <<= 1)
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int pidx = lane; pidx < 512; pidx += 32) {
+                const int lo = 2 * pidx - (pidx & (stride - 1));
+                const int hi = lo + stride;
+                const bool up = ((lo & size) == 0);
+                const T ka = K[lo], kb = K[hi];
+                const int ia = X[lo], ib = X[hi];
+                const bool a_first = (ka > kb) || (ka == kb && ia < ib);
+                if (a_first != up) {
+                    K[lo] = kb; K[hi] = ka;
+                    X[lo] = ib; X[hi] = ia;
+                }
+            }
+            __syncwarp();
+        }
+    if (lane < 32) keep[lane] = 0;
+    __syncwarp();
+    for (int e = lane; e < k; e += 32) {
+        const int pos = X[e];
+        atomicOr(&keep[pos >> 5], 1u << (pos & 31));
+    }
+    __syncwarp();
+}
+
+// Step 2: off-diagonal blocks.  kFirst: every block of the level; kCount /
+// kWrite: the deferred list.
+template <class T, int MODE>
+__global__ void __launch_bounds__(32 * kWarps) k_offdiag(FactorArgs a, T* val, const T* tri, int lb_first, int noff,
+                                                         int pivoting, T* row_norm, T* norm_part, T threshold)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* smem = reinterpret_cast<T*>(smem_raw);
+    const int warp = threadIdx.x >> 5;
+    const int lane = lane_id();
+    T* Tt = smem + (size_t)warp * 3 * kTileElems;
+    T* Q = Tt + kTileElems;
+    T* R = Q + kTileElems;
+    __shared__ unsigned keep_all[kWarps][32];
+
+    const int count = (MODE == kFirst) ? noff : (int)a.state[kStDeferred];
+    const int nw = gridDim.x * kWarps;
+    for (int t = blockIdx.x * kWarps + warp; t < count; t += nw) {
+        const int pos = (MODE == kFirst) ? t : a.deferred[t];  // position in the level's off-diagonal list
+        const int b = a.lb[lb_first + pos];
+        const DevBlock d = a.desc[b];
+        const int from = a.bs[d.row], h = a.bs[d.row + 1] - from;
+        const int w = a.bs[d.col + 1] - a.bs[d.col];
+        const bool sparse = a.fmt[b] == 0;
+        for (int e = lane; e < kTileElems; e += 32) { Q[e] = T(0); R[e] = T(0); }
+        __syncwarp();
+        offdiag_tile(a, val, tri, b, Tt, Q, R, pivoting);
+        const long long off = a.boff[b];
+
+        if (MODE == kFirst) {
+            if (norm_part) {
+                // row norms are needed before any dropping: record this block's
+                // row sums (:1783-1794) and defer sparse blocks
+                T rs = T(0);
+                for (int j = 0; j < w; ++j) rs = fma_rn(Tt[lane * kTileStride + j], Tt[lane * kTileStride + j], rs);
+                if (lane < h) norm_part[(size_t)pos * 32 + lane] = rs;
+            }
+            if (!sparse) {
+                if (lane < w)
+                    for (int i = 0; i < h; ++i) val[off + (long long)i * w + lane] = Tt[i * kTileStride + lane];
+                if (lane == 0) a.nnz[b] = 0;
+                continue;
+            }
+            if (norm_part) {
+                if (lane == 0) {
+                    const int slot = (int)atomicAdd(reinterpret_cast<unsigned long long*>(&a.state[kStDeferred]), 1ull);
+                    a.deferred[slot] = pos;
+                }
+                continue;
+            }
+            const int total = drop_and_count<T>(Tt, h, w, nullptr, from, T(0));
+            const int cp = a.cap[b];
+            if (total <= cp) {
+                write_sparse(Tt, h, w, val, a.idx, off, nullptr);
+                if (lane == 0) {
+                    a.nnz[b] = total;
+                    atomicAdd(reinterpret_cast<unsigned long long*>(&a.state[kStLevelAcc]),
+                              (unsigned long long)(long long)(cp - total));
+                }
+            } else if (lane == 0) {
+                a.nnz[b] = total;  // the count, for the grant scan; entries come in kWrite
+                const int slot = (int)atomicAdd(reinterpret_cast<unsigned long long*>(&a.state[kStDeferred]), 1ull);
+                a.deferred[slot] = pos;
+            }
+            continue;
+        }
+        const int total = drop_and_count<T>(Tt, h, w, row_norm, from, threshold);
+        if (MODE == kCount) {
+            if (lane == 0) a.nnz[b] = total;
+            continue;
+        }
+        const int cp = a.cap[b];  // after grants
+        if (total <= cp) {
+            write_sparse(Tt, h, w, val, a.idx, off, nullptr);
+            if (lane == 0) a.nnz[b] = total;
+        } else {
+            unsigned* keep = keep_all[warp];
+            select_largest(Tt, h, w, cp, Q, reinterpret_cast<int*>(R), keep);
+            write_sparse(Tt, h, w, val, a.idx, off, keep);
+            if (lane == 0) a.nnz[b] = cp;
+            for (int e = lane; e < kTileElems; e += 32) { Q[e] = T(0); R[e] = T(0); }
+            __syncwarp();
+        }
+    }
+}
+
+// row norms: pivot row sums + the off-diagonal row sums in level-list order
+template <class T>
+__global__ void k_row_norms(FactorArgs a, T* row_norm, const T* norm_part, int lvl0, int nrows)
+{
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (warp >= nrows) return;
+    const int lane = lane_id();
+    const int I = a.lvl_rows[lvl0 + warp];
+    const int from = a.bs[I], h = a.bs[I + 1] - from;
+    const int s = a.row_offdiag_start[lvl0 + warp];
+    const int cnt = a.cs_off[I + 1] - a.cs_off[I] - 1;
+    if (lane >= h) return;
+    T acc = row_norm[from + lane];
+    for (int j = 0; j < cnt; ++j) acc = acc + norm_part[(size_t)(s + j) * 32 + lane];
+    row_norm[from + lane] = acc;
+}
+
+// Serialized dual-dropping bookkeeping of one level in block order
+// (:1949-2008): grants from the leftover pool, capacity updates and arena
+// relocation of the blocks granted extra slots.  One CTA; the leftover
+// recurrence x -> max(x + a, b) composes, so per-thread chunks are composed,
+// scanned, then replayed.
+constexpr long long kNeg = LLONG_MIN / 4;
+constexpr int kScanT = 1024;
+
+__global__ void __launch_bounds__(kScanT) k_level_scan(FactorArgs a, int lb_first, int noff)
+{
+    __shared__ long long fa[kScanT], fb[kScanT], rel[kScanT];
+    const int tid = threadIdx.x;
+    if (a.state[kStDeferred] == 0) {
+        if (tid == 0) a.state[kStLeftover] += a.state[kStLevelAcc];
+        return;
+    }
+    const int chunk = (noff + kScanT - 1) / kScanT;
+    const int t0 = min(noff, tid * chunk), t1 = min(noff, t0 + chunk);
+    long long A = 0, B = kNeg;
+    for (int t = t0; t < t1; ++t) {
+        const int b = a.lb[lb_first + t];
+        if (a.fmt[b] != 0) continue;
+        const long long c = a.nnz[b], m = a.cap[b];
+        const long long ea = (c > m) ? -(c - m) : (m - c);
+        const long long eb = (c > m) ? 0 : kNeg;
+        A = A + ea;
+        B = max(B + ea, eb);
+        B = max(B, kNeg);
+    }
+    fa[tid] = A;
+    fb[tid] = B;
+    __syncthreads();
+    if (tid == 0) {
+        // exclusive scan of the compositions: prefix_t = f_{t-1} o ... o f_0
+        long long pa = 0, pb = kNeg;
+        for (int k = 0; k < kScanT; ++k) {
+            const long long ca = fa[k], cb = fb[k];
+            fa[k] = pa;
+            fb[k] = pb;
+            const long long na = pa + ca;
+            const long long nb = max(max(pb + ca, cb), kNeg);
+            pa = na;
+            pb = nb;
+        }
+    }
+    __syncthreads();
+    const long long x0 = a.state[kStLeftover];
+    long long x = max(x0 + fa[tid], fb[tid]);
+    long long my_rel = 0;
+    for (int t = t0; t < t1; ++t) {
+        const int b = a.lb[lb_first + t];
+        if (a.fmt[b] != 0) continue;
+        const long long c = a.nnz[b], m = a.cap[b];
+        if (c > m) {
+            const long long req = c - m;
+            long long g = min(req, x);
+            if (g < 0) g = 0;
+            x -= g;
+            a.got_extra[b] = (int)g;
+            a.cap[b] = (int)(m + g);
+            if (g > 0) my_rel += m + g;
+        } else {
+            x += m - c;
+        }
+    }
+    rel[tid] = my_rel;
+    __syncthreads();
+    if (tid == kScanT - 1) a.state[kStLeftover] = x;  // the last chunk ends the level
+    if (tid == 0) {
+        long long s = 0;
+        for (int k = 0; k < kScanT; ++k) {
+            const long long v = rel[k];
+            rel[k] = s;
+            s += v;
+        }
+    }
+    __syncthreads();
+    const long long base = a.val_slots + a.state[kStArena];
+    long long o = base + rel[tid];
+    for (int t = t0; t < t1; ++t) {
+        const int b = a.lb[lb_first + t];
+        if (a.fmt[b] != 0 || a.got_extra[b] == 0) continue;
+        a.boff[b] = o;
+        o += a.cap[b];
+    }
+    __syncthreads();
+    if (tid == kScanT - 1) a.state[kStArena] = o - a.val_slots;
 }
 
 // Step 3: apply each pivot block's local permutation to the columns of the
@@ -514,8 +540,7 @@ __global__ void k_pivot_columns(FactorArgs a, T* val, int lvl0, int nrows)
     const int I = a.lvl_rows[lvl0 + t];
     const int from = a.bs[I], bw = a.bs[I + 1] - from;
     const int lp = (lane < bw) ? a.perm[from + lane] - from : lane;
-    // inverse permutation via ballots: inv[c] = l with lp[l] == c
-    int inv = lane;
+    int inv = lane;  // inv[c] = l with lp[l] == c
     for (int l = 0; l < bw; ++l) {
         const int v = shfl(lp, l);
         if (v == lane) inv = l;
@@ -544,24 +569,16 @@ __global__ void k_pivot_columns(FactorArgs a, T* val, int lvl0, int nrows)
     }
 }
 
-}  // namespace
-}  // namespace culipx
-
-namespace culipx {
-
-int build_sweeps(Factor* f, cudaStream_t stream, int* launches);  // solve.cu
-
-namespace {
-
 template <class T>
 int set_smem_limits()
 {
     static bool done = false;
     if (done) return CULIPX_OK;
-    CULIPX_CUDA(cudaFuncSetAttribute(k_pivot_blocks<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)(kWarps * 2 * kTileElems * sizeof(T))));
-    CULIPX_CUDA(cudaFuncSetAttribute(k_offdiag_blocks<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)(kWarps * 3 * kTileElems * sizeof(T))));
+    const int s2 = (int)(kWarps * 2 * kTileElems * sizeof(T)), s3 = (int)(kWarps * 3 * kTileElems * sizeof(T));
+    CULIPX_CUDA(cudaFuncSetAttribute(k_pivot_blocks<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, s2));
+    CULIPX_CUDA(cudaFuncSetAttribute(k_offdiag<T, kFirst>, cudaFuncAttributeMaxDynamicSharedMemorySize, s3));
+    CULIPX_CUDA(cudaFuncSetAttribute(k_offdiag<T, kCount>, cudaFuncAttributeMaxDynamicSharedMemorySize, s3));
+    CULIPX_CUDA(cudaFuncSetAttribute(k_offdiag<T, kWrite>, cudaFuncAttributeMaxDynamicSharedMemorySize, s3));
     done = true;
     return CULIPX_OK;
 }
@@ -573,43 +590,68 @@ int run_levels(Factor* f, const void* d_vals, cudaStream_t s, int* launches)
     CULIPX_TRY(set_smem_limits<T>());
     T* val = f->val.as<T>();
     T* tri = f->tri.as<T>();
-    const int grid_n = 148 * 8;
-    k_scatter_values<T><<<grid_n, 256, 0, s>>>((int)p.nnz, p.d_a_dst.as<int>(),
-                                               static_cast<const T*>(d_vals), val);
+    k_scatter_values<T><<<148 * 8, 256, 0, s>>>((int)p.nnz, p.d_a_dst.as<int>(), static_cast<const T*>(d_vals), val);
     ++*launches;
     CULIPX_TRY(launch_check("k_scatter_values"));
+
+    const bool thr = f->threshold > 0.0;
+    if (thr) {
+        CULIPX_TRY(f->row_norm.alloc(p.handle, (size_t)p.n * sizeof(T)));
+        CULIPX_TRY(f->norm_part.alloc(p.handle, (size_t)std::max(p.max_level_blocks, 1) * 32 * sizeof(T)));
+    }
+    T* row_norm = thr ? f->row_norm.as<T>() : nullptr;
+    T* norm_part = thr ? f->norm_part.as<T>() : nullptr;
 
     FactorArgs a;
     a.desc = p.d_desc.as<DevBlock>();
     a.bs = p.d_bs.as<int>();
+    a.cs_off = p.d_cs_off.as<int>();
     a.csc_off = p.d_csc_off.as<int>();
     a.csc_blk = p.d_csc_blk.as<int>();
     a.fmt = p.d_fmt.as<int>();
     a.lb = p.d_lb.as<int>();
     a.lvl_rows = p.d_lvl_rows.as<int>();
+    a.row_offdiag_start = p.d_row_offdiag_start.as<int>();
+    a.nnz_init = p.d_nnz_init.as<int>();
     a.boff = f->boff.as<long long>();
     a.nnz = f->nnz.as<int>();
     a.cap = f->cap.as<int>();
+    a.got_extra = f->got_extra.as<int>();
     a.idx = f->idx.as<int>();
     a.is_piv = f->is_piv.as<int>();
     a.perm = f->perm.as<int>();
     a.rowflags = f->rowflags.as<int>();
     a.state = f->state.as<long long>();
+    a.deferred = f->deferred.as<int>();
+    a.val_slots = p.val_slots;
     const int pivoting = (f->pivot != CULIPX_PIV_STATIC);
+    const size_t s3 = kWarps * 3 * kTileElems * sizeof(T);
+    const T thv = (T)f->threshold;
     for (int L = 0; L < p.num_levels; ++L) {
         const int lb0 = p.lb_off[L];
         const int npiv = p.lvl_off[L + 1] - p.lvl_off[L];
         const int noff = p.lb_off[L + 1] - lb0 - npiv;
-        k_pivot_blocks<T><<<(npiv + kWarps - 1) / kWarps, 32 * kWarps,
-                            kWarps * 2 * kTileElems * sizeof(T), s>>>(a, val, tri, lb0, npiv, f->pivot);
+        k_pivot_blocks<T><<<(npiv + kWarps - 1) / kWarps, 32 * kWarps, kWarps * 2 * kTileElems * sizeof(T), s>>>(
+            a, val, tri, row_norm, lb0, npiv, f->pivot);
         ++*launches;
         CULIPX_TRY(launch_check("k_pivot_blocks"));
         if (noff > 0) {
-            k_offdiag_blocks<T><<<(noff + kWarps - 1) / kWarps, 32 * kWarps,
-                                  kWarps * 3 * kTileElems * sizeof(T), s>>>(a, val, tri, lb0 + npiv, noff,
-                                                                            pivoting);
+            const int lbf = lb0 + npiv;
+            k_offdiag<T, kFirst><<<(noff + kWarps - 1) / kWarps, 32 * kWarps, s3, s>>>(a, val, tri, lbf, noff, pivoting,
+                                                                                   row_norm, norm_part, thv);
             ++*launches;
-            CULIPX_TRY(launch_check("k_offdiag_blocks"));
+            const int dgrid = (std::min(noff, 148 * 16) + kWarps - 1) / kWarps;
+            if (thr) {
+                k_row_norms<T><<<(npiv * 32 + 255) / 256, 256, 0, s>>>(a, row_norm, norm_part, p.lvl_off[L], npiv);
+                k_offdiag<T, kCount><<<dgrid, 32 * kWarps, s3, s>>>(a, val, tri, lbf, noff, pivoting, row_norm,
+                                                                    nullptr, thv);
+                *launches += 2;
+            }
+            k_level_scan<<<1, kScanT, 0, s>>>(a, lbf, noff);
+            k_offdiag<T, kWrite><<<dgrid, 32 * kWarps, s3, s>>>(a, val, tri, lbf, noff, pivoting, row_norm, nullptr,
+                                                                thv);
+            *launches += 2;
+            CULIPX_TRY(launch_check("k_offdiag"));
         }
         if (pivoting) {
             k_pivot_columns<T><<<(npiv + kWarps - 1) / kWarps, 32 * kWarps, 0, s>>>(a, val, p.lvl_off[L], npiv);
@@ -622,6 +664,8 @@ int run_levels(Factor* f, const void* d_vals, cudaStream_t s, int* launches)
 
 }  // namespace
 
+int build_sweeps(Factor* f, cudaStream_t stream, int* launches);  // solve.cu
+
 int factor_create(Pattern* p, Factor** out)
 {
     if (!p || !out) return fail(CULIPX_INVALID_ARG, "culipx_factor_create: null argument");
@@ -631,10 +675,13 @@ int factor_create(Pattern* p, Factor** out)
     f->vbytes = (p->precision == CULIPX_F64) ? 8 : 4;
     culipx_handle_t* h = p->handle;
     const int cnz = p->coarse_nnz, n = p->n, cm = p->num_blocks;
-    f->val_cap = p->val_slots;
+    // pattern layout + arena for blocks relocated by dual dropping: each
+    // relocated block needs cap + grant <= 2 x its cap, summed over sparse blocks
+    f->val_cap = p->val_slots + 2 * p->sparse_slots;
     long long off_slots = 0;  // capacity of the strictly off-diagonal blocks
     for (int b = 0; b < cnz; ++b)
         if (p->blk_row[b] != p->blk_col[b]) off_slots += p->desc[b].cap;
+    off_slots += 2 * p->sparse_slots;
     int st = CULIPX_OK;
     auto al = [&](DeviceBuffer& buf, size_t bytes) {
         if (st == CULIPX_OK) st = buf.alloc(h, bytes ? bytes : 16);
@@ -650,6 +697,7 @@ int factor_create(Pattern* p, Factor** out)
     al(f->perm, (n + 32) * sizeof(int));
     al(f->rowflags, cm * sizeof(int));
     al(f->state, 16 * sizeof(long long));
+    al(f->deferred, (size_t)std::max(p->max_level_blocks, 1) * sizeof(int));
     al(f->u_off, (n + 1) * sizeof(int));
     al(f->ut_off, (n + 1) * sizeof(int));
     al(f->u_col, off_slots * sizeof(int));
@@ -669,8 +717,6 @@ int factor_compute(Factor* f, const void* d_vals, const int* h_is_piv, int pivot
     if (pivot < CULIPX_PIV_STATIC || pivot > CULIPX_PIV_ROOK)
         return fail(CULIPX_INVALID_ARG, "culipx_factor_compute: bad pivot method %d", pivot);
     if (!(threshold >= 0.0)) return fail(CULIPX_INVALID_ARG, "culipx_factor_compute: threshold < 0");
-    if (threshold != 0.0)
-        return fail(CULIPX_NOT_SUPPORTED, "culipx_factor_compute: threshold dropping > 0 is not implemented yet");
     Pattern& p = *f->pat;
     culipx_handle_t* h = p.handle;
     cudaStream_t s = h->stream;
@@ -679,45 +725,35 @@ int factor_compute(Factor* f, const void* d_vals, const int* h_is_piv, int pivot
     f->threshold = threshold;
     f->computed = false;
     int launches = 0;
+    if (h_is_piv)
+        for (int i = 0; i < n; ++i)
+            if (h_is_piv[i] != 0 && h_is_piv[i] != 1)
+                return fail(CULIPX_INVALID_ARG, "culipx_factor_compute: is_piv[%d] = %d is not 0/1", i, h_is_piv[i]);
     CULIPX_CUDA(cudaEventRecord(h->ev_start, s));
-    CULIPX_CUDA(cudaMemsetAsync(f->val.get(), 0, f->val_cap * f->vbytes, s));
+    CULIPX_CUDA(cudaMemsetAsync(f->val.get(), 0, p.val_slots * f->vbytes, s));
     CULIPX_CUDA(cudaMemcpyAsync(f->idx.get(), p.d_idx_init.get(), p.val_slots * sizeof(int),
                                 cudaMemcpyDeviceToDevice, s));
     CULIPX_CUDA(cudaMemcpyAsync(f->nnz.get(), p.d_nnz_init.get(), cnz * sizeof(int), cudaMemcpyDeviceToDevice, s));
     CULIPX_CUDA(cudaMemcpyAsync(f->cap.get(), p.d_maxnnz.get(), cnz * sizeof(int), cudaMemcpyDeviceToDevice, s));
     CULIPX_CUDA(cudaMemsetAsync(f->state.get(), 0, 16 * sizeof(long long), s));
-    CULIPX_CUDA(cudaMemsetAsync(f->tri.get(), 0, (3 * (size_t)n + 96) * f->vbytes, s));
-    if (h_is_piv) {
-        for (int i = 0; i < n; ++i)
-            if (h_is_piv[i] != 0 && h_is_piv[i] != 1)
-                return fail(CULIPX_INVALID_ARG, "culipx_factor_compute: is_piv[%d] = %d is not 0/1", i, h_is_piv[i]);
-        CULIPX_CUDA(cudaMemcpyAsync(f->is_piv.get(), h_is_piv, n * sizeof(int), cudaMemcpyHostToDevice, s));
-    }
-    k_init_rows<<<148 * 4, 256, 0, s>>>(n, f->perm.as<int>(), f->is_piv.as<int>(), f->is_piv.as<int>(),
-                                        h_is_piv ? 1 : 0);
-    ++launches;
+    if (h_is_piv) CULIPX_CUDA(cudaMemcpyAsync(f->is_piv.get(), h_is_piv, n * sizeof(int), cudaMemcpyHostToDevice, s));
+    k_init_rows<<<148 * 4, 256, 0, s>>>(n, f->perm.as<int>(), f->is_piv.as<int>(), h_is_piv ? 1 : 0);
     k_init_blocks<<<148 * 4, 256, 0, s>>>(cnz, p.d_desc.as<DevBlock>(), f->boff.as<long long>(),
                                           f->got_extra.as<int>());
-    ++launches;
+    launches += 2;
     CULIPX_TRY(launch_check("factor init"));
     if (f->precision == CULIPX_F64) CULIPX_TRY(run_levels<double>(f, d_vals, s, &launches));
     else CULIPX_TRY(run_levels<float>(f, d_vals, s, &launches));
     CULIPX_TRY(build_sweeps(f, s, &launches));
     CULIPX_CUDA(cudaEventRecord(h->ev_stop, s));
-    long long st[2] = {0, 0};
-    CULIPX_CUDA(cudaMemcpyAsync(st, f->state.get(), sizeof(st), cudaMemcpyDeviceToHost, s));
-    CULIPX_CUDA(cudaStreamSynchronize(s));
-    CULIPX_CUDA(cudaEventElapsedTime(&f->last_ms, h->ev_start, h->ev_stop));
     f->last_launches = launches;
     h->launches += launches;
-    if (st[kStErr] & kErrOverflow)
-        return fail(CULIPX_NOT_SUPPORTED, "culipx_factor_compute: a sparse block exceeded its fill cap (dual dropping is not implemented yet)");
     f->computed = true;
     return CULIPX_OK;
 }
 
-int factor_export(Factor* f, int* blk_nnz, long long* blk_off, int* idx, void* val, void* tri,
-                  int* is_piv, int* perm, int* got_extra, long long* total)
+int factor_export(Factor* f, int* blk_nnz, long long* blk_off, int* idx, void* val, void* tri, int* is_piv, int* perm,
+                  int* got_extra, long long* total)
 {
     if (!f->computed) return fail(CULIPX_INVALID_ARG, "culipx_factor_export: factor not computed");
     Pattern& p = *f->pat;

@@ -39,6 +39,10 @@ struct Pattern {
     int num_levels = 0;
     std::vector<int> lvl_off, lvl_rows, row_level;
     std::vector<int> lb_off, lb;  // factor order per level: pivots, then off-diagonal (CSR order)
+    // per row position t of lvl_rows: index of the row's first off-diagonal
+    // block inside its level's off-diagonal list
+    std::vector<int> row_offdiag_start;
+    long long sparse_slots = 0;   // sum of the sparse blocks' capacities
     std::vector<int> sb_off, sb;  // U' sweep order per column level
     int max_level_blocks = 0, max_level_rows = 0;
     int num_sparse = 0, num_dense = 0;
@@ -51,6 +55,7 @@ struct Pattern {
     std::vector<int> idx_init;   // val_slots entries: sparse local indices of A's entries (-1 unused)
     std::vector<int> nnz_init;   // per block
 
+    DeviceBuffer d_row_offdiag_start;
     DeviceBuffer d_cs_off, d_desc, d_bs, d_csc_off, d_csc_blk, d_lb, d_lvl_rows, d_a_dst, d_idx_init,
         d_nnz_init, d_fmt, d_maxnnz, d_row_block;
     long long device_bytes = 0;

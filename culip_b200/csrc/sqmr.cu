@@ -82,14 +82,20 @@ __device__ bool grid_sum(double (&v)[NV], double* partials, Scal* S)
     }
     __syncthreads();
     if (!last) return false;
-    if (threadIdx.x == 0) {
-        __threadfence();
+    __threadfence();
+    // the last CTA reduces the partials with all its threads: thread t sums
+    // partials t, t + blockDim, ... (fixed order), then a fixed shuffle tree
+    double w[NV];
 #pragma unroll
-        for (int k = 0; k < NV; ++k) {
-            double t = 0.0;
-            for (int b = 0; b < (int)gridDim.x; ++b) t += ((volatile double*)partials)[k * kGrid + b];
-            v[k] = t;
-        }
+    for (int k = 0; k < NV; ++k) {
+        double t = 0.0;
+        for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) t += __ldcg(partials + k * kGrid + b);
+        w[k] = t;
+    }
+    block_sum<NV>(w, sh);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) v[k] = w[k];
         S->ticket = 0;
     }
     return true;

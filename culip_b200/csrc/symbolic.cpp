@@ -224,6 +224,14 @@ int analyze_pattern(culipx_handle_t* h, int n, const int* rowptr, const int* col
             p.max_level_rows = std::max(p.max_level_rows, p.lvl_off[L + 1] - p.lvl_off[L]);
         }
         p.lb_off[nl] = o;
+        p.row_offdiag_start.resize(cm);
+        for (int L = 0; L < nl; ++L) {
+            int s = 0;
+            for (int t = p.lvl_off[L]; t < p.lvl_off[L + 1]; ++t) {
+                p.row_offdiag_start[t] = s;
+                s += p.cs_off[p.lvl_rows[t] + 1] - p.cs_off[p.lvl_rows[t]] - 1;
+            }
+        }
     }
     // U' sweep order: per column level, pivots then off-diagonal blocks (block-id order)
     p.sb_off.assign(nl + 1, 0);
@@ -289,6 +297,7 @@ int analyze_pattern(culipx_handle_t* h, int n, const int* rowptr, const int* col
             d.cap = (p.fmt[q] == kDense) ? r * c : std::max(p.max_nnz[q], p.blk_nnzA[q]);
             d.val_off = (int)o;
             o += d.cap;
+            if (p.fmt[q] == kSparse) p.sparse_slots += d.cap;
             if (o > 0x7fffffffLL) { delete pp; return fail(CULIPX_NOT_SUPPORTED, "culipx_pattern_analyze: factor storage exceeds 2^31 slots"); }
         }
         p.val_slots = o;
@@ -331,6 +340,7 @@ int analyze_pattern(culipx_handle_t* h, int n, const int* rowptr, const int* col
         if (st == CULIPX_OK) st = buf.upload(h, src, bytes);
     };
     up(p.d_cs_off, p.cs_off.data(), sizeof(int) * (cm + 1));
+    up(p.d_row_offdiag_start, p.row_offdiag_start.data(), sizeof(int) * cm);
     up(p.d_desc, p.desc.data(), sizeof(BlockDesc) * cnz);
     up(p.d_bs, p.bs.data(), sizeof(int) * (cm + 1));
     up(p.d_csc_off, p.csc_off.data(), sizeof(int) * (cm + 1));

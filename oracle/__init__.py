@@ -59,7 +59,7 @@ def lib():
         L.orc_sqmr_d.restype = ctypes.c_int
         L.orc_sqmr_d.argtypes = [ctypes.c_int, vp, vp, vp, vp, vp, vp, ctypes.c_double, ctypes.c_int, vp]
         L.orc_sqmr_ldu_d.restype = ctypes.c_int
-        L.orc_sqmr_ldu_d.argtypes = [ctypes.c_int] + [vp] * 11 + [ctypes.c_double, ctypes.c_int, vp]
+        L.orc_sqmr_ldu_d.argtypes = [ctypes.c_int] + [vp] * 12 + [ctypes.c_double, ctypes.c_int, vp]
         _lib = L
     return _lib
 

@@ -304,15 +304,27 @@ static void F(factorize_tile)(REAL T[32][32], int len, int *is_piv, REAL *D, int
 /* d_left_solve_with_D_Ut: A <- D^-1 U^-T A for an h x w block; U is the
  * factored pivot tile (row-major, unit upper with stored diagonal). */
 static void F(left_solve_D_Ut)(REAL U[32][32], const REAL *D, REAL A[32][32],
-                               const int *is_piv, int h, int w)
+                               const int *is_piv, int h, int w, int literal)
 {
+    /* an identity pivot tile makes the substitution a sequence of exact
+     * no-ops (divide by 1, subtract 0 * x); an all-zero column stays zero */
+    int ident = 1;
+    for (int i = 0; i < h && ident; ++i)
+        for (int l = i; l < h; ++l)
+            if ((l == i) ? (U[i][l] != 1) : (U[i][l] != 0)) { ident = 0; break; }
     for (int j = 0; j < w; ++j) {
+        if (!literal) {
+            int any = 0;
+            for (int l = 0; l < h; ++l) any |= (A[l][j] != 0);
+            if (!any) continue;
+        }
         REAL rhs[32];
         for (int l = 0; l < 32; ++l) rhs[l] = (l < h) ? A[l][j] : (REAL)0;
-        for (int i = 0; i < h; ++i) {
-            const REAL piv = rhs[i] / U[i][i];
-            for (int l = i + 1; l < h; ++l) rhs[l] = FMA(-U[i][l], piv, rhs[l]);
-        }
+        if (!ident || literal)
+            for (int i = 0; i < h; ++i) {
+                const REAL piv = rhs[i] / U[i][i];
+                for (int l = i + 1; l < h; ++l) rhs[l] = FMA(-U[i][l], piv, rhs[l]);
+            }
         for (int l = h; l < 32; ++l) rhs[l] = 0;
         REAL x1v[32], x2v[32];
         for (int l = 0; l < 32; ++l) {
@@ -522,12 +534,13 @@ F(fac_t) *F(orc_factor)(const orc_sym *s, const REAL *vals, const int *is_piv_in
                         for (int l = 0; l < 32; ++l) A[i][l] = tmp[pi][l];
                     }
                 }
-                F(left_solve_D_Ut)(U, f->tri + 3 * (size_t)from, A, f->is_piv + from, h, w);
-                for (int l = 0; l < h; ++l) {
-                    REAL rs = 0;
-                    for (int j = 0; j < w; ++j) rs = FMA(A[l][j], A[l][j], rs);
-                    f->row_norm[from + l] += rs;
-                }
+                F(left_solve_D_Ut)(U, f->tri + 3 * (size_t)from, A, f->is_piv + from, h, w, f->literal);
+                if (f->threshold > 0 || f->literal)
+                    for (int l = 0; l < h; ++l) {
+                        REAL rs = 0;
+                        for (int j = 0; j < w; ++j) rs = FMA(A[l][j], A[l][j], rs);
+                        f->row_norm[from + l] += rs;
+                    }
             }
             for (int k = 0; k < nb; ++k) F(drop_and_save)(f, s->lb[t + k], tiles[k]);
             free(tiles);
