@@ -55,7 +55,7 @@ struct Pattern {
     std::vector<int> idx_init;   // val_slots entries: sparse local indices of A's entries (-1 unused)
     std::vector<int> nnz_init;   // per block
 
-    DeviceBuffer d_row_offdiag_start;
+    DeviceBuffer d_row_offdiag_start, d_lvl_off;
     DeviceBuffer d_cs_off, d_desc, d_bs, d_csc_off, d_csc_blk, d_lb, d_lvl_rows, d_a_dst, d_idx_init,
         d_nnz_init, d_fmt, d_maxnnz, d_row_block;
     long long device_bytes = 0;

@@ -397,9 +397,12 @@ int sqmr_solve(culipx_handle_t* h, Csr* A, Factor* M, const double* b, double* x
     if (A->m != A->n) return fail(CULIPX_INVALID_ARG, "culipx_sqmr_solve: A must be square");
     if (M && (!M->computed || M->pat->n != A->m))
         return fail(CULIPX_INVALID_ARG, "culipx_sqmr_solve: preconditioner not computed or wrong size");
-    if (M && M->precision != CULIPX_F64)
-        return fail(CULIPX_NOT_SUPPORTED, "culipx_sqmr_solve: FP32 preconditioner needs culipx_kkt_solve");
     if (max_it < 0) return fail(CULIPX_INVALID_ARG, "culipx_sqmr_solve: max_it < 0");
+    // with a preconditioner: the single-launch persistent solver (FP64 or FP32 factor)
+    if (M && !w->force_multi_kernel)
+        return sqmr_solve_persistent(h, A, M, b, x, tol, max_it, residual, iterations, w);
+    if (M && M->precision != CULIPX_F64)
+        return fail(CULIPX_NOT_SUPPORTED, "culipx_sqmr_solve: the multi-kernel solver needs an FP64 factor");
     const int n = A->m;
     cudaStream_t s = h->stream;
     CULIPX_TRY(sqmr_workspace(w, h, n));

@@ -11,6 +11,7 @@ struct Factor;
 // Work vectors (13 x n doubles), per-CTA partials and the device scalar block.
 struct Sqmr {
     int n = -1;
+    bool force_multi_kernel = false;  // use the per-phase kernels instead of the persistent solver
     DeviceBuffer vecs, partials, scal;
     void* host_flags = nullptr;  // pinned
     ~Sqmr()
@@ -22,5 +23,7 @@ struct Sqmr {
 int sqmr_workspace(Sqmr* w, culipx_handle_t* h, int n);
 int sqmr_solve(culipx_handle_t* h, Csr* A, Factor* M, const double* b, double* x, double tol, int max_it,
                double* residual, int* iterations, Sqmr* w);
+int sqmr_solve_persistent(culipx_handle_t* h, Csr* A, Factor* M, const double* b, double* x, double tol, int max_it,
+                          double* residual, int* iterations, Sqmr* w);
 
 }  // namespace culipx

@@ -341,6 +341,7 @@ int analyze_pattern(culipx_handle_t* h, int n, const int* rowptr, const int* col
     };
     up(p.d_cs_off, p.cs_off.data(), sizeof(int) * (cm + 1));
     up(p.d_row_offdiag_start, p.row_offdiag_start.data(), sizeof(int) * cm);
+    up(p.d_lvl_off, p.lvl_off.data(), sizeof(int) * (p.num_levels + 1));
     up(p.d_desc, p.desc.data(), sizeof(BlockDesc) * cnz);
     up(p.d_bs, p.bs.data(), sizeof(int) * (cm + 1));
     up(p.d_csc_off, p.csc_off.data(), sizeof(int) * (cm + 1));

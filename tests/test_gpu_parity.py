@@ -113,3 +113,71 @@ def test_sqmr_small_kkt(handle):
     r = b - oracle.spmv(rp, ci, v, xg)
     ro = b - oracle.spmv(rp, ci, v, xo)
     assert np.linalg.norm(r) <= 2 * np.linalg.norm(ro) + 1e-12 * np.linalg.norm(b)
+
+
+def _csr_op(handle, rp, ci, v):
+    return cb.CsrOperator(handle, torch.from_numpy(np.ascontiguousarray(rp, np.int32)).cuda(),
+                          torch.from_numpy(np.ascontiguousarray(ci, np.int32)).cuda(),
+                          torch.from_numpy(np.ascontiguousarray(v, np.float64)).cuda())
+
+
+@pytest.mark.parametrize("fill_level", [0, 1])
+def test_sqmr_deep_levels(handle, fill_level):
+    """Random symmetric indefinite matrix, random blocking: many levels in the
+    persistent solver's sweeps."""
+    from problems import random_blocking
+
+    rp, ci, v = random_spd_ish(900, 0.01, seed=12)
+    bs = random_blocking(900, np.random.default_rng(3), 2, 20)
+    S, OF, P, F = _factor_both(handle, rp, ci, v, bs, fill_level=fill_level)
+    assert P.info()["num_levels"] > 5
+    b = cb.normal_vector(21, len(rp) - 1)
+    xo, reso, ito = oracle.sqmr(rp, ci, v, b, OF, 1e-10, 500)
+    A = _csr_op(handle, rp, ci, v)
+    xg = torch.zeros(len(rp) - 1, dtype=torch.float64, device="cuda")
+    res, its, st = cb.sqmr_solve(handle, A, F, torch.from_numpy(b).cuda(), xg, 1e-10, 500)
+    xg = xg.cpu().numpy()
+    assert abs(its - ito) <= 4
+    assert np.linalg.norm(xg - xo) / np.linalg.norm(xo) < 1e-6
+    import scipy.sparse as sp
+
+    K = sp.csr_matrix((v, ci, rp))
+    assert np.linalg.norm(b - K @ xg) / np.linalg.norm(b) < 1e-6
+
+
+def test_sqmr_reference_fixture_unpreconditioned(handle):
+    """tests/la/test_sqmr.cc small_D: SQMR without preconditioner, term_tol 1e-10,
+    ||b - A x|| <= 1e-5 ||b||, iterations <= n."""
+    import os
+
+    d = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "sqmr_small.npz"))
+    rp, ci, v = d["A_rowptr"], d["A_colidx"], d["A_val"]
+    n = len(rp) - 1
+    import scipy.sparse as sp
+
+    Kh = sp.csr_matrix((v, ci, rp), shape=(n, n))
+    b = Kh @ np.ones(n)
+    A = _csr_op(handle, rp, ci, v)
+    xg = torch.zeros(n, dtype=torch.float64, device="cuda")
+    res, its, st = cb.sqmr_solve(handle, A, None, torch.from_numpy(b).cuda(), xg, 1e-10, n)
+    x = xg.cpu().numpy()
+    assert np.linalg.norm(b - Kh @ x) <= 1e-5 * np.linalg.norm(b)
+    assert its <= n
+    xo, reso, ito = oracle.sqmr(rp, ci, v, b, None, 1e-10, n)
+    assert abs(its - ito) <= 4
+
+
+def test_sqmr_fp32_factor_mixed(handle):
+    """FP32 factor and applies, FP64 recurrence: converges on the small KKT."""
+    rp, ci, v, bs = kkt("small")
+    P = cb.Pattern(handle, rp, ci, bs, 0, 1.0, cb.F32)
+    F = cb.Factor(P)
+    F.compute(torch.from_numpy(v.astype(np.float32)).cuda())
+    b = cb.normal_vector(cb.SEED + 1, len(rp) - 1)
+    A = _csr_op(handle, rp, ci, v)
+    xg = torch.zeros(len(rp) - 1, dtype=torch.float64, device="cuda")
+    res, its, st = cb.sqmr_solve(handle, A, F, torch.from_numpy(b).cuda(), xg, 1e-8, 1000)
+    import scipy.sparse as sp
+
+    K = sp.csr_matrix((v, ci, rp))
+    assert np.linalg.norm(b - K @ xg.cpu().numpy()) / np.linalg.norm(b) < 1e-4
