@@ -264,6 +264,19 @@ def sqmr_solve(handle: Handle, A: CsrOperator, M: Factor | None, b, x, tol=1e-8,
     return res.value, its.value, st
 
 
+def sqmr_solve_noalloc(handle: Handle, A: CsrOperator, M: Factor, b, x, tol=1e-8, max_it=1000):
+    """sqmr_solve without device allocation, for callers that cannot allocate
+    device memory while they solve (GPU memory owned by another allocator, or
+    request loops where cudaMalloc could synchronize the device).  Uses a fixed
+    scratch compiled into the library: n <= 65536, one call at a time on the
+    GPU.  Returns (residual, iterations, status)."""
+    res = ctypes.c_double()
+    its = ctypes.c_int()
+    st = capi.call("culipx_sqmr_solve_noalloc", handle._h, A._h, M._h, _dptr(b), _dptr(x), float(tol), int(max_it),
+                   ctypes.byref(res), ctypes.byref(its), allow=(capi.OK, capi.MAXIT))
+    return res.value, its.value, st
+
+
 # --------------------------------------------------------------------------
 # Reference-named facade (same names, argument meaning and return values)
 

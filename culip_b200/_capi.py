@@ -68,6 +68,7 @@ _SIGS = {
     "culipx_csr_destroy": [vp],
     "culipx_spmv": [vp, vp, vp, f64, f64, i32],
     "culipx_sqmr_solve": [vp, vp, vp, vp, vp, f64, i32, ctypes.POINTER(f64), ctypes.POINTER(i32)],
+    "culipx_sqmr_solve_noalloc": [vp, vp, vp, vp, vp, f64, i32, ctypes.POINTER(f64), ctypes.POINTER(i32)],
 }
 
 _lib = None

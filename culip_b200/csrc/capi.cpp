@@ -320,4 +320,15 @@ CULIPX_API int culipx_sqmr_solve(culipx_handle h, culipx_csr A, culipx_factor M,
     GUARD_END
 }
 
+CULIPX_API int culipx_sqmr_solve_noalloc(culipx_handle h, culipx_csr A, culipx_factor M, const double* d_b,
+                                         double* d_x, double tol, int max_it, double* residual, int* iterations)
+{
+    if (!h) return fail(CULIPX_INVALID_ARG, "null handle");
+    if (h->device < 0) return fail(CULIPX_INVALID_ARG, "culipx_sqmr_solve_noalloc: host-only handle");
+    GUARD_BEGIN
+    CULIPX_TRY(use_device(h));
+    return sqmr_solve_noalloc(h, A, M, d_b, d_x, tol, max_it, residual, iterations);
+    GUARD_END
+}
+
 }  // extern "C"

@@ -25,5 +25,7 @@ int sqmr_solve(culipx_handle_t* h, Csr* A, Factor* M, const double* b, double* x
                double* residual, int* iterations, Sqmr* w);
 int sqmr_solve_persistent(culipx_handle_t* h, Csr* A, Factor* M, const double* b, double* x, double tol, int max_it,
                           double* residual, int* iterations, Sqmr* w);
+int sqmr_solve_noalloc(culipx_handle_t* h, Csr* A, Factor* M, const double* b, double* x, double tol, int max_it,
+                       double* residual, int* iterations);
 
 }  // namespace culipx

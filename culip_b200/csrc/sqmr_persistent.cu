@@ -570,4 +570,163 @@ int sqmr_solve_persistent(culipx_handle_t* h, Csr* A, Factor* M, const double* b
     return CULIPX_OK;
 }
 
+// ---------------------------------------------------------------------------
+// SQMR without device allocation.
+//
+// For callers that cannot allocate device memory when they solve: processes
+// whose device memory is already handed out by another allocator (a caching
+// allocator such as PyTorch's, or an application-wide pool that owns the
+// GPU), and latency-critical request loops, where cudaMalloc / cudaFree can
+// synchronize the device and take milliseconds.  The factor (and K) are set
+// up beforehand through the regular entry points; this call then uses a
+// fixed scratch area compiled into the library instead of the handle's
+// workspace.
+//
+// The scratch is a file-scope device array of kNoAllocMaxRows x 14 doubles
+// plus the per-CTA reduction slots (about 7.4 MB): every GPU that loads this
+// library holds it until the process exits.  All calls share it and it keeps
+// the last call's contents; the call clears what must start at zero.  Calls
+// whose work overlaps on the GPU (two streams, two host threads) race on it.
+// The first call on a device looks up the array's device address with
+// cudaGetSymbolAddress (with that device current); make that first call
+// before any stream capture.
+namespace {
+
+constexpr int kNoAllocMaxRows = 65536;
+constexpr int kNoAllocMaxGrid = 1024;
+constexpr size_t kNoAllocVecs = 14 * (size_t)kNoAllocMaxRows;
+constexpr size_t kNoAllocSlots = kNoAllocVecs + (size_t)2 * kMaxNV * kNoAllocMaxGrid;
+
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocSlots];
+
+double* g_noalloc_ptr[64] = {nullptr};  // per-device address of g_noalloc_scratch
+int g_noalloc_grid[64][2] = {{0, 0}};   // per-device grid size per factor precision
+
+int noalloc_setup(int dev)
+{
+    if (dev < 0 || dev >= 64) return fail(CULIPX_INVALID_ARG, "culipx_sqmr_solve_noalloc: device %d out of range", dev);
+    if (g_noalloc_ptr[dev]) return CULIPX_OK;
+    void* ptr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    if (e != cudaSuccess || !ptr) {
+        cudaGetLastError();
+        return fail(CULIPX_CUDA_ERROR, "culipx_sqmr_solve_noalloc: cudaGetSymbolAddress failed: %s",
+                    cudaGetErrorString(e));
+    }
+    g_noalloc_ptr[dev] = static_cast<double*>(ptr);
+    return CULIPX_OK;
+}
+
+template <class TF>
+int noalloc_grid(int dev, int* G)
+{
+    int& g = g_noalloc_grid[dev][sizeof(TF) == 8 ? 0 : 1];
+    if (g == 0) {
+        const size_t smem = (size_t)kW * kTileElems * sizeof(TF);
+        CULIPX_CUDA(cudaFuncSetAttribute(k_sqmr_persistent<TF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        int per_sm = 0, sms = 0;
+        CULIPX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        CULIPX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sqmr_persistent<TF>, kT, smem));
+        if (per_sm < 1) return fail(CULIPX_NOT_SUPPORTED, "persistent SQMR kernel does not fit on an SM");
+        g = std::min(sms * std::min(per_sm, 2), kNoAllocMaxGrid);
+    }
+    *G = g;
+    return CULIPX_OK;
+}
+
+template <class TF>
+int launch_noalloc(culipx_handle_t* h, Csr* A, Factor* M, const double* b, double* x, double tol, int max_it,
+                   double* residual, int* iterations, bool* converged, bool* breakdown)
+{
+    const int n = A->m;
+    cudaStream_t s = h->stream;
+    int dev = 0;
+    CULIPX_CUDA(cudaGetDevice(&dev));
+    CULIPX_TRY(noalloc_setup(dev));
+    int G = 0;
+    CULIPX_TRY(noalloc_grid<TF>(dev, &G));
+    Pattern& p = *M->pat;
+    double* base = g_noalloc_ptr[dev];
+    PArgs<TF> a;
+    a.n = n;
+    a.nl = p.num_levels;
+    a.max_it = max_it;
+    const double avg = (double)A->nnz / std::max(n, 1);
+    a.spmv_lanes = (avg <= 4.5) ? 4 : (avg <= 12.0) ? 8 : (avg <= 24.0) ? 16 : 32;
+    a.tol = tol;
+    a.rowptr = A->rowptr;
+    a.colidx = A->colidx;
+    a.kval = static_cast<const double*>(A->val);
+    a.fval = M->val.as<TF>();
+    a.tri = M->tri.as<TF>();
+    a.is_piv = M->is_piv.as<int>();
+    a.perm = M->perm.as<int>();
+    a.bs = p.d_bs.as<int>();
+    a.lvl_off = p.d_lvl_off.as<int>();
+    a.lvl_rows = p.d_lvl_rows.as<int>();
+    a.u_off = M->u_off.as<int>();
+    a.u_col = M->u_col.as<int>();
+    a.u_val = M->u_val.as<TF>();
+    a.ut_off = M->ut_off.as<int>();
+    a.ut_col = M->ut_col.as<int>();
+    a.ut_val = M->ut_val.as<TF>();
+    a.piv_off = M->piv_off.as<long long>();
+    a.rowflags = M->rowflags.as<int>();
+    for (int i = 0; i < 3; ++i) {
+        a.v[i] = base + (size_t)i * n;
+        a.w[i] = base + (size_t)(3 + i) * n;
+        a.p[i] = base + (size_t)(6 + i) * n;
+    }
+    a.Av = base + (size_t)9 * n;
+    a.tvec = base + (size_t)10 * n;
+    a.ev = base + (size_t)11 * n;
+    a.ev2 = base + (size_t)12 * n;
+    a.out = base + (size_t)13 * n;
+    a.partials = base + kNoAllocVecs;
+    a.x = x;
+    a.b = b;
+    // the scratch keeps the previous call's contents: clear the recurrence vectors
+    CULIPX_CUDA(cudaMemsetAsync(base, 0, (size_t)13 * n * sizeof(double), s));
+    CULIPX_CUDA(cudaMemsetAsync(x, 0, (size_t)n * sizeof(double), s));
+    const size_t smem = (size_t)kW * kTileElems * sizeof(TF);
+    void* args[] = {&a};
+    CULIPX_CUDA(cudaLaunchCooperativeKernel((const void*)k_sqmr_persistent<TF>, dim3(G), dim3(kT), args, smem, s));
+    h->launches += 1;
+    double out[6];
+    CULIPX_CUDA(cudaMemcpyAsync(out, a.out, sizeof(out), cudaMemcpyDeviceToHost, s));
+    CULIPX_CUDA(cudaStreamSynchronize(s));
+    if (residual) *residual = out[0];
+    if (iterations) *iterations = (int)out[1];
+    *breakdown = out[2] != 0.0;
+    *converged = out[3] != 0.0;
+    return CULIPX_OK;
+}
+
+}  // namespace
+
+int sqmr_solve_noalloc(culipx_handle_t* h, Csr* A, Factor* M, const double* b, double* x, double tol, int max_it,
+                       double* residual, int* iterations)
+{
+    if (!A || !M || !b || !x) return fail(CULIPX_INVALID_ARG, "culipx_sqmr_solve_noalloc: null argument");
+    if (A->precision != CULIPX_F64 || A->m != A->n)
+        return fail(CULIPX_INVALID_ARG, "culipx_sqmr_solve_noalloc: A must be square FP64");
+    if (!M->computed || M->pat->n != A->m)
+        return fail(CULIPX_INVALID_ARG, "culipx_sqmr_solve_noalloc: preconditioner not computed or wrong size");
+    if (A->m > kNoAllocMaxRows)
+        return fail(CULIPX_INVALID_ARG,
+                    "culipx_sqmr_solve_noalloc: n = %d exceeds the fixed scratch of %d rows; use culipx_sqmr_solve",
+                    A->m, kNoAllocMaxRows);
+    if (max_it < 0) return fail(CULIPX_INVALID_ARG, "culipx_sqmr_solve_noalloc: max_it < 0");
+    bool conv = false, bd = false;
+    int st;
+    if (M->precision == CULIPX_F64)
+        st = launch_noalloc<double>(h, A, M, b, x, tol, max_it, residual, iterations, &conv, &bd);
+    else
+        st = launch_noalloc<float>(h, A, M, b, x, tol, max_it, residual, iterations, &conv, &bd);
+    if (st != CULIPX_OK) return st;
+    if (bd) return fail(CULIPX_BREAKDOWN, "culipx_sqmr_solve_noalloc: breakdown (non-finite scalar)");
+    if (!conv && max_it > 0 && iterations && *iterations >= max_it) return CULIPX_MAXIT;
+    return CULIPX_OK;
+}
+
 }  // namespace culipx

@@ -172,6 +172,22 @@ int culipx_spmv(culipx_csr A, const void *d_x, void *d_y, double alpha, double b
 int culipx_sqmr_solve(culipx_handle h, culipx_csr A, culipx_factor M, const double *d_b,
                       double *d_x, double tol, int max_it, double *residual, int *iterations);
 
+/* The same solve (same kernel, same results) without any device allocation;
+ * no counterpart in the reference.  For callers that cannot allocate device
+ * memory while they solve: processes whose GPU memory is already owned by
+ * another allocator (a caching allocator such as PyTorch's, or an
+ * application-wide pool), and latency-critical request loops in which
+ * cudaMalloc / cudaFree could synchronize the device.  M must be a computed
+ * factor (FP64 or FP32); n must not exceed 65536 (larger n is rejected with
+ * CULIPX_INVALID_ARG).  The work vectors live in a fixed scratch array
+ * compiled into the library (about 7.4 MB, held by every GPU that loads the
+ * library until the process exits); it is shared by all calls and keeps the
+ * last call's contents, so calls whose work overlaps on the GPU race.  The
+ * first call on a device looks up the scratch's device address; make it
+ * before any stream capture. */
+int culipx_sqmr_solve_noalloc(culipx_handle h, culipx_csr A, culipx_factor M, const double *d_b,
+                              double *d_x, double tol, int max_it, double *residual, int *iterations);
+
 #ifdef __cplusplus
 }
 #endif
