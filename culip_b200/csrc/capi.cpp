@@ -320,6 +320,34 @@ CULIPX_API int culipx_sqmr_solve(culipx_handle h, culipx_csr A, culipx_factor M,
     GUARD_END
 }
 
+CULIPX_API int culipx_sqmr_profile(culipx_handle h, int enable)
+{
+    if (!h) return fail(CULIPX_INVALID_ARG, "null handle");
+    h->sqmr->profile = enable != 0;
+    return CULIPX_OK;
+}
+
+CULIPX_API int culipx_sqmr_phase_times(culipx_handle h, double* out_us, int iterations)
+{
+    if (!h || !out_us || iterations < 0) return fail(CULIPX_INVALID_ARG, "bad argument");
+    if (!h->sqmr->profile || !h->sqmr->ts.get())
+        return fail(CULIPX_INVALID_ARG, "culipx_sqmr_phase_times: profiling was not enabled for the last solve");
+    CULIPX_TRY(use_device(h));
+    const int its = iterations < 64 ? iterations : 64;
+    unsigned long long ts[64 * 8];
+    CULIPX_CUDA(cudaStreamSynchronize(h->stream));
+    CULIPX_CUDA(cudaMemcpy(ts, h->sqmr->ts.get(), sizeof(ts), cudaMemcpyDeviceToHost));
+    // per iteration: B (v+, ||v+||), U sweep, SpMV, U' sweep + beta, A (x, p, next alpha), total
+    for (int i = 0; i < its; ++i) {
+        const unsigned long long* t = ts + i * 8;
+        const unsigned long long next = (i + 1 < 64 && ts[(i + 1) * 8]) ? ts[(i + 1) * 8] : t[5];
+        const double d[6] = {(t[1] - t[0]) * 1e-3, (t[2] - t[1]) * 1e-3, (t[3] - t[2]) * 1e-3,
+                             (t[4] - t[3]) * 1e-3, (t[5] - t[4]) * 1e-3, (next - t[0]) * 1e-3};
+        for (int k = 0; k < 6; ++k) out_us[i * 6 + k] = t[5] ? d[k] : 0.0;
+    }
+    return CULIPX_OK;
+}
+
 CULIPX_API int culipx_sqmr_solve_noalloc(culipx_handle h, culipx_csr A, culipx_factor M, const double* d_b,
                                          double* d_x, double tol, int max_it, double* residual, int* iterations)
 {

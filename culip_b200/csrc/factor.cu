@@ -40,7 +40,10 @@ namespace {
 constexpr int kWarps = 4;  // blocks per CTA
 
 // device scalars in Factor::state
-enum StateSlot { kStErr = 0, kStLeftover = 1, kStArena = 2, kStDeferred = 3, kStLevelAcc = 4 };
+enum StateSlot { kStErr = 0, kStLeftover = 1, kStArena = 2, kStDeferred = 3, kStLevelAcc = 4, kStSlow = 5 };
+
+// per block row flags set by the pivot kernel
+enum RowFlags { kRowIdentity = 1, kRowHas2x2 = 2, kRowPermIdentity = 4, kRowNoUpdates = 8 };
 enum ErrBits { kErrLeftoverNegative = 1 };
 
 enum OffdiagMode { kFirst = 0, kCount = 1, kWrite = 2 };
@@ -66,6 +69,7 @@ struct FactorArgs {
     int* rowflags;
     long long* state;
     int* deferred;
+    int* slowlist;        // off-diagonal positions left to the tiled kernel
     long long val_slots;  // first arena slot
 };
 
@@ -106,6 +110,7 @@ __global__ void __launch_bounds__(32 * kWarps) k_pivot_blocks(FactorArgs a, T* v
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         a.state[kStDeferred] = 0;
         a.state[kStLevelAcc] = 0;
+        a.state[kStSlow] = 0;
     }
     const int warp = threadIdx.x >> 5;
     const int t = blockIdx.x * kWarps + warp;
@@ -121,8 +126,9 @@ __global__ void __launch_bounds__(32 * kWarps) k_pivot_blocks(FactorArgs a, T* v
     for (int e = lane; e < kTileElems; e += 32) Q[e] = T(0);
     load_block(Tt, b, a.desc, a.bs, a.boff, a.nnz, a.fmt, val, a.idx, true);
 
+    const int q_beg = a.csc_off[I];
     const int q_end = a.csc_off[I + 1] - 1;  // the last block of the column is the pivot
-    for (int q = a.csc_off[I]; q < q_end; ++q) {
+    for (int q = q_beg; q < q_end; ++q) {
         const int kb = a.csc_blk[q];
         const int K = a.desc[kb].row;
         const int bw = a.bs[K + 1] - a.bs[K];
@@ -131,7 +137,30 @@ __global__ void __launch_bounds__(32 * kWarps) k_pivot_blocks(FactorArgs a, T* v
         unload_block(Q, kb, a.desc, a.bs, a.boff, a.nnz, a.fmt, a.idx);
     }
     __syncwarp();
-    factorize_tile(Tt, len, a.is_piv + from, tri + 3 * (size_t)from, a.perm + from, method);
+    // A diagonal tile under BK / Rook pivoting takes a 1x1 pivot at every step
+    // without swaps (the off-diagonal maximum is 0); each step leaves U = I and
+    // D = the diagonal (perturbed to 1e-6 below 1e-8, d_ldlt_1x1_step :556-560),
+    // all other updates being fma(-0, x, y).  Done directly:
+    bool diag = true;
+    for (int i = 0; i < len; ++i) diag &= (lane == i || lane >= len || Tt[i * kTileStride + lane] == T(0));
+    diag = __all_sync(0xffffffffu, diag) && method != CULIPX_PIV_STATIC;
+    if (diag) {
+        T* D = tri + 3 * (size_t)from;
+        if (lane < len) {
+            T d = Tt[lane * kTileStride + lane];
+            if (fabs(d) < 1e-8) d = T(1e-6);
+            Tt[lane * kTileStride + lane] = T(1);
+            D[3 * lane] = T(0);
+            D[3 * lane + 1] = d;
+            D[3 * lane + 2] = T(0);
+            a.is_piv[from + lane] = 1;
+        }
+        __syncwarp();
+    } else {
+        factorize_tile(Tt, len, a.is_piv + from, tri + 3 * (size_t)from, a.perm + from, method);
+    }
+    const bool perm_ident = __all_sync(0xffffffffu, lane >= len || a.perm[from + lane] == from + lane);
+    const bool no_updates = (q_end == q_beg);
 
     if (row_norm) {
         T rs = T(0);
@@ -153,7 +182,75 @@ __global__ void __launch_bounds__(32 * kWarps) k_pivot_blocks(FactorArgs a, T* v
     bool two = false;
     if (lane < len) two = (tri[3 * (size_t)(from + lane) + 2] != T(0)) || (tri[3 * (size_t)(from + lane)] != T(0));
     two = __any_sync(0xffffffffu, two);
-    if (lane == 0) a.rowflags[I] = (ident ? 1 : 0) | (two ? 2 : 0);
+    if (lane == 0)
+        a.rowflags[I] = (ident ? kRowIdentity : 0) | (two ? kRowHas2x2 : 0) | (perm_ident ? kRowPermIdentity : 0) |
+                        (no_updates ? kRowNoUpdates : 0);
+}
+
+// Off-diagonal blocks of rows with no fan-in updates, an identity pivot tile,
+// 1x1 pivots only and no swaps: U_ij = D_i^-1 A_ij entry by entry, with the
+// same Givens-form arithmetic as the tiled path (d_left_solve_with_D_Ut
+// :1536-1557 reduces to x = (c a) / |d|); |u| <= NZ_EPS dropped, compacted in
+// place in row-major order.  Every other block goes to the slow list that
+// k_offdiag<kFirst> processes.
+template <class T>
+__global__ void k_offdiag_fast(FactorArgs a, T* val, const T* tri, int lb_first, int noff, int allow)
+{
+    const int lane = lane_id();
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < noff; t += nw) {
+        const int b = a.lb[lb_first + t];
+        const DevBlock d = a.desc[b];
+        const int flags = a.rowflags[d.row];
+        const bool fast = allow && a.fmt[b] == 0 &&
+                          (flags & (kRowIdentity | kRowHas2x2 | kRowPermIdentity | kRowNoUpdates)) ==
+                              (kRowIdentity | kRowPermIdentity | kRowNoUpdates);
+        if (!fast) {
+            if (lane == 0) {
+                const int slot = (int)atomicAdd(reinterpret_cast<unsigned long long*>(&a.state[kStSlow]), 1ull);
+                a.slowlist[slot] = t;
+            }
+            continue;
+        }
+        const int from = a.bs[d.row], h = a.bs[d.row + 1] - from;
+        const int w = a.bs[d.col + 1] - a.bs[d.col];
+        const T* D = tri + 3 * (size_t)from;
+        const long long off = d.val_off;
+        const int cnt = a.nnz_init[b];
+        int o = 0;
+        for (int base = 0; base < cnt; base += 32) {
+            const int e = base + lane;
+            const bool valid = e < cnt;
+            const int li = valid ? a.idx[off + e] : 0;
+            const T v = valid ? val[off + e] : T(0);
+            T u = T(0);
+            if (valid) {
+                const int r = li / w;
+                const T d11 = D[3 * r + 1], d12 = D[3 * r + 2];
+                const T d22 = (r < 31) ? ((r + 1 < h) ? D[3 * (r + 1) + 1] : T(0)) : D[3 * 31 + 1];
+                const T gr = sqrt(fma_rn(d11, d11, d12 * d12));
+                const T gc = d11 / gr, gs = d12 / gr;
+                const T td11 = fma_rn(gc, d11, gs * d12);
+                const T td12 = fma_rn(gc, d12, gs * d22);
+                T x1 = fma_rn(gc, v, gs * T(0));
+                x1 = fma_rn(-td12, T(0), x1) / td11;
+                u = x1;
+            }
+            const bool nz = valid && fabs(u) > T(kNzEps);
+            const unsigned m = __ballot_sync(0xffffffffu, nz);
+            if (nz) {
+                const int pos = o + __popc(m & ((1u << lane) - 1u));
+                val[off + pos] = u;
+                a.idx[off + pos] = li;
+            }
+            o += __popc(m);
+        }
+        if (lane == 0) {
+            a.nnz[b] = o;
+            atomicAdd(reinterpret_cast<unsigned long long*>(&a.state[kStLevelAcc]),
+                      (unsigned long long)(long long)(a.cap[b] - o));
+        }
+    }
 }
 
 // Off-diagonal block (I, J) up to its final values in Tt: fan-in updates over
@@ -351,10 +448,11 @@ __global__ void __launch_bounds__(32 * kWarps) k_offdiag(FactorArgs a, T* val, c
     T* R = Q + kTileElems;
     __shared__ unsigned keep_all[kWarps][32];
 
-    const int count = (MODE == kFirst) ? noff : (int)a.state[kStDeferred];
+    const int count = (int)a.state[(MODE == kFirst) ? kStSlow : kStDeferred];
     const int nw = gridDim.x * kWarps;
     for (int t = blockIdx.x * kWarps + warp; t < count; t += nw) {
-        const int pos = (MODE == kFirst) ? t : a.deferred[t];  // position in the level's off-diagonal list
+        // position in the level's off-diagonal list
+        const int pos = (MODE == kFirst) ? a.slowlist[t] : a.deferred[t];
         const int b = a.lb[lb_first + pos];
         const DevBlock d = a.desc[b];
         const int from = a.bs[d.row], h = a.bs[d.row + 1] - from;
@@ -623,6 +721,7 @@ int run_levels(Factor* f, const void* d_vals, cudaStream_t s, int* launches)
     a.rowflags = f->rowflags.as<int>();
     a.state = f->state.as<long long>();
     a.deferred = f->deferred.as<int>();
+    a.slowlist = f->slowlist.as<int>();
     a.val_slots = p.val_slots;
     const int pivoting = (f->pivot != CULIPX_PIV_STATIC);
     const size_t s3 = kWarps * 3 * kTileElems * sizeof(T);
@@ -637,10 +736,11 @@ int run_levels(Factor* f, const void* d_vals, cudaStream_t s, int* launches)
         CULIPX_TRY(launch_check("k_pivot_blocks"));
         if (noff > 0) {
             const int lbf = lb0 + npiv;
-            k_offdiag<T, kFirst><<<(noff + kWarps - 1) / kWarps, 32 * kWarps, s3, s>>>(a, val, tri, lbf, noff, pivoting,
-                                                                                   row_norm, norm_part, thv);
-            ++*launches;
             const int dgrid = (std::min(noff, 148 * 16) + kWarps - 1) / kWarps;
+            k_offdiag_fast<T><<<std::min((noff + 7) / 8, 148 * 32), 256, 0, s>>>(a, val, tri, lbf, noff, thr ? 0 : 1);
+            k_offdiag<T, kFirst><<<dgrid, 32 * kWarps, s3, s>>>(a, val, tri, lbf, noff, pivoting, row_norm, norm_part,
+                                                               thv);
+            *launches += 2;
             if (thr) {
                 k_row_norms<T><<<(npiv * 32 + 255) / 256, 256, 0, s>>>(a, row_norm, norm_part, p.lvl_off[L], npiv);
                 k_offdiag<T, kCount><<<dgrid, 32 * kWarps, s3, s>>>(a, val, tri, lbf, noff, pivoting, row_norm,
@@ -698,6 +798,7 @@ int factor_create(Pattern* p, Factor** out)
     al(f->rowflags, cm * sizeof(int));
     al(f->state, 16 * sizeof(long long));
     al(f->deferred, (size_t)std::max(p->max_level_blocks, 1) * sizeof(int));
+    al(f->slowlist, (size_t)std::max(p->max_level_blocks, 1) * sizeof(int));
     al(f->u_off, (n + 1) * sizeof(int));
     al(f->ut_off, (n + 1) * sizeof(int));
     al(f->u_col, off_slots * sizeof(int));

@@ -26,6 +26,7 @@ struct Factor {
     DeviceBuffer rowflags;       // per block row: bit0 pivot tile is identity, bit1 D has a 2x2
     DeviceBuffer state;          // device scalars (see factor.cu)
     DeviceBuffer deferred;       // per level list of deferred blocks
+    DeviceBuffer slowlist;       // per level list of blocks for the tiled off-diagonal kernel
     DeviceBuffer norm_part;      // threshold > 0: row-norm partials
     DeviceBuffer row_norm;       // n values
 

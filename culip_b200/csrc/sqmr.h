@@ -12,6 +12,8 @@ struct Factor;
 struct Sqmr {
     int n = -1;
     bool force_multi_kernel = false;  // use the per-phase kernels instead of the persistent solver
+    bool profile = false;             // record per-phase device timestamps of the persistent solver
+    DeviceBuffer ts;                  // 64 iterations x 8 phase stamps (ns, %globaltimer)
     DeviceBuffer vecs, partials, scal;
     void* host_flags = nullptr;  // pinned
     ~Sqmr()

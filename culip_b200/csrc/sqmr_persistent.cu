@@ -74,7 +74,23 @@ struct PArgs {
     const double* b;
     double* partials;  // 2 buffers x kMaxNV x gridDim
     double* out;       // [0] gamma/norm_pb, [1] iterations, [2] breakdown, [3] converged, [4] norm_pb, [5] it
+    unsigned long long* ts;  // optional phase timestamps: [it * 8 + phase], it < kTsIters
 };
+
+constexpr int kTsIters = 64;
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// CTA 0 stamps phase boundaries (right after the barrier that ends a phase)
+__device__ __forceinline__ void stamp(unsigned long long* ts, int it, int phase)
+{
+    if (ts && it < kTsIters && blockIdx.x == 0 && threadIdx.x == 0) ts[it * 8 + phase] = global_ns();
+}
 
 struct Scal {
     double alpha, beta[3], delta[3], c[3], s[3];
@@ -374,6 +390,7 @@ __global__ void __launch_bounds__(kT) k_sqmr_persistent(PArgs<TF> a)
     int it = 0;
     while (!S.done && it < a.max_it) {
         const int k0 = acc3(it), k1 = acc3(it + 1), km1 = acc3(it - 1), km2 = acc3(it - 2);
+        stamp(a.ts, it, 0);
         S.alpha = ad[0] / ad[1];
         // ---- B: v+ and ||v+|| ----
         {
@@ -390,14 +407,18 @@ __global__ void __launch_bounds__(kT) k_sqmr_persistent(PArgs<TF> a)
             S.delta[k1] = sqrt(acc[0]);
             S.inv_delta = 1.0 / S.delta[k1];
         }
+        stamp(a.ts, it, 1);
         // ---- U: v+ /= delta, w+ = eta delta D^-1 v+, ev = P U^-1 D^-1 v+ ----
         usweep<TF>(a, a.v[k1], S.inv_delta, true, a.w[k1], S.eta * S.delta[k1], a.ev, tile, grid);
+        stamp(a.ts, it, 2);
         // ---- S: ev2 = K ev ----
         spmv_phase<TF>(a, a.ev, a.ev2, grid);
+        stamp(a.ts, it, 3);
         // ---- L: Av = U'^-1 P' ev2, beta dots ----
         double bd[2] = {0.0, 0.0};
         utsweep<TF>(a, a.ev2, a.Av, a.w[k0], a.v[k0], bd, tile, grid, false);
         grid_allsum<2>(bd, a.partials, red, sh, grid);
+        stamp(a.ts, it, 4);
         {
             const double bt = bd[0] / bd[1];
             S.beta[k1] = bt;
@@ -442,6 +463,7 @@ __global__ void __launch_bounds__(kT) k_sqmr_persistent(PArgs<TF> a)
             ad[1] = r3[2];
             S.norm_x = sqrt(r3[0]);
         }
+        stamp(a.ts, it, 5);
         S.gamma = S.s[k1] * S.gamma;
         S.test0 |= (fabs(S.delta[k1]) <= a.tol);
         S.test1 |= (S.gamma / fma_rn(S.norm_A, S.norm_x, S.norm_pb) <= a.tol);
@@ -540,6 +562,13 @@ int launch_persistent(culipx_handle_t* h, Csr* A, Factor* M, const double* b, do
     a.b = b;
     a.partials = w->partials.as<double>();
     a.out = base + (size_t)13 * n;
+    a.ts = nullptr;
+    if (w->profile) {
+        if (w->ts.bytes() < (size_t)kTsIters * 8 * sizeof(unsigned long long))
+            CULIPX_TRY(w->ts.alloc(h, (size_t)kTsIters * 8 * sizeof(unsigned long long)));
+        CULIPX_CUDA(cudaMemsetAsync(w->ts.get(), 0, (size_t)kTsIters * 8 * sizeof(unsigned long long), s));
+        a.ts = w->ts.as<unsigned long long>();
+    }
     CULIPX_CUDA(cudaMemsetAsync(base, 0, (size_t)13 * n * sizeof(double), s));
     CULIPX_CUDA(cudaMemsetAsync(x, 0, (size_t)n * sizeof(double), s));
     void* args[] = {&a};
@@ -683,6 +712,7 @@ int launch_noalloc(culipx_handle_t* h, Csr* A, Factor* M, const double* b, doubl
     a.ev2 = base + (size_t)12 * n;
     a.out = base + (size_t)13 * n;
     a.partials = base + kNoAllocVecs;
+    a.ts = nullptr;
     a.x = x;
     a.b = b;
     // the scratch keeps the previous call's contents: clear the recurrence vectors

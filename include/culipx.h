@@ -172,6 +172,15 @@ int culipx_spmv(culipx_csr A, const void *d_x, void *d_y, double alpha, double b
 int culipx_sqmr_solve(culipx_handle h, culipx_csr A, culipx_factor M, const double *d_b,
                       double *d_x, double tol, int max_it, double *residual, int *iterations);
 
+/* Per-phase device timing of the persistent solver (no counterpart in the
+ * reference, which has wall-clock timers only, libs/utils/defines.h:65-85):
+ * enable, solve, then read for each of the first min(iterations, 64)
+ * iterations six values in microseconds: v+ and its norm, U sweep, SpMV,
+ * U' sweep with beta's dots, the x / p / w update with the next alpha's
+ * dots, and the whole iteration. */
+int culipx_sqmr_profile(culipx_handle h, int enable);
+int culipx_sqmr_phase_times(culipx_handle h, double *out_us, int iterations);
+
 /* The same solve (same kernel, same results) without any device allocation;
  * no counterpart in the reference.  For callers that cannot allocate device
  * memory while they solve: processes whose GPU memory is already owned by
