@@ -337,13 +337,14 @@ CULIPX_API int culipx_sqmr_phase_times(culipx_handle h, double* out_us, int iter
     unsigned long long ts[64 * 8];
     CULIPX_CUDA(cudaStreamSynchronize(h->stream));
     CULIPX_CUDA(cudaMemcpy(ts, h->sqmr->ts.get(), sizeof(ts), cudaMemcpyDeviceToHost));
-    // per iteration: B (v+, ||v+||), U sweep, SpMV, U' sweep + beta, A (x, p, next alpha), total
+    // per iteration: P1 (v+, ||v+||, first U level), the other U levels, the
+    // U' levels with the fused SpMV and the dots, 0, 0, total
     for (int i = 0; i < its; ++i) {
         const unsigned long long* t = ts + i * 8;
-        const unsigned long long next = (i + 1 < 64 && ts[(i + 1) * 8]) ? ts[(i + 1) * 8] : t[5];
-        const double d[6] = {(t[1] - t[0]) * 1e-3, (t[2] - t[1]) * 1e-3, (t[3] - t[2]) * 1e-3,
-                             (t[4] - t[3]) * 1e-3, (t[5] - t[4]) * 1e-3, (next - t[0]) * 1e-3};
-        for (int k = 0; k < 6; ++k) out_us[i * 6 + k] = t[5] ? d[k] : 0.0;
+        const unsigned long long next = (i + 1 < 64 && ts[(i + 1) * 8]) ? ts[(i + 1) * 8] : t[3];
+        const double d[6] = {(t[1] - t[0]) * 1e-3, (t[2] - t[1]) * 1e-3, (t[3] - t[2]) * 1e-3, 0.0, 0.0,
+                             (next - t[0]) * 1e-3};
+        for (int k = 0; k < 6; ++k) out_us[i * 6 + k] = t[3] ? d[k] : 0.0;
     }
     return CULIPX_OK;
 }

@@ -43,7 +43,6 @@ constexpr int kWarps = 4;  // blocks per CTA
 enum StateSlot { kStErr = 0, kStLeftover = 1, kStArena = 2, kStDeferred = 3, kStLevelAcc = 4, kStSlow = 5 };
 
 // per block row flags set by the pivot kernel
-enum RowFlags { kRowIdentity = 1, kRowHas2x2 = 2, kRowPermIdentity = 4, kRowNoUpdates = 8 };
 enum ErrBits { kErrLeftoverNegative = 1 };
 
 enum OffdiagMode { kFirst = 0, kCount = 1, kWrite = 2 };
@@ -807,6 +806,19 @@ int factor_create(Pattern* p, Factor** out)
     al(f->ut_val, off_slots * f->vbytes);
     al(f->piv_off, cm * sizeof(long long));
     al(f->work, (size_t)n * f->vbytes);
+    {
+        // packed pivot tile triangles: h_I (h_I + 1) / 2 slots per block row
+        std::vector<long long> pko(cm + 1, 0);
+        for (int I = 0; I < cm; ++I) {
+            const long long hI = p->bs[I + 1] - p->bs[I];
+            pko[I + 1] = pko[I] + hI * (hI + 1) / 2;
+        }
+        if (st == CULIPX_OK) st = f->pk_off.upload(h, pko.data(), (cm + 1) * sizeof(long long));
+        al(f->pk_col, (size_t)pko[cm] * f->vbytes);
+        al(f->pk_row, (size_t)pko[cm] * f->vbytes);
+    }
+    al(f->u_colp, off_slots * sizeof(int));
+    al(f->dg, ((size_t)n + 32) * f->vbytes);
     if (st != CULIPX_OK) { delete f; return st; }
     *out = f;
     return CULIPX_OK;

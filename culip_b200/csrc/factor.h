@@ -6,6 +6,14 @@
 
 namespace culipx {
 
+// per block row flags written by the factor's pivot kernel
+enum RowFlags : int {
+    kRowIdentity = 1,      // the factored pivot tile is exactly the identity
+    kRowHas2x2 = 2,        // D has a 2x2 pivot in this block row
+    kRowPermIdentity = 4,  // no pivot swaps inside the tile
+    kRowNoUpdates = 8,     // the pivot block received no Schur updates
+};
+
 struct Factor {
     Pattern* pat = nullptr;
     int precision = CULIPX_F64;
@@ -34,6 +42,13 @@ struct Factor {
     DeviceBuffer u_off, u_col, u_val;    // rows of U
     DeviceBuffer ut_off, ut_col, ut_val; // rows of U' (columns of U)
     DeviceBuffer piv_off;                // per block row: value slot of its pivot tile
+    // the persistent solver's copies: upper triangles of the non-identity
+    // pivot tiles packed column by column (U sweep) and row by row (U'
+    // sweep), h(h+1)/2 slots per block row at pk_off; the U columns mapped
+    // through the pivot permutation; the diagonal of D
+    DeviceBuffer pk_col, pk_row, pk_off;
+    DeviceBuffer u_colp;
+    DeviceBuffer dg;
     DeviceBuffer work;                   // n values of apply scratch
     DeviceBuffer scan_tmp;               // scan partial sums
     long long u_nnz = 0;

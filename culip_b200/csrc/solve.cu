@@ -21,6 +21,8 @@
 #include "kernels_common.cuh"
 #include "block_io.cuh"
 
+#include <algorithm>
+
 namespace culipx {
 
 namespace {
@@ -232,6 +234,51 @@ __global__ void k_pivot_offsets(int cm, const int* csc_off, const int* csc_blk, 
         piv_off[I] = boff[csc_blk[csc_off[I + 1] - 1]];
 }
 
+// Upper triangle of each non-identity pivot tile, packed twice: column by
+// column (U[r][c] at c(c+1)/2 + r; the U sweep's back substitution reads one
+// column per step) and row by row (U[r][c] at r h - r(r-1)/2 + c - r; the U'
+// sweep reads one row per step).  Both reads are coalesced, and together the
+// two copies take the room of one square tile.
+template <class T>
+__global__ void k_pack_tiles(int cm, const int* __restrict__ bs, const long long* __restrict__ piv_off,
+                             const int* __restrict__ rowflags, const T* __restrict__ val,
+                             const long long* __restrict__ pk_off, T* __restrict__ pk_col, T* __restrict__ pk_row)
+{
+    const int lane = lane_id();
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int I = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; I < cm; I += nw) {
+        if (rowflags[I] & kRowIdentity) continue;
+        const int h = bs[I + 1] - bs[I];
+        const T* P = val + piv_off[I];
+        T* pc = pk_col + pk_off[I];
+        T* pr = pk_row + pk_off[I];
+        for (int r = 0; r < h; ++r) {
+            const int c = lane;
+            if (c >= r && c < h) {
+                const T v = P[r * h + c];
+                pc[c * (c + 1) / 2 + r] = v;
+                pr[r * h - r * (r - 1) / 2 + c - r] = v;
+            }
+        }
+    }
+}
+
+// U's column indices mapped through the pivot permutation (the persistent
+// solver gathers the finished U-sweep values from P t directly), and the
+// diagonal of D
+template <class T>
+__global__ void k_sweep_extras(const int* __restrict__ u_off, const int* __restrict__ u_col,
+                               const int* __restrict__ perm, int* __restrict__ u_colp, int n,
+                               const T* __restrict__ tri, T* __restrict__ dg)
+{
+    const long long nu = u_off[n];
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nu; k += stride)
+        u_colp[k] = perm[u_col[k]];
+    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < n; g += stride)
+        dg[g] = tri[3 * g + 1];
+}
+
 // ---------------------------------------------------------------------------
 // one level of the U (UPPER) or U' sweep, in place on x
 template <class T, bool UPPER>
@@ -352,7 +399,12 @@ int build_sweeps_t(Factor* f, cudaStream_t s, int* launches)
     k_fill_u_rows<T><<<grid, 32 * kSweepWarps, 0, s>>>(a, val, cm, u_off, f->u_col.as<int>(), f->u_val.as<T>());
     k_fill_ut_rows<T><<<grid, 32 * kSweepWarps, 0, s>>>(a, val, cm, ut_off, f->ut_col.as<int>(), f->ut_val.as<T>());
     k_pivot_offsets<<<(cm + 255) / 256, 256, 0, s>>>(cm, a.csc_off, a.csc_blk, a.boff, f->piv_off.as<long long>());
-    *launches += 3;
+    k_pack_tiles<T><<<std::min((cm + 7) / 8, 148 * 8), 256, 0, s>>>(
+        cm, a.bs, f->piv_off.as<long long>(), f->rowflags.as<int>(), val, f->pk_off.as<long long>(),
+        f->pk_col.as<T>(), f->pk_row.as<T>());
+    k_sweep_extras<T><<<148 * 4, 256, 0, s>>>(u_off, f->u_col.as<int>(), f->perm.as<int>(), f->u_colp.as<int>(), n,
+                                              f->tri.as<T>(), f->dg.as<T>());
+    *launches += 5;
     return launch_check("build_sweeps");
 }
 

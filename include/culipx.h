@@ -175,9 +175,10 @@ int culipx_sqmr_solve(culipx_handle h, culipx_csr A, culipx_factor M, const doub
 /* Per-phase device timing of the persistent solver (no counterpart in the
  * reference, which has wall-clock timers only, libs/utils/defines.h:65-85):
  * enable, solve, then read for each of the first min(iterations, 64)
- * iterations six values in microseconds: v+ and its norm, U sweep, SpMV,
- * U' sweep with beta's dots, the x / p / w update with the next alpha's
- * dots, and the whole iteration. */
+ * iterations six values in microseconds: phase 1 (v+, its norm and the
+ * first U-sweep level), the other U-sweep levels, the U'-sweep levels with
+ * the fused SpMV, beta's and alpha's dots and the p / x update, two unused
+ * slots (0), and the whole iteration. */
 int culipx_sqmr_profile(culipx_handle h, int enable);
 int culipx_sqmr_phase_times(culipx_handle h, double *out_us, int iterations);
 
@@ -189,7 +190,7 @@ int culipx_sqmr_phase_times(culipx_handle h, double *out_us, int iterations);
  * cudaMalloc / cudaFree could synchronize the device.  M must be a computed
  * factor (FP64 or FP32); n must not exceed 65536 (larger n is rejected with
  * CULIPX_INVALID_ARG).  The work vectors live in a fixed scratch array
- * compiled into the library (about 7.4 MB, held by every GPU that loads the
+ * compiled into the library (about 5.3 MB, held by every GPU that loads the
  * library until the process exits); it is shared by all calls and keeps the
  * last call's contents, so calls whose work overlaps on the GPU race.  The
  * first call on a device looks up the scratch's device address; make it
