@@ -338,12 +338,15 @@ CULIPX_API int culipx_sqmr_phase_times(culipx_handle h, double* out_us, int iter
     CULIPX_CUDA(cudaStreamSynchronize(h->stream));
     CULIPX_CUDA(cudaMemcpy(ts, h->sqmr->ts.get(), sizeof(ts), cudaMemcpyDeviceToHost));
     // per iteration: P1 (v+, ||v+||, first U level), the other U levels, the
-    // U' levels with the fused SpMV and the dots, 0, 0, total
+    // first U' level (with the p / x update), the other U' levels with the
+    // final reduction, 0, total; stamps: 0 start, 1 after P1, 2 after P2,
+    // 4 after the first U' level (if there are two or more), 3 end
     for (int i = 0; i < its; ++i) {
         const unsigned long long* t = ts + i * 8;
         const unsigned long long next = (i + 1 < 64 && ts[(i + 1) * 8]) ? ts[(i + 1) * 8] : t[3];
-        const double d[6] = {(t[1] - t[0]) * 1e-3, (t[2] - t[1]) * 1e-3, (t[3] - t[2]) * 1e-3, 0.0, 0.0,
-                             (next - t[0]) * 1e-3};
+        const unsigned long long mid = t[4] ? t[4] : t[3];
+        const double d[6] = {(t[1] - t[0]) * 1e-3, (t[2] - t[1]) * 1e-3, (mid - t[2]) * 1e-3,
+                             (t[3] - mid) * 1e-3, 0.0, (next - t[0]) * 1e-3};
         for (int k = 0; k < 6; ++k) out_us[i * 6 + k] = t[3] ? d[k] : 0.0;
     }
     return CULIPX_OK;

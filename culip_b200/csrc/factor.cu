@@ -817,6 +817,7 @@ int factor_create(Pattern* p, Factor** out)
         al(f->pk_col, (size_t)pko[cm] * f->vbytes);
         al(f->pk_row, (size_t)pko[cm] * f->vbytes);
     }
+    al(f->ndmask, cm * sizeof(unsigned));
     al(f->u_colp, off_slots * sizeof(int));
     al(f->dg, ((size_t)n + 32) * f->vbytes);
     if (st != CULIPX_OK) { delete f; return st; }

@@ -47,6 +47,7 @@ struct Factor {
     // sweep), h(h+1)/2 slots per block row at pk_off; the U columns mapped
     // through the pivot permutation; the diagonal of D
     DeviceBuffer pk_col, pk_row, pk_off;
+    DeviceBuffer ndmask;  // per block row: bit r set if U_rr != 1 in its pivot tile
     DeviceBuffer u_colp;
     DeviceBuffer dg;
     DeviceBuffer work;                   // n values of apply scratch

@@ -238,11 +238,14 @@ __global__ void k_pivot_offsets(int cm, const int* csc_off, const int* csc_blk, 
 // column (U[r][c] at c(c+1)/2 + r; the U sweep's back substitution reads one
 // column per step) and row by row (U[r][c] at r h - r(r-1)/2 + c - r; the U'
 // sweep reads one row per step).  Both reads are coalesced, and together the
-// two copies take the room of one square tile.
+// two copies take the room of one square tile.  ndmask[I] marks the diagonal
+// entries that are not exactly 1 (only the first row of a 2x2 pivot can be):
+// the substitutions divide only there, x / 1 being x.
 template <class T>
 __global__ void k_pack_tiles(int cm, const int* __restrict__ bs, const long long* __restrict__ piv_off,
                              const int* __restrict__ rowflags, const T* __restrict__ val,
-                             const long long* __restrict__ pk_off, T* __restrict__ pk_col, T* __restrict__ pk_row)
+                             const long long* __restrict__ pk_off, T* __restrict__ pk_col, T* __restrict__ pk_row,
+                             unsigned* __restrict__ ndmask)
 {
     const int lane = lane_id();
     const int nw = (gridDim.x * blockDim.x) >> 5;
@@ -250,6 +253,8 @@ __global__ void k_pack_tiles(int cm, const int* __restrict__ bs, const long long
         if (rowflags[I] & kRowIdentity) continue;
         const int h = bs[I + 1] - bs[I];
         const T* P = val + piv_off[I];
+        const unsigned nd = __ballot_sync(0xffffffffu, (int)lane < h && P[lane * h + lane] != T(1));
+        if (lane == 0) ndmask[I] = nd;
         T* pc = pk_col + pk_off[I];
         T* pr = pk_row + pk_off[I];
         for (int r = 0; r < h; ++r) {
@@ -401,7 +406,7 @@ int build_sweeps_t(Factor* f, cudaStream_t s, int* launches)
     k_pivot_offsets<<<(cm + 255) / 256, 256, 0, s>>>(cm, a.csc_off, a.csc_blk, a.boff, f->piv_off.as<long long>());
     k_pack_tiles<T><<<std::min((cm + 7) / 8, 148 * 8), 256, 0, s>>>(
         cm, a.bs, f->piv_off.as<long long>(), f->rowflags.as<int>(), val, f->pk_off.as<long long>(),
-        f->pk_col.as<T>(), f->pk_row.as<T>());
+        f->pk_col.as<T>(), f->pk_row.as<T>(), f->ndmask.as<unsigned>());
     k_sweep_extras<T><<<148 * 4, 256, 0, s>>>(u_off, f->u_col.as<int>(), f->perm.as<int>(), f->u_colp.as<int>(), n,
                                               f->tri.as<T>(), f->dg.as<T>());
     *launches += 5;

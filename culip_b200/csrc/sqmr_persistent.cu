@@ -82,6 +82,7 @@ struct PArgs {
     const TF* pk_col;          // pivot tile upper triangles, column by column
     const TF* pk_row;          // the same, row by row
     const long long* pk_off;   // per block row
+    const unsigned* ndmask;    // per block row: non-unit diagonal entries of the pivot tile
     const TF* dg;              // diagonal of D
     const TF* tri;
     const int* is_piv;
@@ -280,13 +281,13 @@ __device__ __forceinline__ double spmv_row(const PArgs<TF>& a, int q, const doub
 // Back substitution with the block row's pivot tile, upper triangle packed
 // column by column (U sweep; d_left_solve_row_major,
 // block_ildlt_kernels.impl.cuh:2087-2113): for c = h-1 .. 0:
-// x_c = t_c / U_cc, t_r -= U_rc x_c (r < c).  A unit diagonal entry skips
-// the division (t / 1 == t exactly).
-template <class TF>
-__device__ __forceinline__ double tile_upper(double in, const TF* __restrict__ P, int h)
+// x_c = t_c / U_cc, t_r -= U_rc x_c (r < c).  The division is taken only
+// where bit c of nd says U_cc != 1 (t / 1 == t exactly); with nd == 0 the
+// chain is shuffle + fma per step.
+template <class TF, bool DIV>
+__device__ __forceinline__ TF tile_upper_t(TF t, const TF* __restrict__ P, int h, unsigned nd)
 {
     const int lane = (int)lane_id();
-    TF t = (TF)in;
     for (int c0 = h - 1; c0 >= 0; c0 -= kBatch) {
         TF u[kBatch];
 #pragma unroll
@@ -298,22 +299,30 @@ __device__ __forceinline__ double tile_upper(double in, const TF* __restrict__ P
         for (int j = 0; j < kBatch; ++j) {
             const int c = c0 - j;
             if (c >= 0) {
-                if (lane == c && u[j] != TF(1)) t = t / u[j];
+                if (DIV && ((nd >> c) & 1u)) {
+                    if (lane == c) t = t / u[j];
+                }
                 const TF xc = __shfl_sync(kFull, t, c);
                 if (lane < c) t = fma_rn(-u[j], xc, t);
             }
         }
     }
-    return (double)t;
+    return t;
+}
+
+template <class TF>
+__device__ __forceinline__ double tile_upper(double in, const TF* __restrict__ P, int h, unsigned nd)
+{
+    return (double)(nd ? tile_upper_t<TF, true>((TF)in, P, h, nd) : tile_upper_t<TF, false>((TF)in, P, h, 0u));
 }
 
 // Forward substitution with the upper triangle packed row by row (U'
-// sweep): for r = 0 .. h-1: x_r = t_r / U_rr, t_c -= U_rc x_r (r < c < h)
-template <class TF>
-__device__ __forceinline__ double tile_lower(double in, const TF* __restrict__ P, int h)
+// sweep): for r = 0 .. h-1: x_r = t_r / U_rr, t_c -= U_rc x_r (r < c < h);
+// divisions as in tile_upper_t
+template <class TF, bool DIV>
+__device__ __forceinline__ TF tile_lower_t(TF t, const TF* __restrict__ P, int h, unsigned nd)
 {
     const int lane = (int)lane_id();
-    TF t = (TF)in;
     for (int r0 = 0; r0 < h; r0 += kBatch) {
         TF u[kBatch];
 #pragma unroll
@@ -325,13 +334,21 @@ __device__ __forceinline__ double tile_lower(double in, const TF* __restrict__ P
         for (int j = 0; j < kBatch; ++j) {
             const int r = r0 + j;
             if (r < h) {
-                if (lane == r && u[j] != TF(1)) t = t / u[j];
+                if (DIV && ((nd >> r) & 1u)) {
+                    if (lane == r) t = t / u[j];
+                }
                 const TF xr = __shfl_sync(kFull, t, r);
                 if (lane > r && lane < h) t = fma_rn(-u[j], xr, t);
             }
         }
     }
-    return (double)t;
+    return t;
+}
+
+template <class TF>
+__device__ __forceinline__ double tile_lower(double in, const TF* __restrict__ P, int h, unsigned nd)
+{
+    return (double)(nd ? tile_lower_t<TF, true>((TF)in, P, h, nd) : tile_lower_t<TF, false>((TF)in, P, h, 0u));
 }
 
 // One U-sweep work item: block row I (rows fr .. fr+h-1), lane's right-hand
@@ -350,7 +367,7 @@ __device__ __forceinline__ double u_item(const PArgs<TF>& a, int I, int fr, int 
     if (lane < h)
         t = (double)row_sub<TF>((TF)d, __ldg(a.u_off + fr + lane), __ldg(a.u_off + fr + lane + 1), a.u_colp,
                                 a.u_val, out);
-    if (!(flags & kRowIdentity)) t = tile_upper<TF>(t, a.pk_col + __ldg(a.pk_off + I), h);
+    if (!(flags & kRowIdentity)) t = tile_upper<TF>(t, a.pk_col + __ldg(a.pk_off + I), h, __ldg(a.ndmask + I));
     if (lane < h) out[(flags & kRowPermIdentity) ? fr + lane : __ldg(a.perm + fr + lane)] = t;
     return d;
 }
@@ -370,7 +387,7 @@ __device__ __forceinline__ double ut_item(const PArgs<TF>& a, int I, int fr, int
         t = (double)row_sub<TF>((TF)y, __ldg(a.ut_off + fr + lane), __ldg(a.ut_off + fr + lane + 1), a.ut_col,
                                 a.ut_val, dst);
     }
-    if (!(flags & kRowIdentity)) t = tile_lower<TF>(t, a.pk_row + __ldg(a.pk_off + I), h);
+    if (!(flags & kRowIdentity)) t = tile_lower<TF>(t, a.pk_row + __ldg(a.pk_off + I), h, __ldg(a.ndmask + I));
     if (lane < h) dst[fr + lane] = t;
     return t;
 }
@@ -600,7 +617,10 @@ __global__ void __launch_bounds__(kT, CTAS) k_sqmr_persistent(PArgs<TF> a)
                         r[2] = fma_rn(vs, dv, r[2]);
                     }
                 }
-                if (L < a.nl - 1) grid.sync();
+                if (L < a.nl - 1) {
+                    grid.sync();
+                    if (L == 0) stamp(a.ts, it, 4);
+                }
             }
             grid_reduce<4>(r, a.partials, red, sh, grid);
             if (tid == 0) {
@@ -680,6 +700,7 @@ PArgs<TF> make_args(Csr* A, Factor* M, double* base, double* partials, const dou
     a.pk_col = M->pk_col.as<TF>();
     a.pk_row = M->pk_row.as<TF>();
     a.pk_off = M->pk_off.as<long long>();
+    a.ndmask = M->ndmask.as<unsigned>();
     a.dg = M->dg.as<TF>();
     a.tri = M->tri.as<TF>();
     a.is_piv = M->is_piv.as<int>();

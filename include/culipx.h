@@ -176,9 +176,10 @@ int culipx_sqmr_solve(culipx_handle h, culipx_csr A, culipx_factor M, const doub
  * reference, which has wall-clock timers only, libs/utils/defines.h:65-85):
  * enable, solve, then read for each of the first min(iterations, 64)
  * iterations six values in microseconds: phase 1 (v+, its norm and the
- * first U-sweep level), the other U-sweep levels, the U'-sweep levels with
- * the fused SpMV, beta's and alpha's dots and the p / x update, two unused
- * slots (0), and the whole iteration. */
+ * first U-sweep level), the other U-sweep levels, the first U'-sweep level
+ * (with the fused SpMV, the dots and the p / x update), the other U'-sweep
+ * levels with the final reduction, an unused slot (0), and the whole
+ * iteration. */
 int culipx_sqmr_profile(culipx_handle h, int enable);
 int culipx_sqmr_phase_times(culipx_handle h, double *out_us, int iterations);
 
