@@ -807,17 +807,23 @@ int factor_create(Pattern* p, Factor** out)
     al(f->piv_off, cm * sizeof(long long));
     al(f->work, (size_t)n * f->vbytes);
     {
-        // packed pivot tile triangles: h_I (h_I + 1) / 2 slots per block row
+        // packed pivot tile triangles: h_I (h_I + 1) / 2 slots per block row,
+        // rounded up to 4 slots so that every tile starts on a 16-byte
+        // boundary (16-byte asynchronous copies into shared memory)
         std::vector<long long> pko(cm + 1, 0);
         for (int I = 0; I < cm; ++I) {
             const long long hI = p->bs[I + 1] - p->bs[I];
-            pko[I + 1] = pko[I] + hI * (hI + 1) / 2;
+            pko[I + 1] = pko[I] + (hI * (hI + 1) / 2 + 3) / 4 * 4;
         }
         if (st == CULIPX_OK) st = f->pk_off.upload(h, pko.data(), (cm + 1) * sizeof(long long));
         al(f->pk_col, (size_t)pko[cm] * f->vbytes);
         al(f->pk_row, (size_t)pko[cm] * f->vbytes);
     }
     al(f->ndmask, cm * sizeof(unsigned));
+    al(f->scan_s, (cm + 1) * sizeof(int));
+    al(f->scan_c, (cm + 1) * sizeof(int));
+    al(f->simple_rows, (size_t)n * sizeof(int));
+    al(f->cplx, cm * sizeof(int));
     al(f->u_colp, off_slots * sizeof(int));
     al(f->dg, ((size_t)n + 32) * f->vbytes);
     if (st != CULIPX_OK) { delete f; return st; }

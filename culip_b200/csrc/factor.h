@@ -50,6 +50,12 @@ struct Factor {
     DeviceBuffer ndmask;  // per block row: bit r set if U_rr != 1 in its pivot tile
     DeviceBuffer u_colp;
     DeviceBuffer dg;
+    // each level's block rows split in level-list order into simple ones
+    // (identity pivot tile, no swaps, 1x1 pivots: every fine row is
+    // independent) and the others; scan_s / scan_c (num_blocks + 1) are the
+    // running counts of simple fine rows / other block rows, so level L owns
+    // simple_rows[scan_s[lvl_off[L]] ..) and cplx[scan_c[lvl_off[L]] ..)
+    DeviceBuffer scan_s, scan_c, simple_rows, cplx;
     DeviceBuffer work;                   // n values of apply scratch
     DeviceBuffer scan_tmp;               // scan partial sums
     long long u_nnz = 0;

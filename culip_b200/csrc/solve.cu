@@ -268,6 +268,47 @@ __global__ void k_pack_tiles(int cm, const int* __restrict__ bs, const long long
     }
 }
 
+// Simple block rows: identity pivot tile, no swaps, 1x1 pivots only.  Their
+// fine rows are independent in both sweeps.
+__device__ __forceinline__ bool simple_block(int flags)
+{
+    return (flags & (kRowIdentity | kRowPermIdentity | kRowHas2x2)) == (kRowIdentity | kRowPermIdentity);
+}
+
+// per level-list position q: fine rows of a simple block / 1 for another block
+__global__ void k_split_count(int cm, const int* __restrict__ lvl_rows, const int* __restrict__ bs,
+                              const int* __restrict__ rowflags, int* __restrict__ cnt_s, int* __restrict__ cnt_c)
+{
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q <= cm; q += gridDim.x * blockDim.x) {
+        if (q == cm) {
+            cnt_s[q] = 0;
+            cnt_c[q] = 0;
+            continue;
+        }
+        const int I = lvl_rows[q];
+        const bool simple = simple_block(rowflags[I]);
+        cnt_s[q] = simple ? bs[I + 1] - bs[I] : 0;
+        cnt_c[q] = simple ? 0 : 1;
+    }
+}
+
+// after the exclusive scans: the simple fine rows and the other block rows,
+// both in level-list order
+__global__ void k_split_fill(int cm, const int* __restrict__ lvl_rows, const int* __restrict__ bs,
+                             const int* __restrict__ rowflags, const int* __restrict__ scan_s,
+                             const int* __restrict__ scan_c, int* __restrict__ simple_rows, int* __restrict__ cplx)
+{
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < cm; q += gridDim.x * blockDim.x) {
+        const int I = lvl_rows[q];
+        if (simple_block(rowflags[I])) {
+            const int fr = bs[I], h = bs[I + 1] - fr;
+            for (int r = 0; r < h; ++r) simple_rows[scan_s[q] + r] = fr + r;
+        } else {
+            cplx[scan_c[q]] = I;
+        }
+    }
+}
+
 // U's column indices mapped through the pivot permutation (the persistent
 // solver gathers the finished U-sweep values from P t directly), and the
 // diagonal of D
@@ -409,7 +450,17 @@ int build_sweeps_t(Factor* f, cudaStream_t s, int* launches)
         f->pk_col.as<T>(), f->pk_row.as<T>(), f->ndmask.as<unsigned>());
     k_sweep_extras<T><<<148 * 4, 256, 0, s>>>(u_off, f->u_col.as<int>(), f->perm.as<int>(), f->u_colp.as<int>(), n,
                                               f->tri.as<T>(), f->dg.as<T>());
-    *launches += 5;
+    const int* lvl_rows = p.d_lvl_rows.as<int>();
+    const int* rowflags = f->rowflags.as<int>();
+    k_split_count<<<std::min(cm / 256 + 1, 148 * 4), 256, 0, s>>>(cm, lvl_rows, a.bs, rowflags, f->scan_s.as<int>(),
+                                                                  f->scan_c.as<int>());
+    *launches += 6;
+    CULIPX_TRY(exclusive_scan(f->scan_s.as<int>(), cm + 1, f->scan_tmp, p.handle, s, launches));
+    CULIPX_TRY(exclusive_scan(f->scan_c.as<int>(), cm + 1, f->scan_tmp, p.handle, s, launches));
+    k_split_fill<<<std::min(cm / 256 + 1, 148 * 4), 256, 0, s>>>(cm, lvl_rows, a.bs, rowflags, f->scan_s.as<int>(),
+                                                                 f->scan_c.as<int>(), f->simple_rows.as<int>(),
+                                                                 f->cplx.as<int>());
+    *launches += 1;
     return launch_check("build_sweeps");
 }
 

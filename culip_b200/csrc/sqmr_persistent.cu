@@ -69,7 +69,7 @@ constexpr int kW = kT / 32;      // warps per CTA
 constexpr int kCtasPerSm = 2;    // 32 resident warps per SM
 constexpr int kMaxNV = 4;        // values per grid reduction
 constexpr int kBatch = 8;        // loads issued ahead in row sums and tile solves
-constexpr int kVecs = 9;         // work vectors of n doubles
+constexpr int kVecs = 7;         // work vectors of n doubles
 constexpr unsigned kFull = 0xffffffffu;
 
 template <class TF>
@@ -97,8 +97,12 @@ struct PArgs {
     const int* ut_col;
     const TF* ut_val;
     const int* rowflags;
-    double* v[3];
-    double* p[3];
+    const int* scan_s;         // simple / other block rows per level (factor.h)
+    const int* scan_c;
+    const int* simple_rows;
+    const int* cplx;
+    double* v[2];              // v_k and v_k-1, v_k+1 overwrites v_k-1 in place
+    double* p[2];              // p_k-1 and p_k-2, p_k overwrites p_k-2 in place
     double* Av;
     double* ev;    // P U^-1 D^-1 (...)
     double* tmp;
@@ -285,7 +289,7 @@ __device__ __forceinline__ double spmv_row(const PArgs<TF>& a, int q, const doub
 // where bit c of nd says U_cc != 1 (t / 1 == t exactly); with nd == 0 the
 // chain is shuffle + fma per step.
 template <class TF, bool DIV>
-__device__ __forceinline__ TF tile_upper_t(TF t, const TF* __restrict__ P, int h, unsigned nd)
+__device__ __forceinline__ TF tile_upper_t(TF t, const TF* P, int h, unsigned nd)
 {
     const int lane = (int)lane_id();
     for (int c0 = h - 1; c0 >= 0; c0 -= kBatch) {
@@ -293,7 +297,7 @@ __device__ __forceinline__ TF tile_upper_t(TF t, const TF* __restrict__ P, int h
 #pragma unroll
         for (int j = 0; j < kBatch; ++j) {
             const int c = c0 - j;
-            u[j] = (c >= 0 && lane <= c) ? __ldg(P + c * (c + 1) / 2 + lane) : TF(0);
+            u[j] = (c >= 0 && lane <= c) ? P[c * (c + 1) / 2 + lane] : TF(0);
         }
 #pragma unroll
         for (int j = 0; j < kBatch; ++j) {
@@ -311,7 +315,7 @@ __device__ __forceinline__ TF tile_upper_t(TF t, const TF* __restrict__ P, int h
 }
 
 template <class TF>
-__device__ __forceinline__ double tile_upper(double in, const TF* __restrict__ P, int h, unsigned nd)
+__device__ __forceinline__ double tile_upper(double in, const TF* P, int h, unsigned nd)
 {
     return (double)(nd ? tile_upper_t<TF, true>((TF)in, P, h, nd) : tile_upper_t<TF, false>((TF)in, P, h, 0u));
 }
@@ -320,7 +324,7 @@ __device__ __forceinline__ double tile_upper(double in, const TF* __restrict__ P
 // sweep): for r = 0 .. h-1: x_r = t_r / U_rr, t_c -= U_rc x_r (r < c < h);
 // divisions as in tile_upper_t
 template <class TF, bool DIV>
-__device__ __forceinline__ TF tile_lower_t(TF t, const TF* __restrict__ P, int h, unsigned nd)
+__device__ __forceinline__ TF tile_lower_t(TF t, const TF* P, int h, unsigned nd)
 {
     const int lane = (int)lane_id();
     for (int r0 = 0; r0 < h; r0 += kBatch) {
@@ -328,7 +332,7 @@ __device__ __forceinline__ TF tile_lower_t(TF t, const TF* __restrict__ P, int h
 #pragma unroll
         for (int j = 0; j < kBatch; ++j) {
             const int r = r0 + j;
-            u[j] = (r < h && lane >= r && lane < h) ? __ldg(P + r * h - r * (r - 1) / 2 + lane - r) : TF(0);
+            u[j] = (r < h && lane >= r && lane < h) ? P[r * h - r * (r - 1) / 2 + lane - r] : TF(0);
         }
 #pragma unroll
         for (int j = 0; j < kBatch; ++j) {
@@ -346,7 +350,7 @@ __device__ __forceinline__ TF tile_lower_t(TF t, const TF* __restrict__ P, int h
 }
 
 template <class TF>
-__device__ __forceinline__ double tile_lower(double in, const TF* __restrict__ P, int h, unsigned nd)
+__device__ __forceinline__ double tile_lower(double in, const TF* P, int h, unsigned nd)
 {
     return (double)(nd ? tile_lower_t<TF, true>((TF)in, P, h, nd) : tile_lower_t<TF, false>((TF)in, P, h, 0u));
 }
@@ -507,35 +511,52 @@ __global__ void __launch_bounds__(kT, CTAS) k_sqmr_persistent(PArgs<TF> a)
 
     int it = 0;
     while (!S.done && it < a.max_it) {
-        const int k0 = acc3(it), k1 = acc3(it + 1), km1 = acc3(it - 1), km2 = acc3(it - 2);
+        const int k0 = acc3(it), k1 = acc3(it + 1), km1 = acc3(it - 1);
         stamp(a.ts, it, 0);
         const double alpha = S.alpha_next, na = -alpha, nb = -S.beta[k0];
-        double* const vk1 = a.v[k1];
-        const double* const vk = a.v[k0];
-        const double* const vkm1 = a.v[km1];
-        // ---- P1: v+ (unscaled), ||v+||^2; U sweep of the last level ----
+        const double* const vk = a.v[it & 1];
+        double* const vk1 = a.v[(it + 1) & 1];
+        const double* const vkm1 = vk1;  // read, then overwritten element by element
+        // ---- U sweep on v+ = Av - alpha v - beta v- (each item computes and
+        //      stores its rows' v+, kept unscaled), ||v+||^2 ----
         {
             double r[1] = {0.0};
-            for (int g = g0; g < n; g += gstride) {
-                double v = a.Av[g];
-                v = fma_rn(na, vk[g], v);
-                v = fma_rn(nb, vkm1[g], v);
-                vk1[g] = v;
-                r[0] = fma_rn(v, v, r[0]);
-            }
-            const int L = a.nl - 1;
-            const int r0 = __ldg(a.lvl_off + L), nr = __ldg(a.lvl_off + L + 1) - r0;
-            for (int t = wid; t < nr; t += nwarps) {
-                const int I = __ldg(a.lvl_rows + r0 + t);
-                const int fr = __ldg(a.bs + I), h = __ldg(a.bs + I + 1) - fr;
-                double y = 0.0;
-                if (lane < h) {  // the same value the vector loop stores
-                    const int g = fr + lane;
-                    y = a.Av[g];
+            for (int L = a.nl - 1; L >= 0; --L) {
+                const int q0 = __ldg(a.lvl_off + L), q1 = __ldg(a.lvl_off + L + 1);
+                // block rows with a pivot tile, swaps or 2x2 pivots: warp per block row
+                const int c1 = __ldg(a.scan_c + q1);
+                for (int t = __ldg(a.scan_c + q0) + wid; t < c1; t += nwarps) {
+                    const int I = __ldg(a.cplx + t);
+                    const int fr = __ldg(a.bs + I), h = __ldg(a.bs + I + 1) - fr;
+                    double y = 0.0;
+                    if (lane < h) {
+                        const int g = fr + lane;
+                        y = a.Av[g];
+                        y = fma_rn(na, vk[g], y);
+                        y = fma_rn(nb, vkm1[g], y);
+                        vk1[g] = y;
+                        r[0] = fma_rn(y, y, r[0]);
+                    }
+                    u_item<TF>(a, I, fr, h, y, a.ev);
+                }
+                // rows of simple block rows: thread per row (u_item with D = d,
+                // an identity tile and no swaps)
+                const int s1 = __ldg(a.scan_s + q1);
+                for (int i = __ldg(a.scan_s + q0) + g0; i < s1; i += gstride) {
+                    const int g = __ldg(a.simple_rows + i);
+                    double y = a.Av[g];
                     y = fma_rn(na, vk[g], y);
                     y = fma_rn(nb, vkm1[g], y);
+                    vk1[g] = y;
+                    r[0] = fma_rn(y, y, r[0]);
+                    const double d = y / (double)__ldg(a.dg + g);
+                    a.ev[g] = (double)row_sub<TF>((TF)d, __ldg(a.u_off + g), __ldg(a.u_off + g + 1), a.u_colp, a.u_val,
+                                                  a.ev);
                 }
-                u_item<TF>(a, I, fr, h, y, a.ev);
+                if (L > 0) {
+                    grid.sync();
+                    if (L == a.nl - 1) stamp(a.ts, it, 1);
+                }
             }
             grid_reduce<1>(r, a.partials, red, sh, grid);
             if (tid == 0) {
@@ -561,43 +582,21 @@ __global__ void __launch_bounds__(kT, CTAS) k_sqmr_persistent(PArgs<TF> a)
             }
             __syncthreads();
         }
-        stamp(a.ts, it, 1);
-        // ---- P2: the remaining U-sweep levels ----
-        for (int L = a.nl - 2; L >= 0; --L) {
-            const int r0 = __ldg(a.lvl_off + L), nr = __ldg(a.lvl_off + L + 1) - r0;
-            for (int t = wid; t < nr; t += nwarps) {
-                const int I = __ldg(a.lvl_rows + r0 + t);
-                const int fr = __ldg(a.bs + I), h = __ldg(a.bs + I + 1) - fr;
-                const double y = (lane < h) ? vk1[fr + lane] : 0.0;
-                u_item<TF>(a, I, fr, h, y, a.ev);
-            }
-            grid.sync();
-        }
+        if (a.nl == 1) stamp(a.ts, it, 1);
         stamp(a.ts, it, 2);
         // ---- P3: U' sweep with the fused SpMV; beta's and alpha's dots; p, x ----
         {
             double r[4] = {0.0, 0.0, 0.0, 0.0};
             const double sc = S.inv_delta;
             const double nbrr = -S.beta_rr, ne = -S.epsilon, ir = S.inv_rho, tau = S.tau;
+            double* const pk = a.p[it & 1];
+            const double* const pkm1 = a.p[(it + 1) & 1];
+            const double* const pkm2 = pk;  // read, then overwritten element by element
             for (int L = 0; L < a.nl; ++L) {
-                if (L == 0) {
-                    double* const pk = a.p[k0];
-                    const double* const pkm1 = a.p[km1];
-                    const double* const pkm2 = a.p[km2];
-                    for (int g = g0; g < n; g += gstride) {
-                        double p = vk[g];
-                        p = fma_rn(nbrr, pkm1[g], p);
-                        p = fma_rn(ne, pkm2[g], p);
-                        p = p * ir;
-                        pk[g] = p;
-                        const double xv = fma_rn(tau, p, a.x[g]);
-                        a.x[g] = xv;
-                        r[3] = fma_rn(xv, xv, r[3]);
-                    }
-                }
-                const int r0 = __ldg(a.lvl_off + L), nr = __ldg(a.lvl_off + L + 1) - r0;
-                for (int t = wid; t < nr; t += nwarps) {
-                    const int I = __ldg(a.lvl_rows + r0 + t);
+                const int q0 = __ldg(a.lvl_off + L), q1 = __ldg(a.lvl_off + L + 1);
+                const int c1 = __ldg(a.scan_c + q1);
+                for (int t = __ldg(a.scan_c + q0) + wid; t < c1; t += nwarps) {
+                    const int I = __ldg(a.cplx + t);
                     const int fr = __ldg(a.bs + I), h = __ldg(a.bs + I + 1) - fr;
                     const int flags = __ldg(a.rowflags + I);
                     const double av = ut_item<TF, true>(a, I, fr, h, flags, a.ev, sc, a.Av);
@@ -607,6 +606,15 @@ __global__ void __launch_bounds__(kT, CTAS) k_sqmr_persistent(PArgs<TF> a)
                         vkr = vk[g];
                         vs = vk1[g] * sc;
                         vk1[g] = vs;
+                        // p_k = (v_k - beta_rr p_k-1 - epsilon p_k-2) / rho, x += tau p_k
+                        double p = vkr;
+                        p = fma_rn(nbrr, pkm1[g], p);
+                        p = fma_rn(ne, pkm2[g], p);
+                        p = p * ir;
+                        pk[g] = p;
+                        const double xv = fma_rn(tau, p, a.x[g]);
+                        a.x[g] = xv;
+                        r[3] = fma_rn(xv, xv, r[3]);
                     }
                     DBlock<TF> D;
                     D.load(a, fr, h, flags);
@@ -616,6 +624,30 @@ __global__ void __launch_bounds__(kT, CTAS) k_sqmr_persistent(PArgs<TF> a)
                         r[1] = fma_rn(vs, da, r[1]);
                         r[2] = fma_rn(vs, dv, r[2]);
                     }
+                }
+                const int s1 = __ldg(a.scan_s + q1);
+                for (int i = __ldg(a.scan_s + q0) + g0; i < s1; i += gstride) {
+                    const int g = __ldg(a.simple_rows + i);
+                    const double y = spmv_row(a, g, a.ev) * sc;
+                    const double av = (double)row_sub<TF>((TF)y, __ldg(a.ut_off + g), __ldg(a.ut_off + g + 1), a.ut_col,
+                                                          a.ut_val, a.Av);
+                    a.Av[g] = av;
+                    const double vkr = vk[g];
+                    const double vs = vk1[g] * sc;
+                    vk1[g] = vs;
+                    double p = vkr;
+                    p = fma_rn(nbrr, pkm1[g], p);
+                    p = fma_rn(ne, pkm2[g], p);
+                    p = p * ir;
+                    pk[g] = p;
+                    const double xv = fma_rn(tau, p, a.x[g]);
+                    a.x[g] = xv;
+                    r[3] = fma_rn(xv, xv, r[3]);
+                    const double dd = (double)__ldg(a.dg + g);
+                    const double da = av / dd, dv = vs / dd;
+                    r[0] = fma_rn(vkr, da, r[0]);
+                    r[1] = fma_rn(vs, da, r[1]);
+                    r[2] = fma_rn(vs, dv, r[2]);
                 }
                 if (L < a.nl - 1) {
                     grid.sync();
@@ -715,13 +747,17 @@ PArgs<TF> make_args(Csr* A, Factor* M, double* base, double* partials, const dou
     a.ut_col = M->ut_col.as<int>();
     a.ut_val = M->ut_val.as<TF>();
     a.rowflags = M->rowflags.as<int>();
-    for (int i = 0; i < 3; ++i) {
+    a.scan_s = M->scan_s.as<int>();
+    a.scan_c = M->scan_c.as<int>();
+    a.simple_rows = M->simple_rows.as<int>();
+    a.cplx = M->cplx.as<int>();
+    for (int i = 0; i < 2; ++i) {
         a.v[i] = base + (size_t)i * n;
-        a.p[i] = base + (size_t)(3 + i) * n;
+        a.p[i] = base + (size_t)(2 + i) * n;
     }
-    a.Av = base + (size_t)6 * n;
-    a.ev = base + (size_t)7 * n;
-    a.tmp = base + (size_t)8 * n;
+    a.Av = base + (size_t)4 * n;
+    a.ev = base + (size_t)5 * n;
+    a.tmp = base + (size_t)6 * n;
     a.out = base + (size_t)kVecs * n;
     a.partials = partials;
     a.ts = nullptr;
@@ -831,8 +867,8 @@ int sqmr_solve_persistent(culipx_handle_t* h, Csr* A, Factor* M, const double* b
 // fixed scratch area compiled into the library instead of the handle's
 // workspace.
 //
-// The scratch is a file-scope device array of kNoAllocMaxRows x 10 doubles
-// plus the per-CTA reduction slots (about 5.3 MB): every GPU that loads this
+// The scratch is a file-scope device array of kNoAllocMaxRows x 8 doubles
+// plus the per-CTA reduction slots (about 4.3 MB): every GPU that loads this
 // library holds it until the process exits.  All calls share it and it keeps
 // the last call's contents; the call clears what must start at zero.  Calls
 // whose work overlaps on the GPU (two streams, two host threads) race on it.

@@ -191,7 +191,7 @@ int culipx_sqmr_phase_times(culipx_handle h, double *out_us, int iterations);
  * cudaMalloc / cudaFree could synchronize the device.  M must be a computed
  * factor (FP64 or FP32); n must not exceed 65536 (larger n is rejected with
  * CULIPX_INVALID_ARG).  The work vectors live in a fixed scratch array
- * compiled into the library (about 5.3 MB, held by every GPU that loads the
+ * compiled into the library (about 4.3 MB, held by every GPU that loads the
  * library until the process exits); it is shared by all calls and keeps the
  * last call's contents, so calls whose work overlaps on the GPU race.  The
  * first call on a device looks up the scratch's device address; make it
