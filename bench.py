@@ -49,6 +49,7 @@ def _parse():
     ap.add_argument("--impl", default="culipx", choices=["culipx", "reference"])
     ap.add_argument("--config", default="scale", choices=["small", "scale"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--max-it", type=int, default=1000, help="SQMR iteration cap (1000 = the driver's setting)")
     return ap.parse_args()
 
 
@@ -163,10 +164,15 @@ def run_culipx(args):
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
     iters_seen = []
+    sq_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
 
-    def step():
+    def step(i=None):
         F.compute(d_v, None, cb.PIV_BK, 0.0)
-        res, its, st = cb.sqmr_solve(h, A, F, d_b, d_x, 1e-8, 1000)
+        if i is not None:
+            sq_ev[i][0].record(stream)
+        res, its, st = cb.sqmr_solve(h, A, F, d_b, d_x, 1e-8, args.max_it)
+        if i is not None:
+            sq_ev[i][1].record(stream)
         iters_seen.append(its)
         return res, its
 
@@ -184,7 +190,7 @@ def run_culipx(args):
     for i in range(args.steps):
         flush.fill_(float(i))
         evs[i][0].record(stream)
-        step()
+        step(i)
         evs[i][1].record(stream)
     torch.cuda.synchronize()
     ck = clocks.stop()
@@ -204,20 +210,9 @@ def run_culipx(args):
     K = sp.csr_matrix((v, ci, rp), shape=(N, N))
     relres = float(np.linalg.norm(b - K @ x) / np.linalg.norm(b))
 
-    # SpMV roofline: the operator's HBM-bound kernel, timed with events on the stream
-    y = torch.empty_like(d_x)
-    spmv_ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-    reps = 50
-    flush.fill_(0.0)
-    A.spmv(d_b, y)
-    torch.cuda.synchronize()
-    spmv_ev[0].record(stream)
-    for _ in range(reps):
-        A.spmv(d_b, y)
-    spmv_ev[1].record(stream)
-    torch.cuda.synchronize()
-    spmv_ms = spmv_ev[0].elapsed_time(spmv_ev[1]) / reps
-    spmv_bytes = nnz * (8 + 4) + 4 * (N + 1) + 8 * N + 8 * N
+    # roofline of the dominant kernel, the persistent SQMR launch (one per solve)
+    sq_ms = float(np.mean([a0.elapsed_time(b0) for a0, b0 in sq_ev]))
+    roof = sqmr_roofline(F.info(), N, nnz, int(np.median(iters_seen)), sq_ms)
 
     # e2e through the public API with host buffers
     hv = torch.from_numpy(v).pin_memory()
@@ -240,7 +235,7 @@ def run_culipx(args):
         d_v2.copy_(hv, non_blocking=True)
         d_b2.copy_(hb, non_blocking=True)
         F.compute(d_v2, None, cb.PIV_BK, 0.0)
-        cb.sqmr_solve(h, A2, F, d_b2, d_x, 1e-8, 1000)
+        cb.sqmr_solve(h, A2, F, d_b2, d_x, 1e-8, args.max_it)
         hx.copy_(d_x, non_blocking=True)
         e1.record(stream)
         torch.cuda.synchronize()
@@ -257,7 +252,8 @@ def run_culipx(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded KKT generator)",
-        "config": _config_dict(args.config, cfg, nnz, {"parallelism": f"replicas x{world} (independent KKT systems)"}),
+        "config": _config_dict(args.config, cfg, nnz, {"parallelism": f"replicas x{world} (independent KKT systems)",
+                                                        "max_it": args.max_it}),
         "sqmr_iterations": int(np.median(iters_seen)) if iters_seen else None,
         "true_relres": relres,
         "factor_ms": fac_ms,
@@ -265,11 +261,7 @@ def run_culipx(args):
         "clocks": ck,
         "e2e": {"value": world * e2e_steps / (e2e_total / 1e3), "unit": UNIT,
                 "h2d_bytes_per_step": int(nnz * 8 + N * 8), "d2h_bytes_per_step": int(N * 8)},
-        "roofline": {"kernel": "k_csr_spmv<double,8>", "bound": "hbm", "achieved": spmv_bytes / (spmv_ms * 1e-3) / 1e9,
-                     "peak": _peak_hbm(), "unit": "GB/s",
-                     "frac": spmv_bytes / (spmv_ms * 1e-3) / 1e9 / _peak_hbm(), "traffic": None,
-                     "algorithmic_bytes": int(spmv_bytes), "avg_launch_ms": spmv_ms,
-                     "note": "x (2.4 MB) is L2-resident; matrix streamed from HBM after a flush"},
+        "roofline": roof,
     }
     if rank == 0 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(args.config, rp, ci, v, bs, b, int(np.median(iters_seen)))
@@ -277,6 +269,38 @@ def run_culipx(args):
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(out), flush=True)
+
+
+def sqmr_roofline(info, N, nnz, its, launch_ms):
+    """Algorithmic bytes of one persistent SQMR launch (init, its iterations,
+    final solve) over its CUDA-event duration.  Per iteration:
+      B_spmv = nnz_K (8 + 4) + 4 (N + 1) + 8 N (x) + 8 N (y)
+      B_tri  = nnz_U (s + 4) + 4 (N + 1) + s * (upper-triangle entries of the
+               non-identity pivot tiles) + 2 * 8 N
+      B_D    = 3 N s + 2 * 8 N
+      B_iter = B_spmv + 2 B_tri + 2 B_D + 11 * 8 N
+    and the launch adds B_spmv + 4 B_tri for the initial sweeps and the final
+    x = P U^-1 D^-1 x~.  traffic: DRAM bytes per iteration from the ncu
+    summary profiles/sqmr_persistent_scale.txt, times the iterations."""
+    s = info["value_bytes"]
+    b_spmv = nnz * 12 + 4 * (N + 1) + 16 * N
+    b_tri = info["u_nnz"] * (s + 4) + 4 * (N + 1) + s * info["tile_entries"] + 16 * N
+    b_d = 3 * N * s + 16 * N
+    b_iter = b_spmv + 2 * b_tri + 2 * b_d + 11 * 8 * N
+    b_launch = its * b_iter + b_spmv + 4 * b_tri
+    achieved = b_launch / (launch_ms * 1e-3) / 1e9
+    peak = _peak_hbm()
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "sqmr_persistent_scale.txt")
+    if os.path.exists(prof):
+        for ln in open(prof):
+            if ln.startswith("dram_bytes_per_iteration"):
+                traffic = float(ln.split("=")[1]) * its
+    return {"kernel": "k_sqmr_persistent<double> (one cooperative launch per solve)", "bound": "hbm",
+            "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+            "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
+            "algorithmic_bytes": int(b_launch), "bytes_per_iteration": int(b_iter), "iterations": its,
+            "avg_launch_ms": launch_ms, "us_per_iteration": launch_ms * 1e3 / max(its, 1)}
 
 
 def _peak_hbm():
@@ -326,7 +350,7 @@ def run_reference(args):
         _, _, it = oracle.sqmr(rp, ci, v, b, F, 1e-8, 20)
         t2 = time.perf_counter()
         if iters_full is None:
-            iters_full = _reference_iterations(args.config)
+            iters_full = min(_reference_iterations(args.config), args.max_it)
         if i >= args.warmup:
             ms.append(((t1 - t0) + (t2 - t1) / 20 * iters_full) * 1e3)
     total = float(np.sum(ms))
@@ -334,7 +358,8 @@ def run_reference(args):
     out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
            "ms_per_step": total / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
            "dtype": "f64", "data": "synthetic (seeded KKT generator)", "impl": "reference",
-           "config": _config_dict(args.config, cfg, len(ci)),
+           "config": _config_dict(args.config, cfg, len(ci), {"parallelism": f"replicas x{world} (independent KKT systems)",
+                                                             "max_it": args.max_it}),
            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
                             "sample": f"per step: oracle factor (full) + 20 SQMR iterations scaled to {iters_full}"},
            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}

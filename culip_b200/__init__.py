@@ -198,6 +198,13 @@ class Factor:
         capi.call("culipx_factor_stats", self._h, ctypes.byref(ms), ctypes.byref(nl))
         return ms.value, nl.value
 
+    def info(self) -> dict:
+        """Sizes of the solve structures of the last computed factor."""
+        out = np.zeros(8, dtype=np.int64)
+        capi.call("culipx_factor_info", self._h, out.ctypes.data_as(ctypes.c_void_p))
+        keys = ["u_nnz", "tiles", "tile_entries", "simple_rows", "blocks_2x2", "value_bytes"]
+        return {k: int(v) for k, v in zip(keys, out)}
+
     def export(self) -> dict:
         tot = ctypes.c_longlong()
         capi.call("culipx_factor_export_size", self._h, ctypes.byref(tot))

@@ -63,6 +63,7 @@ _SIGS = {
     "culipx_factor_export_size": [vp, ctypes.POINTER(i64)],
     "culipx_factor_export": [vp] * 9,
     "culipx_factor_stats": [vp, ctypes.POINTER(f64), ctypes.POINTER(i32)],
+    "culipx_factor_info": [vp, vp],
     "culipx_prec_apply": [vp, i32, vp, vp],
     "culipx_csr_create": [vp, i32, i32, i64, vp, vp, vp, i32, i32, ctypes.POINTER(vp)],
     "culipx_csr_destroy": [vp],

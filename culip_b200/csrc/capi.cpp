@@ -256,6 +256,42 @@ CULIPX_API int culipx_factor_stats(culipx_factor f, double* ms, int* launches)
     return CULIPX_OK;
 }
 
+CULIPX_API int culipx_factor_info(culipx_factor f, long long* info8)
+{
+    if (!f || !info8) return fail(CULIPX_INVALID_ARG, "null argument");
+    if (!f->computed) return fail(CULIPX_INVALID_ARG, "culipx_factor_info: factor not computed");
+    GUARD_BEGIN
+    culipx_handle_t* h = f->pat->handle;
+    CULIPX_TRY(use_device(h));
+    const Pattern& p = *f->pat;
+    const int n = p.n, cm = p.num_blocks;
+    int u_nnz = 0, simple = 0;
+    std::vector<int> flags(cm);
+    CULIPX_CUDA(cudaStreamSynchronize(h->stream));
+    CULIPX_CUDA(cudaMemcpy(&u_nnz, f->u_off.as<int>() + n, sizeof(int), cudaMemcpyDeviceToHost));
+    CULIPX_CUDA(cudaMemcpy(&simple, f->scan_s.as<int>() + cm, sizeof(int), cudaMemcpyDeviceToHost));
+    if (cm) CULIPX_CUDA(cudaMemcpy(flags.data(), f->rowflags.get(), cm * sizeof(int), cudaMemcpyDeviceToHost));
+    long long tiles = 0, tile_slots = 0, two = 0;
+    for (int I = 0; I < cm; ++I) {
+        const long long hI = p.bs[I + 1] - p.bs[I];
+        if (!(flags[I] & kRowIdentity)) {
+            ++tiles;
+            tile_slots += hI * (hI + 1) / 2;
+        }
+        if (flags[I] & kRowHas2x2) ++two;
+    }
+    info8[0] = u_nnz;       // stored strictly off-diagonal entries of U (= of U')
+    info8[1] = tiles;       // block rows whose pivot tile is not the identity
+    info8[2] = tile_slots;  // upper-triangle entries of those tiles
+    info8[3] = simple;      // fine rows in simple block rows
+    info8[4] = two;         // block rows with a 2x2 pivot
+    info8[5] = f->vbytes;
+    info8[6] = 0;
+    info8[7] = 0;
+    return CULIPX_OK;
+    GUARD_END
+}
+
 CULIPX_API int culipx_prec_apply(culipx_factor f, int stage, const void* d_b, void* d_x)
 {
     if (!f) return fail(CULIPX_INVALID_ARG, "null factor");

@@ -148,6 +148,13 @@ int culipx_factor_export(culipx_factor f, int *h_blk_nnz, long long *h_blk_off, 
                          void *h_val, void *h_tri, int *h_is_piv, int *h_perm, int *h_got_extra);
 /* timing of the last culipx_factor_compute on the device (ms), and launches */
 int culipx_factor_stats(culipx_factor f, double *ms, int *launches);
+/* sizes of the last computed factor's solve structures (no counterpart in
+ * the reference; used for algorithmic-byte counts): info[0] stored strictly
+ * off-diagonal entries of U, [1] block rows with a non-identity pivot tile,
+ * [2] upper-triangle entries of those tiles, [3] fine rows of simple block
+ * rows (identity tile, no swaps, 1x1 pivots), [4] block rows with a 2x2
+ * pivot, [5] bytes per value, [6..7] 0 */
+int culipx_factor_info(culipx_factor f, long long *info8);
 
 /* Preconditioner applies; b and x are device vectors of n values in the
  * factor's precision (b == x allowed for MIDDLE). */
