@@ -48,6 +48,21 @@ def _dptr(t) -> ctypes.c_void_p:
     return ctypes.c_void_p(t.data_ptr())
 
 
+def _release(obj, destroy: str):
+    """Destroys obj's C handle once; a no-op while the interpreter shuts down
+    (module globals may already be gone then)."""
+    h = getattr(obj, "_h", None)
+    if h is None or not h.value:
+        return
+    try:
+        lib = capi._lib
+        if lib is not None:
+            getattr(lib, destroy)(h)
+    except Exception:
+        pass
+    obj._h = None
+
+
 def kkt_generate(n, m, nnz_per_col, band_half, hmin, hmax, delta=1e-8, gamma=1e-8, seed=SEED):
     """Seeded KKT system as full symmetric CSR (rowptr, colidx, val) numpy arrays."""
     spec = KktSpec(n, m, nnz_per_col, band_half, hmin, hmax, delta, gamma, seed)
@@ -161,9 +176,7 @@ class Pattern:
         return out
 
     def __del__(self):
-        if getattr(self, "_h", None) is not None and self._h.value:
-            capi.load().culipx_pattern_destroy(self._h)
-            self._h = None
+        _release(self, "culipx_pattern_destroy")
 
 
 class Factor:
@@ -231,9 +244,41 @@ class Factor:
         return x
 
     def __del__(self):
-        if getattr(self, "_h", None) is not None and self._h.value:
-            capi.load().culipx_factor_destroy(self._h)
-            self._h = None
+        _release(self, "culipx_factor_destroy")
+
+
+class PermutePlan:
+    """B = diag(1/r) P_r K P_c' diag(1/c), sorted (T_matrix_permute_scale /
+    host_permute).  Built once per pattern from device rowptr/colidx and host
+    permutations; apply() maps a device value array into B's order."""
+
+    def __init__(self, handle: Handle, d_rowptr, d_colidx, row_perm, col_perm=None, perm_is_old_to_new=True):
+        self.handle = handle
+        self.n = int(d_rowptr.numel()) - 1
+        self.nnz = int(d_colidx.numel())
+        rp = np.ascontiguousarray(row_perm, np.int32)
+        cp = None if col_perm is None else np.ascontiguousarray(col_perm, np.int32)
+        h = ctypes.c_void_p()
+        capi.call("culipx_permute_create", handle._h, self.n, self.nnz, _dptr(d_rowptr), _dptr(d_colidx),
+                  rp.ctypes.data_as(ctypes.c_void_p), None if cp is None else cp.ctypes.data_as(ctypes.c_void_p),
+                  int(bool(perm_is_old_to_new)), ctypes.byref(h))
+        self._h = h
+
+    def structure(self):
+        """(rowptr, colidx) of B as host numpy int32 arrays."""
+        rowptr = np.zeros(self.n + 1, np.int32)
+        colidx = np.zeros(max(self.nnz, 1), np.int32)
+        capi.call("culipx_permute_export", self._h, rowptr.ctypes.data_as(ctypes.c_void_p),
+                  colidx.ctypes.data_as(ctypes.c_void_p))
+        return rowptr, colidx[: self.nnz]
+
+    def apply(self, d_val, d_out, row_scale=None, col_scale=None, scale_before_match=False):
+        prec = F64 if d_val.dtype.itemsize == 8 else F32
+        capi.call("culipx_permute_apply", self._h, prec, _dptr(d_val), _dptr(row_scale), _dptr(col_scale),
+                  int(bool(scale_before_match)), _dptr(d_out))
+
+    def __del__(self):
+        _release(self, "culipx_permute_destroy")
 
 
 class CsrOperator:
@@ -257,9 +302,7 @@ class CsrOperator:
         return y
 
     def __del__(self):
-        if getattr(self, "_h", None) is not None and self._h.value:
-            capi.load().culipx_csr_destroy(self._h)
-            self._h = None
+        _release(self, "culipx_csr_destroy")
 
 
 def sqmr_solve(handle: Handle, A: CsrOperator, M: Factor | None, b, x, tol=1e-8, max_it=1000):

@@ -65,6 +65,11 @@ _SIGS = {
     "culipx_factor_stats": [vp, ctypes.POINTER(f64), ctypes.POINTER(i32)],
     "culipx_factor_info": [vp, vp],
     "culipx_prec_apply": [vp, i32, vp, vp],
+    "culipx_permute_create": [vp, i32, i64, vp, vp, vp, vp, i32, ctypes.POINTER(vp)],
+    "culipx_permute_destroy": [vp],
+    "culipx_permute_structure": [vp, ctypes.POINTER(vp), ctypes.POINTER(vp)],
+    "culipx_permute_apply": [vp, i32, vp, vp, vp, i32, vp],
+    "culipx_permute_export": [vp, vp, vp],
     "culipx_csr_create": [vp, i32, i32, i64, vp, vp, vp, i32, i32, ctypes.POINTER(vp)],
     "culipx_csr_destroy": [vp],
     "culipx_spmv": [vp, vp, vp, f64, f64, i32],

@@ -1,6 +1,7 @@
 // extern "C" entry points of libculipx (declared in include/culipx.h).
 #include "factor.h"
 #include "pattern.h"
+#include "permute.h"
 #include "spmv.h"
 #include "sqmr.h"
 
@@ -327,6 +328,61 @@ CULIPX_API int culipx_csr_create(culipx_handle h, int m, int n, long long nnz, c
     }
     *out = A;
     return CULIPX_OK;
+    GUARD_END
+}
+
+CULIPX_API int culipx_permute_create(culipx_handle h, int n, long long nnz, const int* d_rowptr,
+                                     const int* d_colidx, const int* h_row_perm, const int* h_col_perm,
+                                     int perm_is_old_to_new, culipx_permute* out)
+{
+    if (!h || !out) return fail(CULIPX_INVALID_ARG, "culipx_permute_create: null argument");
+    GUARD_BEGIN
+    CULIPX_TRY(use_device(h));
+    PermutePlan* p = nullptr;
+    CULIPX_TRY(permute_plan_create(h, n, nnz, d_rowptr, d_colidx, h_row_perm, h_col_perm, perm_is_old_to_new, &p));
+    *out = static_cast<culipx_permute>(p);
+    return CULIPX_OK;
+    GUARD_END
+}
+
+CULIPX_API int culipx_permute_destroy(culipx_permute p)
+{
+    if (p) {
+        if (p->handle->device >= 0) cudaSetDevice(p->handle->device);
+        delete p;
+    }
+    return CULIPX_OK;
+}
+
+CULIPX_API int culipx_permute_structure(culipx_permute p, const int** d_rowptr, const int** d_colidx)
+{
+    if (!p) return fail(CULIPX_INVALID_ARG, "null plan");
+    if (d_rowptr) *d_rowptr = p->rowptr.as<int>();
+    if (d_colidx) *d_colidx = p->colidx.as<int>();
+    return CULIPX_OK;
+}
+
+CULIPX_API int culipx_permute_export(culipx_permute p, int* h_rowptr, int* h_colidx)
+{
+    if (!p) return fail(CULIPX_INVALID_ARG, "null plan");
+    GUARD_BEGIN
+    CULIPX_TRY(use_device(p->handle));
+    CULIPX_CUDA(cudaStreamSynchronize(p->handle->stream));
+    if (h_rowptr)
+        CULIPX_CUDA(cudaMemcpy(h_rowptr, p->rowptr.get(), (size_t)(p->n + 1) * sizeof(int), cudaMemcpyDeviceToHost));
+    if (h_colidx && p->nnz)
+        CULIPX_CUDA(cudaMemcpy(h_colidx, p->colidx.get(), (size_t)p->nnz * sizeof(int), cudaMemcpyDeviceToHost));
+    return CULIPX_OK;
+    GUARD_END
+}
+
+CULIPX_API int culipx_permute_apply(culipx_permute p, int precision, const void* d_val, const void* d_row_scale,
+                                    const void* d_col_scale, int scale_before_match, void* d_out)
+{
+    if (!p) return fail(CULIPX_INVALID_ARG, "null plan");
+    GUARD_BEGIN
+    CULIPX_TRY(use_device(p->handle));
+    return permute_plan_apply(p, precision, d_val, d_row_scale, d_col_scale, scale_before_match, d_out);
     GUARD_END
 }
 

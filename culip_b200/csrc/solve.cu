@@ -25,6 +25,8 @@
 
 namespace culipx {
 
+int exclusive_scan(int* d, int n, DeviceBuffer& tmp, culipx_handle_t* h, cudaStream_t s, int* launches);
+
 namespace {
 
 constexpr int kSweepWarps = 4;
@@ -405,16 +407,6 @@ __global__ void k_perm_scatter(const T* __restrict__ b, T* __restrict__ x, const
     for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < n; g += gridDim.x * blockDim.x) x[perm[g]] = b[g];
 }
 
-int exclusive_scan(int* d, int n, DeviceBuffer& tmp, culipx_handle_t* h, cudaStream_t s, int* launches)
-{
-    const int chunks = (n + kScanChunk - 1) / kScanChunk;
-    if ((size_t)chunks * sizeof(int) > tmp.bytes()) CULIPX_TRY(tmp.alloc(h, (size_t)chunks * sizeof(int)));
-    k_scan_chunks<<<chunks, kScanThreads, 0, s>>>(d, n, tmp.as<int>());
-    k_scan_sums<<<1, 1024, 0, s>>>(tmp.as<int>(), chunks);
-    k_scan_add<<<chunks, kScanThreads, 0, s>>>(d, n, tmp.as<int>());
-    *launches += 3;
-    return launch_check("exclusive_scan");
-}
 
 template <class T>
 int build_sweeps_t(Factor* f, cudaStream_t s, int* launches)
@@ -508,6 +500,19 @@ int apply_t(Factor* f, int stage, const void* d_b, void* d_x, cudaStream_t s)
 }
 
 }  // namespace
+
+// exclusive scan of n int counts in place (n - 1 counts and a trailing 0 give
+// the offsets and the total), three launches
+int exclusive_scan(int* d, int n, DeviceBuffer& tmp, culipx_handle_t* h, cudaStream_t s, int* launches)
+{
+    const int chunks = (n + kScanChunk - 1) / kScanChunk;
+    if ((size_t)chunks * sizeof(int) > tmp.bytes()) CULIPX_TRY(tmp.alloc(h, (size_t)chunks * sizeof(int)));
+    k_scan_chunks<<<chunks, kScanThreads, 0, s>>>(d, n, tmp.as<int>());
+    k_scan_sums<<<1, 1024, 0, s>>>(tmp.as<int>(), chunks);
+    k_scan_add<<<chunks, kScanThreads, 0, s>>>(d, n, tmp.as<int>());
+    *launches += 3;
+    return launch_check("exclusive_scan");
+}
 
 int build_sweeps(Factor* f, cudaStream_t s, int* launches)
 {

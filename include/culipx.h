@@ -161,6 +161,32 @@ int culipx_factor_info(culipx_factor f, long long *info8);
 int culipx_prec_apply(culipx_factor f, int stage, const void *d_b, void *d_x);
 
 /* ------------------------------------------------------------------------ */
+/* Permutation and scaling of K before the factorization: B = diag(1/r)
+ * P_r K P_c' diag(1/c) with sorted rows and columns, as T_matrix_permute_scale
+ * (libs/la/sparse_la.impl.cuh:599-657) called by the driver's host_permute
+ * (apps/block_ildlt/block_ildlt_invariants.h:31-69).  The plan holds B's
+ * structure and is built once per pattern; apply() maps each new set of
+ * values with one gather.
+ *   h_row_perm / h_col_perm : n entries each (h_col_perm NULL = h_row_perm);
+ *     old -> new if perm_is_old_to_new, else new -> old (inverted first, as
+ *     the reference's k_inv_perm)
+ *   d_row_scale / d_col_scale : NULL for unit scaling, else both given; B's
+ *     value is a / (r * c) with r, c taken at the old (row, column) when
+ *     scale_before_match, else at the new ones.
+ * d_rowptr / d_colidx are read during create only. */
+typedef struct culipx_permute_t *culipx_permute;
+int culipx_permute_create(culipx_handle h, int n, long long nnz, const int *d_rowptr, const int *d_colidx,
+                          const int *h_row_perm, const int *h_col_perm, int perm_is_old_to_new,
+                          culipx_permute *out);
+int culipx_permute_destroy(culipx_permute p);
+/* B's row offsets (n + 1) and columns (nnz), device arrays owned by the plan */
+int culipx_permute_structure(culipx_permute p, const int **d_rowptr, const int **d_colidx);
+/* the same copied to host arrays (n + 1 and nnz entries) */
+int culipx_permute_export(culipx_permute p, int *h_rowptr, int *h_colidx);
+int culipx_permute_apply(culipx_permute p, int precision, const void *d_val, const void *d_row_scale,
+                         const void *d_col_scale, int scale_before_match, void *d_out);
+
+/* ------------------------------------------------------------------------ */
 /* CSR operator (CSRMatrixSPMV<T>).  Device arrays are borrowed, not copied:
  * they must outlive the operator, as the reference's raw pointer does. */
 int culipx_csr_create(culipx_handle h, int m, int n, long long nnz, const int *d_rowptr,

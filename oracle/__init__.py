@@ -195,3 +195,45 @@ def sqmr_ldu(rowptr, colidx, val, L_rowptr, L_colidx, L_val, tri, is_piv, perm, 
     res = np.zeros(1)
     it = lib().orc_sqmr_ldu_d(m, *[_p(v) for v in a], _p(x), float(tol), int(max_it), _p(res))
     return x, float(res[0]), int(it)
+
+
+def permute_scale(rowptr, colidx, val, row_perm, col_perm=None, row_scale=None, col_scale=None,
+                  scale_before_match=False, perm_is_old_to_new=True):
+    """B = diag(1/r) P_r A P_c' diag(1/c) as sorted CSR (numpy restatement of
+    T_matrix_permute_scale, libs/la/sparse_la.impl.cuh:599-657):
+      * k_inv_perm (:586-595) inverts each given map when it is new -> old;
+      * k_transform_coo (:552-582) maps every triplet (r, c, a) to
+        (p_r[r], p_c[c], a / s), s = row_scale[r] * col_scale[c] when
+        scale_before_match, else row_scale[p_r[r]] * col_scale[p_c[c]];
+        without scales the reference divides by 1 (a value is unchanged);
+      * T_coo2csr (:939-975) sorts the triplets by (row, column) (ties,
+        i.e. duplicate entries, are kept in input order here).
+    Returns (rowptr, colidx, val) of B; val keeps the input dtype."""
+    rowptr = np.asarray(rowptr, np.int64)
+    colidx = np.asarray(colidx, np.int64)
+    val = np.asarray(val)
+    n = len(rowptr) - 1
+
+    def fwd(p):
+        p = np.asarray(p, np.int64)
+        if perm_is_old_to_new:
+            return p
+        inv = np.empty(n, np.int64)
+        inv[p] = np.arange(n)
+        return inv
+
+    pr = fwd(row_perm)
+    pc = pr if col_perm is None else fwd(col_perm)
+    rows = np.repeat(np.arange(n), np.diff(rowptr))
+    new_r, new_c = pr[rows], pc[colidx]
+    if row_scale is None:
+        v = val.copy()
+    else:
+        rs = np.asarray(row_scale, val.dtype)
+        cs = np.asarray(col_scale, val.dtype)
+        sc = rs[rows] * cs[colidx] if scale_before_match else rs[new_r] * cs[new_c]
+        v = val / sc
+    order = np.lexsort((np.arange(len(val)), new_c, new_r))
+    b_rowptr = np.zeros(n + 1, np.int32)
+    np.add.at(b_rowptr, new_r + 1, 1)
+    return np.cumsum(b_rowptr).astype(np.int32), new_c[order].astype(np.int32), v[order]
