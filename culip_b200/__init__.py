@@ -18,10 +18,10 @@ import ctypes
 import numpy as np
 
 from . import _capi as capi
-from ._capi import (F32, F64, LEFT, MIDDLE, PIV_BK, PIV_ROOK, PIV_STATIC, RIGHT, CulipxError,  # noqa: F401
-                    KktSpec)
+from ._capi import (F32, F64, LEFT, MIDDLE, PIV_BK, PIV_ROOK, PIV_STATIC, RIGHT, SOLVE_BLOCK,  # noqa: F401
+                    SOLVE_JACOBI, SOLVE_SCALAR, SOLVE_STRIPE, CulipxError, KktSpec)
 
-__all__ = ["Handle", "Pattern", "Factor", "CsrOperator", "BlockiLDLt", "CSRMatrixSPMV", "SQMR", "kkt_generate",
+__all__ = ["Handle", "Pattern", "Factor", "CsrOperator", "PermutePlan", "BlockiLDLt", "CSRMatrixSPMV", "SQMR", "kkt_generate",
            "kkt_blocking", "normal_vector", "CulipxError", "KKT_CONFIGS"]
 
 # The benchmark systems: K = [[H + delta I, A'], [A, -gamma I]] (see DESIGN.md for the construction)
@@ -205,6 +205,9 @@ class Factor:
             capi.call("culipx_factor_compute", self._h, _dptr(vals), None if ip is None else _p(ip), int(pivot),
                       float(threshold))
 
+    def set_solve_algorithm(self, algorithm, sweeps=0):
+        capi.call("culipx_factor_set_solve_algorithm", self._h, int(algorithm), int(sweeps))
+
     def stats(self):
         ms = ctypes.c_double()
         nl = ctypes.c_int()
@@ -330,7 +333,6 @@ def sqmr_solve_noalloc(handle: Handle, A: CsrOperator, M: Factor, b, x, tol=1e-8
 # --------------------------------------------------------------------------
 # Reference-named facade (same names, argument meaning and return values)
 
-SOLVE_STRIPE, SOLVE_BLOCK, SOLVE_SCALAR, SOLVE_JACOBI = range(4)
 
 
 class BlockiLDLt:
@@ -357,6 +359,7 @@ class BlockiLDLt:
         self.pattern = None
         self.factor = None
         self.algorithm = SOLVE_BLOCK
+        self.jacobi_sweeps = 0
 
     def n(self):
         return self.n_
@@ -365,6 +368,7 @@ class BlockiLDLt:
         self.pattern = Pattern(self.handle, self.rowptr, self.colidx, self.block_starts, fill_level,
                                max(1.0, float(fill_factor)), self.precision)
         self.factor = Factor(self.pattern)
+        self.factor.set_solve_algorithm(self.algorithm, self.jacobi_sweeps)
         self.factor.compute(self.val, self.is_piv, self.pivot, threshold)
         return 0
 
@@ -378,9 +382,13 @@ class BlockiLDLt:
         return True
 
     def set_solve_algorithm(self, algorithm, num_jacobi_sweeps=0):
-        if algorithm != SOLVE_BLOCK:
-            raise CulipxError(capi.NOT_SUPPORTED, "only the level-scheduled block solve (SOLVE_BLOCK) is provided")
-        self.algorithm = algorithm
+        """SOLVE_STRIPE / SOLVE_BLOCK / SOLVE_SCALAR: exact block triangular
+        solves (one level-scheduled implementation); SOLVE_JACOBI: that many
+        block-Jacobi sweeps per triangular solve."""
+        self.algorithm = int(algorithm)
+        self.jacobi_sweeps = int(num_jacobi_sweeps)
+        if self.factor is not None:
+            self.factor.set_solve_algorithm(self.algorithm, self.jacobi_sweeps)
 
     def solve_analysis(self):
         # the sweep structures are built with the factor

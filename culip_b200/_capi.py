@@ -16,6 +16,7 @@ OK, INVALID_ARG, OOM, BREAKDOWN, MAXIT, TIMEOUT, CUDA_ERROR, NOT_SUPPORTED = ran
 F64, F32 = 0, 1
 PIV_STATIC, PIV_BK, PIV_ROOK = 0, 1, 2
 LEFT, MIDDLE, RIGHT = 0, 1, 2
+SOLVE_STRIPE, SOLVE_BLOCK, SOLVE_SCALAR, SOLVE_JACOBI = 0, 1, 2, 3
 
 STATUS_NAMES = {0: "OK", 1: "INVALID_ARG", 2: "OOM", 3: "BREAKDOWN", 4: "MAXIT", 5: "TIMEOUT", 6: "CUDA_ERROR",
                 7: "NOT_SUPPORTED"}
@@ -65,6 +66,7 @@ _SIGS = {
     "culipx_factor_stats": [vp, ctypes.POINTER(f64), ctypes.POINTER(i32)],
     "culipx_factor_info": [vp, vp],
     "culipx_prec_apply": [vp, i32, vp, vp],
+    "culipx_factor_set_solve_algorithm": [vp, i32, i32],
     "culipx_permute_create": [vp, i32, i64, vp, vp, vp, vp, i32, ctypes.POINTER(vp)],
     "culipx_permute_destroy": [vp],
     "culipx_permute_structure": [vp, ctypes.POINTER(vp), ctypes.POINTER(vp)],

@@ -293,6 +293,17 @@ CULIPX_API int culipx_factor_info(culipx_factor f, long long* info8)
     GUARD_END
 }
 
+CULIPX_API int culipx_factor_set_solve_algorithm(culipx_factor f, int algorithm, int sweeps)
+{
+    if (!f) return fail(CULIPX_INVALID_ARG, "null factor");
+    if (algorithm < CULIPX_SOLVE_STRIPE || algorithm > CULIPX_SOLVE_JACOBI)
+        return fail(CULIPX_INVALID_ARG, "culipx_factor_set_solve_algorithm: bad algorithm %d", algorithm);
+    if (sweeps < 0) return fail(CULIPX_INVALID_ARG, "culipx_factor_set_solve_algorithm: sweeps < 0");
+    f->solve_algorithm = algorithm;
+    f->jacobi_sweeps = sweeps;
+    return CULIPX_OK;
+}
+
 CULIPX_API int culipx_prec_apply(culipx_factor f, int stage, const void* d_b, void* d_x)
 {
     if (!f) return fail(CULIPX_INVALID_ARG, "null factor");

@@ -21,6 +21,8 @@ struct Factor {
     bool computed = false;
     int pivot = CULIPX_PIV_BK;
     double threshold = 0.0;
+    int solve_algorithm = CULIPX_SOLVE_BLOCK;  // set_solve_algorithm
+    int jacobi_sweeps = 0;
 
     // block storage (pattern layout + relocation arena for blocks that were
     // granted extra slots by dual dropping)
@@ -57,6 +59,7 @@ struct Factor {
     // simple_rows[scan_s[lvl_off[L]] ..) and cplx[scan_c[lvl_off[L]] ..)
     DeviceBuffer scan_s, scan_c, simple_rows, cplx;
     DeviceBuffer work;                   // n values of apply scratch
+    DeviceBuffer jac_a, jac_b;           // SOLVE_JACOBI iterates (n values each, allocated on first use)
     DeviceBuffer scan_tmp;               // scan partial sums
     long long u_nnz = 0;
 

@@ -372,6 +372,51 @@ __global__ void __launch_bounds__(32 * kSweepWarps)
     if (lane < h) x[fr + lane] = acc;
 }
 
+// one block-Jacobi sweep over all block rows (SOLVE_JACOBI; the stripe
+// kernel of solve_U_jacobi / solve_Ut_jacobi, block_ildlt.impl.cuh:2455-2494
+// and 2635-2674): x_out_I = U_II^-1 (b_I - U_I* x_in) for U (UPPER) or U'
+template <class T, bool UPPER>
+__global__ void __launch_bounds__(32 * kSweepWarps)
+    k_sweep_jacobi(int cm, const int* __restrict__ bs, const int* __restrict__ off, const int* __restrict__ col,
+                   const T* __restrict__ vals, const long long* __restrict__ piv_off,
+                   const int* __restrict__ rowflags, const T* __restrict__ fval, const T* __restrict__ b,
+                   const T* __restrict__ x_in, T* __restrict__ x_out)
+{
+    __shared__ T tiles[kSweepWarps][kTileElems];
+    const int warp = threadIdx.x >> 5;
+    const int I = blockIdx.x * kSweepWarps + warp;
+    if (I >= cm) return;
+    const int lane = lane_id();
+    const int fr = bs[I], h = bs[I + 1] - fr;
+    T acc = T(0);
+    if (lane < h) {
+        acc = b[fr + lane];
+        const int e1 = off[fr + lane + 1];
+        for (int k = off[fr + lane]; k < e1; ++k) acc = fma_rn(-vals[k], x_in[col[k]], acc);
+    }
+    if (!(rowflags[I] & kRowIdentity)) {
+        T* tile = tiles[warp];
+        const T* P = fval + piv_off[I];
+        if (lane < h)
+            for (int i = 0; i < h; ++i) tile[i * kTileStride + lane] = P[i * h + lane];
+        __syncwarp();
+        if (UPPER) {
+            for (int c = h - 1; c >= 0; --c) {
+                if (lane == c) acc = acc / tile[c * kTileStride + c];
+                const T xc = shfl(acc, c);
+                if (lane < c) acc = fma_rn(-tile[lane * kTileStride + c], xc, acc);
+            }
+        } else {
+            for (int r = 0; r < h; ++r) {
+                if (lane == r) acc = acc / tile[r * kTileStride + r];
+                const T xr = shfl(acc, r);
+                if (lane > r && lane < h) acc = fma_rn(-tile[r * kTileStride + lane], xr, acc);
+            }
+        }
+    }
+    if (lane < h) x_out[fr + lane] = acc;
+}
+
 // k_solve_D: Givens-based 1x1 / 2x2 block-diagonal solve (out may equal in)
 template <class T>
 __global__ void k_solve_D(const T* __restrict__ tri, const int* __restrict__ is_piv, const T* in, T* out, int n)
@@ -469,6 +514,34 @@ int apply_t(Factor* f, int stage, const void* d_b, void* d_x, cudaStream_t s)
         return launch_check("k_solve_D");
     }
     const T* fval = f->val.as<T>();
+    if (f->solve_algorithm == CULIPX_SOLVE_JACOBI) {
+        // x = 0, then `sweeps` block-Jacobi sweeps on the right-hand side rhs
+        if (!f->jac_a.get()) CULIPX_TRY(f->jac_a.alloc(p.handle, (size_t)n * sizeof(T) + 16));
+        if (!f->jac_b.get()) CULIPX_TRY(f->jac_b.alloc(p.handle, (size_t)n * sizeof(T) + 16));
+        const int cm = p.num_blocks;
+        const bool left = stage == CULIPX_LEFT;
+        T* rhs = f->work.as<T>();
+        if (left) k_perm_gather<T><<<grid_n, 256, 0, s>>>(b, rhs, f->perm.as<int>(), n);
+        else CULIPX_CUDA(cudaMemcpyAsync(rhs, b, n * sizeof(T), cudaMemcpyDeviceToDevice, s));
+        T* xa = f->jac_a.as<T>();
+        T* xb = f->jac_b.as<T>();
+        CULIPX_CUDA(cudaMemsetAsync(xa, 0, n * sizeof(T), s));
+        const int grid = (cm + kSweepWarps - 1) / kSweepWarps;
+        for (int sw = 0; sw < f->jacobi_sweeps; ++sw) {
+            if (left)
+                k_sweep_jacobi<T, false><<<grid, 32 * kSweepWarps, 0, s>>>(
+                    cm, p.d_bs.as<int>(), f->ut_off.as<int>(), f->ut_col.as<int>(), f->ut_val.as<T>(),
+                    f->piv_off.as<long long>(), f->rowflags.as<int>(), fval, rhs, xa, xb);
+            else
+                k_sweep_jacobi<T, true><<<grid, 32 * kSweepWarps, 0, s>>>(
+                    cm, p.d_bs.as<int>(), f->u_off.as<int>(), f->u_col.as<int>(), f->u_val.as<T>(),
+                    f->piv_off.as<long long>(), f->rowflags.as<int>(), fval, rhs, xa, xb);
+            std::swap(xa, xb);
+        }
+        if (left) CULIPX_CUDA(cudaMemcpyAsync(x, xa, n * sizeof(T), cudaMemcpyDeviceToDevice, s));
+        else k_perm_scatter<T><<<grid_n, 256, 0, s>>>(xa, x, f->perm.as<int>(), n);
+        return launch_check("Jacobi sweeps");
+    }
     if (stage == CULIPX_LEFT) {
         T* t = x;
         if ((const void*)b == (void*)x) {
@@ -526,7 +599,9 @@ int prec_apply(Factor* f, int stage, const void* d_b, void* d_x, cudaStream_t s)
     if (!d_b || !d_x) return fail(CULIPX_INVALID_ARG, "culipx_prec_apply: null vector");
     if (stage < CULIPX_LEFT || stage > CULIPX_RIGHT) return fail(CULIPX_INVALID_ARG, "culipx_prec_apply: bad stage");
     Pattern& p = *f->pat;
-    p.handle->launches += (stage == CULIPX_MIDDLE) ? 1 : p.num_levels + 1;
+    if (stage == CULIPX_MIDDLE) p.handle->launches += 1;
+    else if (f->solve_algorithm == CULIPX_SOLVE_JACOBI) p.handle->launches += f->jacobi_sweeps + 1 + (stage == CULIPX_LEFT);
+    else p.handle->launches += p.num_levels + 1;
     if (f->precision == CULIPX_F64) return apply_t<double>(f, stage, d_b, d_x, s);
     return apply_t<float>(f, stage, d_b, d_x, s);
 }

@@ -398,8 +398,9 @@ int sqmr_solve(culipx_handle_t* h, Csr* A, Factor* M, const double* b, double* x
     if (M && (!M->computed || M->pat->n != A->m))
         return fail(CULIPX_INVALID_ARG, "culipx_sqmr_solve: preconditioner not computed or wrong size");
     if (max_it < 0) return fail(CULIPX_INVALID_ARG, "culipx_sqmr_solve: max_it < 0");
-    // with a preconditioner: the single-launch persistent solver (FP64 or FP32 factor)
-    if (M && !w->force_multi_kernel)
+    // with a preconditioner: the single-launch persistent solver (FP64 or FP32
+    // factor); block-Jacobi sweeps (SOLVE_JACOBI) run through the per-phase kernels
+    if (M && !w->force_multi_kernel && M->solve_algorithm != CULIPX_SOLVE_JACOBI)
         return sqmr_solve_persistent(h, A, M, b, x, tol, max_it, residual, iterations, w);
     if (M && M->precision != CULIPX_F64)
         return fail(CULIPX_NOT_SUPPORTED, "culipx_sqmr_solve: the multi-kernel solver needs an FP64 factor");

@@ -939,6 +939,8 @@ int sqmr_solve_noalloc(culipx_handle_t* h, Csr* A, Factor* M, const double* b, d
         return fail(CULIPX_INVALID_ARG, "culipx_sqmr_solve_noalloc: A must be square FP64");
     if (!M->computed || M->pat->n != A->m)
         return fail(CULIPX_INVALID_ARG, "culipx_sqmr_solve_noalloc: preconditioner not computed or wrong size");
+    if (M->solve_algorithm == CULIPX_SOLVE_JACOBI)
+        return fail(CULIPX_NOT_SUPPORTED, "culipx_sqmr_solve_noalloc: SOLVE_JACOBI needs culipx_sqmr_solve");
     if (A->m > kNoAllocMaxRows)
         return fail(CULIPX_INVALID_ARG,
                     "culipx_sqmr_solve_noalloc: n = %d exceeds the fixed scratch of %d rows; use culipx_sqmr_solve",

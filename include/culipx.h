@@ -47,6 +47,16 @@ extern "C" {
 #define CULIPX_PIV_BK     1
 #define CULIPX_PIV_ROOK   2
 
+/* ---- triangular-solve algorithm (SOLVE_ALGORITHM, libs/la/preconditioner/block_ildlt.cuh:24-30) ----
+ * STRIPE, BLOCK and SCALAR are the reference's three schedules of the same
+ * exact block triangular solves; here all three run the level-scheduled
+ * sweeps.  JACOBI replaces each triangular solve by a number of block-Jacobi
+ * sweeps from x = 0 (solve_U_jacobi / solve_Ut_jacobi, block_ildlt.impl.cuh:2455-2494). */
+#define CULIPX_SOLVE_STRIPE 0
+#define CULIPX_SOLVE_BLOCK  1
+#define CULIPX_SOLVE_SCALAR 2
+#define CULIPX_SOLVE_JACOBI 3
+
 /* ---- preconditioner stage (Preconditioner<T>, libs/la/preconditioner.cuh:18-40) ---- */
 #define CULIPX_LEFT   0   /* x = U'^-1 P' b   (solve_left)   */
 #define CULIPX_MIDDLE 1   /* x = D^-1 b       (solve_middle) */
@@ -155,6 +165,11 @@ int culipx_factor_stats(culipx_factor f, double *ms, int *launches);
  * rows (identity tile, no swaps, 1x1 pivots), [4] block rows with a 2x2
  * pivot, [5] bytes per value, [6..7] 0 */
 int culipx_factor_info(culipx_factor f, long long *info8);
+
+/* set_solve_algorithm (block_ildlt.impl.cuh:253-258): algorithm one of
+ * CULIPX_SOLVE_*, sweeps (>= 0) used by CULIPX_SOLVE_JACOBI.  Applies and
+ * culipx_sqmr_solve follow it; SQMR with JACOBI needs an FP64 factor. */
+int culipx_factor_set_solve_algorithm(culipx_factor f, int algorithm, int sweeps);
 
 /* Preconditioner applies; b and x are device vectors of n values in the
  * factor's precision (b == x allowed for MIDDLE). */

@@ -55,9 +55,13 @@ def lib():
             g.argtypes = [vp]
             getattr(L, "orc_fac_export" + sfx).argtypes = [vp] * 9
             getattr(L, "orc_prec_apply" + sfx).argtypes = [vp, ctypes.c_int, vp, vp]
+            getattr(L, "orc_prec_apply_jacobi" + sfx).argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, vp]
         L.orc_spmv_d.argtypes = [ctypes.c_int, vp, vp, vp, vp, vp, ctypes.c_double, ctypes.c_double]
         L.orc_sqmr_d.restype = ctypes.c_int
         L.orc_sqmr_d.argtypes = [ctypes.c_int, vp, vp, vp, vp, vp, vp, ctypes.c_double, ctypes.c_int, vp]
+        L.orc_sqmr_jacobi_d.restype = ctypes.c_int
+        L.orc_sqmr_jacobi_d.argtypes = [ctypes.c_int, vp, vp, vp, vp, ctypes.c_int, vp, vp, ctypes.c_double,
+                                        ctypes.c_int, vp]
         L.orc_sqmr_ldu_d.restype = ctypes.c_int
         L.orc_sqmr_ldu_d.argtypes = [ctypes.c_int] + [vp] * 12 + [ctypes.c_double, ctypes.c_int, vp]
         _lib = L
@@ -154,10 +158,15 @@ class Fac:
         out["val"] = out["val"][:tot]
         return out
 
-    def apply(self, stage: int, b) -> np.ndarray:
+    def apply(self, stage: int, b, jacobi_sweeps: int = 0) -> np.ndarray:
+        """solve_left (0) / middle (1) / right (2); jacobi_sweeps > 0 replaces the
+        exact triangular solves by that many block-Jacobi sweeps (SOLVE_JACOBI)."""
         b = np.ascontiguousarray(b, dtype=self.sym.dtype)
         x = np.zeros_like(b)
-        getattr(lib(), "orc_prec_apply" + self.sfx)(self._h, int(stage), _p(b), _p(x))
+        if jacobi_sweeps > 0:
+            getattr(lib(), "orc_prec_apply_jacobi" + self.sfx)(self._h, int(stage), int(jacobi_sweeps), _p(b), _p(x))
+        else:
+            getattr(lib(), "orc_prec_apply" + self.sfx)(self._h, int(stage), _p(b), _p(x))
         return x
 
 
@@ -172,7 +181,7 @@ def spmv(rowptr, colidx, val, x, alpha=1.0, beta=0.0, y=None) -> np.ndarray:
     return y
 
 
-def sqmr(rowptr, colidx, val, b, fac: Fac | None = None, tol=1e-8, max_it=1000):
+def sqmr(rowptr, colidx, val, b, fac: Fac | None = None, tol=1e-8, max_it=1000, jacobi_sweeps=0):
     rowptr = np.ascontiguousarray(rowptr, np.int32)
     colidx = np.ascontiguousarray(colidx, np.int32)
     val = np.ascontiguousarray(val, np.float64)
@@ -180,6 +189,10 @@ def sqmr(rowptr, colidx, val, b, fac: Fac | None = None, tol=1e-8, max_it=1000):
     m = len(rowptr) - 1
     x = np.zeros(m)
     res = np.zeros(1)
+    if jacobi_sweeps > 0:
+        it = lib().orc_sqmr_jacobi_d(m, _p(rowptr), _p(colidx), _p(val), fac._h, int(jacobi_sweeps), _p(b), _p(x),
+                                     float(tol), int(max_it), _p(res))
+        return x, float(res[0]), int(it)
     it = lib().orc_sqmr_d(m, _p(rowptr), _p(colidx), _p(val), fac._h if fac is not None else None, _p(b), _p(x),
                           float(tol), int(max_it), _p(res))
     return x, float(res[0]), int(it)

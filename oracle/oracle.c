@@ -57,6 +57,7 @@ void orc_spmv_d(int m, const int *rowptr, const int *colidx, const double *val,
 typedef struct {
     int kind;                 /* 0 none, 1 block factor, 2 imported LDU */
     const orc_fac_d *fac;
+    int sweeps;               /* kind 1: > 0 = block-Jacobi sweeps instead of exact solves */
     int n;
     const int *L_rowptr, *L_colidx;
     const double *L_val, *tri, *scale;
@@ -121,7 +122,8 @@ static void ldu_apply(const prec_t *P, int stage, const double *b, double *x)
 
 static void prec_apply(const prec_t *P, int stage, const double *b, double *x)
 {
-    if (P->kind == 1) orc_prec_apply_d(P->fac, stage, b, x);
+    if (P->kind == 1 && P->sweeps > 0) orc_prec_apply_jacobi_d(P->fac, stage, P->sweeps, b, x);
+    else if (P->kind == 1) orc_prec_apply_d(P->fac, stage, b, x);
     else if (P->kind == 2) ldu_apply(P, stage, b, x);
     else memcpy(x, b, sizeof(double) * P->n);
 }
@@ -270,6 +272,18 @@ int orc_sqmr_d(int m, const int *rowptr, const int *colidx, const double *val,
     memset(&P, 0, sizeof(P));
     P.kind = f ? 1 : 0;
     P.fac = f;
+    P.n = m;
+    return sqmr_core(m, rowptr, colidx, val, &P, b, x, tol, max_it, residual);
+}
+
+int orc_sqmr_jacobi_d(int m, const int *rowptr, const int *colidx, const double *val, const orc_fac_d *f,
+                      int sweeps, const double *b, double *x, double tol, int max_it, double *residual)
+{
+    prec_t P;
+    memset(&P, 0, sizeof(P));
+    P.kind = 1;
+    P.fac = f;
+    P.sweeps = sweeps;
     P.n = m;
     return sqmr_core(m, rowptr, colidx, val, &P, b, x, tol, max_it, residual);
 }

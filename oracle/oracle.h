@@ -62,6 +62,10 @@ void orc_fac_export_s(const orc_fac_s *f, int *blk_nnz, long *blk_off, int *idx,
  * 2 = right (U then P) */
 void orc_prec_apply_d(const orc_fac_d *f, int stage, const double *b, double *x);
 void orc_prec_apply_s(const orc_fac_s *f, int stage, const float *b, float *x);
+void orc_prec_apply_jacobi_d(const orc_fac_d *f, int stage, int sweeps, const double *b, double *x);
+void orc_prec_apply_jacobi_s(const orc_fac_s *f, int stage, int sweeps, const float *b, float *x);
+int orc_sqmr_jacobi_d(int m, const int *rowptr, const int *colidx, const double *val, const orc_fac_d *f,
+                      int sweeps, const double *b, double *x, double tol, int max_it, double *residual);
 
 /* y = alpha * A x + beta * y (beta == 0: y is not read) */
 void orc_spmv_d(int m, const int *rowptr, const int *colidx, const double *val,

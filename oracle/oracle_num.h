@@ -770,6 +770,79 @@ static void F(solve_D)(int n, const REAL *tri, const int *is_piv, const REAL *in
     }
 }
 
+/* One block-Jacobi sweep of U x = b (UPPER) or U' x = b: every block row at
+ * once from the previous iterate, x_out_I = U_II^-1 (b_I - U_I* x_in), with
+ * the same per-row term order and pivot-tile substitution as solve_U /
+ * solve_Ut; k_solve_block_stripe_level in solve_U_jacobi / solve_Ut_jacobi
+ * (block_ildlt.impl.cuh:2455-2494, 2635-2674), starting from x = 0. */
+static void F(jacobi_sweep)(const F(fac_t) *f, const F(rowlist_t) *R, int upper, const REAL *b,
+                            const REAL *x_in, REAL *x_out)
+{
+    const orc_sym *s = f->s;
+    for (int I = 0; I < s->num_blocks; ++I) {
+        const int from = s->bs[I], h = F(bsize)(s, I);
+        REAL t[32];
+        for (int r = 0; r < h; ++r) {
+            REAL acc = b[from + r];
+            for (int k = R->off[from + r]; k < R->off[from + r + 1]; ++k)
+                acc = FMA(-R->val[k], x_in[R->col[k]], acc);
+            t[r] = acc;
+        }
+        const int pb = s->csc_blk[s->csc_off[I + 1] - 1];
+        const REAL *P = f->val[pb];
+        if (upper) {
+            for (int c = h - 1; c >= 0; --c) {
+                t[c] = t[c] / P[c * h + c];
+                for (int r = 0; r < c; ++r) t[r] = FMA(-P[r * h + c], t[c], t[r]);
+            }
+        } else {
+            for (int r = 0; r < h; ++r) {
+                t[r] = t[r] / P[r * h + r];
+                for (int c = r + 1; c < h; ++c) t[c] = FMA(-P[r * h + c], t[r], t[c]);
+            }
+        }
+        for (int r = 0; r < h; ++r) x_out[from + r] = t[r];
+    }
+}
+
+static void F(jacobi_solve)(const F(fac_t) *f, const F(rowlist_t) *R, int upper, int sweeps, const REAL *b,
+                            REAL *x)
+{
+    const int n = f->s->n;
+    REAL *a = (REAL *)calloc(n ? n : 1, sizeof(REAL));
+    REAL *c = (REAL *)calloc(n ? n : 1, sizeof(REAL));
+    for (int sw = 0; sw < sweeps; ++sw) {
+        F(jacobi_sweep)(f, R, upper, b, a, c);
+        REAL *t = a; a = c; c = t;
+    }
+    memcpy(x, a, sizeof(REAL) * n);
+    free(a);
+    free(c);
+}
+
+/* solve_left / solve_right with SOLVE_JACOBI (set_solve_algorithm,
+ * block_ildlt.impl.cuh:253-258): the triangular solves replaced by `sweeps`
+ * block-Jacobi sweeps; P, P' and D as in the exact applies. */
+void F(orc_prec_apply_jacobi)(const F(fac_t) *f, int stage, int sweeps, const REAL *b, REAL *x)
+{
+    const int n = f->s->n;
+    if (stage == 1) {
+        F(orc_prec_apply)(f, 1, b, x);
+        return;
+    }
+    REAL *t = (REAL *)malloc(sizeof(REAL) * (n ? n : 1));
+    if (stage == 0) {
+        for (int g = 0; g < n; ++g) t[g] = b[f->perm[g]];        /* k_permute_Pt */
+        F(jacobi_solve)(f, &f->Ut, 0, sweeps, t, x);
+    } else {
+        REAL *u = (REAL *)malloc(sizeof(REAL) * (n ? n : 1));
+        F(jacobi_solve)(f, &f->U, 1, sweeps, b, u);
+        for (int g = 0; g < n; ++g) x[f->perm[g]] = u[g];        /* k_permute_P */
+        free(u);
+    }
+    free(t);
+}
+
 /* solve_left (P' then U'^-1), solve_middle (D^-1, applied to a copy of b as in
  * block_ildlt.impl.cuh:216-219) and solve_right (U^-1 then P),
  * block_ildlt.impl.cuh:183-246. */

@@ -181,3 +181,39 @@ def test_sqmr_fp32_factor_mixed(handle):
 
     K = sp.csr_matrix((v, ci, rp))
     assert np.linalg.norm(b - K @ xg.cpu().numpy()) / np.linalg.norm(b) < 1e-4
+
+
+@pytest.mark.parametrize("stage", [cb.LEFT, cb.RIGHT])
+@pytest.mark.parametrize("sweeps", [0, 1, 3, "levels"])
+def test_prec_apply_jacobi(handle, stage, sweeps):
+    """SOLVE_JACOBI (set_solve_algorithm): block-Jacobi sweeps from x = 0,
+    bit-exact against the oracle; with as many sweeps as levels it is the
+    exact solve."""
+    rp, ci, v, bs = scrambled_kkt(seed=8)
+    S, OF, P, F = _factor_both(handle, rp, ci, v, bs)
+    nl = P.info()["num_levels"]
+    sw = nl if sweeps == "levels" else sweeps
+    F.set_solve_algorithm(cb.SOLVE_JACOBI, sw)
+    b = cb.normal_vector(13, len(rp) - 1)
+    xo = OF.apply(stage, b, jacobi_sweeps=sw) if sw > 0 else np.zeros_like(b)
+    xg = F.apply(stage, torch.from_numpy(b).cuda()).cpu().numpy()
+    assert np.array_equal(xo, xg)
+    if sweeps == "levels":
+        assert np.array_equal(xg, OF.apply(stage, b))
+    F.set_solve_algorithm(cb.SOLVE_BLOCK, 0)
+    assert np.array_equal(F.apply(stage, torch.from_numpy(b).cuda()).cpu().numpy(), OF.apply(stage, b))
+
+
+def test_sqmr_jacobi(handle):
+    """SQMR with the SOLVE_JACOBI preconditioner (2 sweeps) against the oracle."""
+    rp, ci, v, bs = kkt("small")
+    S, OF, P, F = _factor_both(handle, rp, ci, v, bs)
+    F.set_solve_algorithm(cb.SOLVE_JACOBI, 2)
+    b = cb.normal_vector(cb.SEED + 1, len(rp) - 1)
+    xo, reso, ito = oracle.sqmr(rp, ci, v, b, OF, 1e-8, 1000, jacobi_sweeps=2)
+    A = _csr_op(handle, rp, ci, v)
+    xg = torch.zeros(len(rp) - 1, dtype=torch.float64, device="cuda")
+    res, its, st = cb.sqmr_solve(handle, A, F, torch.from_numpy(b).cuda(), xg, 1e-8, 1000)
+    xg = xg.cpu().numpy()
+    assert abs(its - ito) <= 4
+    assert np.linalg.norm(xg - xo) / np.linalg.norm(xo) < 1e-6
