@@ -176,7 +176,10 @@ class Pattern:
         return out
 
     def __del__(self):
-        _release(self, "culipx_pattern_destroy")
+        try:
+            _release(self, "culipx_pattern_destroy")
+        except Exception:  # interpreter shutdown
+            pass
 
 
 class Factor:
@@ -247,7 +250,10 @@ class Factor:
         return x
 
     def __del__(self):
-        _release(self, "culipx_factor_destroy")
+        try:
+            _release(self, "culipx_factor_destroy")
+        except Exception:  # interpreter shutdown
+            pass
 
 
 class PermutePlan:
@@ -281,7 +287,10 @@ class PermutePlan:
                   int(bool(scale_before_match)), _dptr(d_out))
 
     def __del__(self):
-        _release(self, "culipx_permute_destroy")
+        try:
+            _release(self, "culipx_permute_destroy")
+        except Exception:  # interpreter shutdown
+            pass
 
 
 class CsrOperator:
@@ -305,7 +314,10 @@ class CsrOperator:
         return y
 
     def __del__(self):
-        _release(self, "culipx_csr_destroy")
+        try:
+            _release(self, "culipx_csr_destroy")
+        except Exception:  # interpreter shutdown
+            pass
 
 
 def sqmr_solve(handle: Handle, A: CsrOperator, M: Factor | None, b, x, tol=1e-8, max_it=1000):
@@ -315,6 +327,20 @@ def sqmr_solve(handle: Handle, A: CsrOperator, M: Factor | None, b, x, tol=1e-8,
     st = capi.call("culipx_sqmr_solve", handle._h, A._h, M._h if M is not None else None, _dptr(b), _dptr(x),
                    float(tol), int(max_it), ctypes.byref(res), ctypes.byref(its), allow=(capi.OK, capi.MAXIT))
     return res.value, its.value, st
+
+
+def sqmr_refine(handle: Handle, A: CsrOperator, M: Factor, b, x, tol=1e-8, inner_tol=1e-6, inner_max_it=1000,
+                max_refine=20):
+    """FP64 iterative refinement around SQMR (mixed precision with an FP32
+    factor).  Returns (relres, total SQMR iterations, corrections, status);
+    status is OK or MAXIT."""
+    rel = ctypes.c_double()
+    its = ctypes.c_int()
+    steps = ctypes.c_int()
+    st = capi.call("culipx_sqmr_refine", handle._h, A._h, M._h, _dptr(b), _dptr(x), float(tol), float(inner_tol),
+                   int(inner_max_it), int(max_refine), ctypes.byref(rel), ctypes.byref(its), ctypes.byref(steps),
+                   allow=(capi.OK, capi.MAXIT))
+    return rel.value, its.value, steps.value, st
 
 
 def sqmr_solve_noalloc(handle: Handle, A: CsrOperator, M: Factor, b, x, tol=1e-8, max_it=1000):

@@ -77,6 +77,8 @@ _SIGS = {
     "culipx_spmv": [vp, vp, vp, f64, f64, i32],
     "culipx_sqmr_solve": [vp, vp, vp, vp, vp, f64, i32, ctypes.POINTER(f64), ctypes.POINTER(i32)],
     "culipx_sqmr_solve_noalloc": [vp, vp, vp, vp, vp, f64, i32, ctypes.POINTER(f64), ctypes.POINTER(i32)],
+    "culipx_sqmr_refine": [vp, vp, vp, vp, vp, f64, f64, i32, i32, ctypes.POINTER(f64), ctypes.POINTER(i32),
+                           ctypes.POINTER(i32)],
     "culipx_sqmr_profile": [vp, i32],
     "culipx_sqmr_phase_times": [vp, vp, i32],
 }

@@ -455,6 +455,18 @@ CULIPX_API int culipx_sqmr_phase_times(culipx_handle h, double* out_us, int iter
     return CULIPX_OK;
 }
 
+CULIPX_API int culipx_sqmr_refine(culipx_handle h, culipx_csr A, culipx_factor M, const double* d_b, double* d_x,
+                                  double tol, double inner_tol, int inner_max_it, int max_refine, double* relres,
+                                  int* iterations, int* steps)
+{
+    if (!h) return fail(CULIPX_INVALID_ARG, "null handle");
+    GUARD_BEGIN
+    CULIPX_TRY(use_device(h));
+    return sqmr_refine(h, A, M, d_b, d_x, tol, inner_tol, inner_max_it, max_refine, relres, iterations, steps,
+                       h->sqmr);
+    GUARD_END
+}
+
 CULIPX_API int culipx_sqmr_solve_noalloc(culipx_handle h, culipx_csr A, culipx_factor M, const double* d_b,
                                          double* d_x, double tol, int max_it, double* residual, int* iterations)
 {

@@ -15,6 +15,7 @@ struct Sqmr {
     bool profile = false;             // record per-phase device timestamps of the persistent solver
     DeviceBuffer ts;                  // 64 iterations x 8 phase stamps (ns, %globaltimer)
     DeviceBuffer vecs, partials, scal;
+    DeviceBuffer ref_r, ref_d, ref_part;  // iterative refinement: residual, correction, norm partials
     void* host_flags = nullptr;  // pinned
     ~Sqmr()
     {
@@ -27,6 +28,8 @@ int sqmr_solve(culipx_handle_t* h, Csr* A, Factor* M, const double* b, double* x
                double* residual, int* iterations, Sqmr* w);
 int sqmr_solve_persistent(culipx_handle_t* h, Csr* A, Factor* M, const double* b, double* x, double tol, int max_it,
                           double* residual, int* iterations, Sqmr* w);
+int sqmr_refine(culipx_handle_t* h, Csr* A, Factor* M, const double* b, double* x, double tol, double inner_tol,
+                int inner_max_it, int max_refine, double* relres, int* iterations, int* steps, Sqmr* w);
 int sqmr_solve_noalloc(culipx_handle_t* h, Csr* A, Factor* M, const double* b, double* x, double tol, int max_it,
                        double* residual, int* iterations);
 

@@ -220,6 +220,17 @@ int culipx_spmv(culipx_csr A, const void *d_x, void *d_y, double alpha, double b
 int culipx_sqmr_solve(culipx_handle h, culipx_csr A, culipx_factor M, const double *d_b,
                       double *d_x, double tol, int max_it, double *residual, int *iterations);
 
+/* FP64 iterative refinement around SQMR (no counterpart in the reference,
+ * whose SQMR solves once in the factor's precision): x = 0, r = b; while
+ * ||r|| > tol ||b|| and fewer than max_refine corrections: d = SQMR(K, M, r,
+ * inner_tol, inner_max_it), x += d, r = b - K x (FP64).  With an FP32 factor
+ * the preconditioner applies are single precision and everything else FP64.
+ * relres = ||b - K x|| / ||b||, iterations = SQMR iterations summed, steps =
+ * corrections.  Returns CULIPX_MAXIT if tol was not reached. */
+int culipx_sqmr_refine(culipx_handle h, culipx_csr A, culipx_factor M, const double *d_b, double *d_x,
+                       double tol, double inner_tol, int inner_max_it, int max_refine, double *relres,
+                       int *iterations, int *steps);
+
 /* Per-phase device timing of the persistent solver (no counterpart in the
  * reference, which has wall-clock timers only, libs/utils/defines.h:65-85):
  * enable, solve, then read for each of the first min(iterations, 64)

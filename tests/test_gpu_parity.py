@@ -8,6 +8,7 @@ import numpy as np
 import pytest
 
 import culip_b200 as cb
+from culip_b200 import _capi as capi
 import oracle
 from problems import kkt, random_spd_ish, scrambled_kkt
 
@@ -217,3 +218,29 @@ def test_sqmr_jacobi(handle):
     xg = xg.cpu().numpy()
     assert abs(its - ito) <= 4
     assert np.linalg.norm(xg - xo) / np.linalg.norm(xo) < 1e-6
+
+
+@pytest.mark.parametrize("precision", [cb.F32, cb.F64])
+def test_sqmr_refine_small(handle, precision):
+    """FP64 iterative refinement around SQMR reaches a true relative residual
+    the single FP32-factor solve cannot (1e-10); the returned relres is the
+    true one, and the solution agrees with the FP64 oracle's SQMR solve."""
+    rp, ci, v, bs = kkt("small")
+    P = cb.Pattern(handle, rp, ci, bs, 0, 1.0, precision)
+    F = cb.Factor(P)
+    dt = np.float32 if precision == cb.F32 else np.float64
+    F.compute(torch.from_numpy(v.astype(dt)).cuda())
+    b = cb.normal_vector(cb.SEED + 1, len(rp) - 1)
+    A = _csr_op(handle, rp, ci, v)
+    xg = torch.zeros(len(rp) - 1, dtype=torch.float64, device="cuda")
+    rel, its, steps, st = cb.sqmr_refine(handle, A, F, torch.from_numpy(b).cuda(), xg, 1e-10, 1e-6, 1000, 20)
+    import scipy.sparse as sp
+
+    K = sp.csr_matrix((v, ci, rp))
+    x = xg.cpu().numpy()
+    true_rel = np.linalg.norm(b - K @ x) / np.linalg.norm(b)
+    assert st == capi.OK and rel <= 1e-10 and steps >= 1
+    assert abs(true_rel - rel) <= 1e-3 * rel + 1e-15
+    S = oracle.Sym(rp, ci, bs, 0, 1.0)
+    xo, _, _ = oracle.sqmr(rp, ci, v, b, S.factor(v), 1e-12, 2000)
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < 1e-4
