@@ -221,7 +221,7 @@ class Factor:
         """Sizes of the solve structures of the last computed factor."""
         out = np.zeros(8, dtype=np.int64)
         capi.call("culipx_factor_info", self._h, out.ctypes.data_as(ctypes.c_void_p))
-        keys = ["u_nnz", "tiles", "tile_entries", "simple_rows", "blocks_2x2", "value_bytes"]
+        keys = ["u_nnz", "tiles", "tile_entries", "simple_rows", "blocks_2x2", "value_bytes", "granted_blocks"]
         return {k: int(v) for k, v in zip(keys, out)}
 
     def export(self) -> dict:
@@ -327,6 +327,56 @@ def sqmr_solve(handle: Handle, A: CsrOperator, M: Factor | None, b, x, tol=1e-8,
     st = capi.call("culipx_sqmr_solve", handle._h, A._h, M._h if M is not None else None, _dptr(b), _dptr(x),
                    float(tol), int(max_it), ctypes.byref(res), ctypes.byref(its), allow=(capi.OK, capi.MAXIT))
     return res.value, its.value, st
+
+
+def union_systems(systems):
+    """Block-diagonal union of independent systems, each (rowptr, colidx, val,
+    block_starts) with block_starts ending at its n.  Returns (rowptr, colidx,
+    val, block_starts, row_offsets) of the union."""
+    rps, cis, vs, bss, offs = [], [], [], [], [0]
+    nnz = 0
+    for rp, ci, v, bs in systems:
+        rp = np.asarray(rp, np.int64)
+        n0 = offs[-1]
+        rps.append(rp[:-1] + nnz)
+        cis.append(np.asarray(ci, np.int64) + n0)
+        vs.append(np.asarray(v))
+        b = np.asarray(bs, np.int64)
+        bss.append((b[:-1] if b[-1] == len(rp) - 1 else b) + n0)
+        nnz += int(rp[-1])
+        offs.append(n0 + len(rp) - 1)
+    rowptr = np.concatenate(rps + [np.array([nnz])]).astype(np.int32)
+    bs = np.concatenate(bss + [np.array([offs[-1]])]).astype(np.int32)
+    return rowptr, np.concatenate(cis).astype(np.int32), np.concatenate(vs), bs, np.asarray(offs, np.int32)
+
+
+class Batch:
+    """Independent systems stored as consecutive row ranges of one union
+    pattern, solved together by batch_sqmr_solve (one CTA per system)."""
+
+    def __init__(self, pattern: Pattern, row_offsets):
+        self.pattern = pattern
+        self.row_offsets = np.ascontiguousarray(row_offsets, np.int32)
+        self.num = len(self.row_offsets) - 1
+        h = ctypes.c_void_p()
+        capi.call("culipx_batch_create", pattern._h, self.num, _p(self.row_offsets), ctypes.byref(h))
+        self._h = h
+
+    def __del__(self):
+        try:
+            _release(self, "culipx_batch_destroy")
+        except Exception:  # interpreter shutdown
+            pass
+
+
+def batch_sqmr_solve(batch: Batch, A: CsrOperator, M: Factor, b, x, tol=1e-8, max_it=1000):
+    """Returns per-system (residual, iterations, status) numpy arrays."""
+    res = np.zeros(batch.num)
+    its = np.zeros(batch.num, np.int32)
+    st = np.zeros(batch.num, np.int32)
+    capi.call("culipx_batch_sqmr_solve", batch._h, A._h, M._h, _dptr(b), _dptr(x), float(tol), int(max_it), _p(res),
+              _p(its), _p(st))
+    return res, its, st
 
 
 def sqmr_refine(handle: Handle, A: CsrOperator, M: Factor, b, x, tol=1e-8, inner_tol=1e-6, inner_max_it=1000,

@@ -272,6 +272,11 @@ CULIPX_API int culipx_factor_info(culipx_factor f, long long* info8)
     CULIPX_CUDA(cudaMemcpy(&u_nnz, f->u_off.as<int>() + n, sizeof(int), cudaMemcpyDeviceToHost));
     CULIPX_CUDA(cudaMemcpy(&simple, f->scan_s.as<int>() + cm, sizeof(int), cudaMemcpyDeviceToHost));
     if (cm) CULIPX_CUDA(cudaMemcpy(flags.data(), f->rowflags.get(), cm * sizeof(int), cudaMemcpyDeviceToHost));
+    std::vector<int> extra(p.coarse_nnz);
+    if (p.coarse_nnz)
+        CULIPX_CUDA(cudaMemcpy(extra.data(), f->got_extra.get(), p.coarse_nnz * sizeof(int), cudaMemcpyDeviceToHost));
+    long long granted = 0;
+    for (int v : extra) granted += (v > 0);
     long long tiles = 0, tile_slots = 0, two = 0;
     for (int I = 0; I < cm; ++I) {
         const long long hI = p.bs[I + 1] - p.bs[I];
@@ -287,7 +292,7 @@ CULIPX_API int culipx_factor_info(culipx_factor f, long long* info8)
     info8[3] = simple;      // fine rows in simple block rows
     info8[4] = two;         // block rows with a 2x2 pivot
     info8[5] = f->vbytes;
-    info8[6] = 0;
+    info8[6] = granted;     // blocks that drew extra capacity from the dropping pass's leftover pool
     info8[7] = 0;
     return CULIPX_OK;
     GUARD_END
@@ -453,6 +458,39 @@ CULIPX_API int culipx_sqmr_phase_times(culipx_handle h, double* out_us, int iter
         for (int k = 0; k < 6; ++k) out_us[i * 6 + k] = t[3] ? d[k] : 0.0;
     }
     return CULIPX_OK;
+}
+
+CULIPX_API int culipx_batch_create(culipx_pattern p, int num_systems, const int* h_row_offsets,
+                                   culipx_batch* out)
+{
+    if (!p || !out) return fail(CULIPX_INVALID_ARG, "culipx_batch_create: null argument");
+    if (p->handle->device < 0) return fail(CULIPX_INVALID_ARG, "culipx_batch_create: host-only handle");
+    GUARD_BEGIN
+    CULIPX_TRY(use_device(p->handle));
+    Batch* b = nullptr;
+    CULIPX_TRY(batch_create(p->handle, p, num_systems, h_row_offsets, &b));
+    *out = static_cast<culipx_batch>(b);
+    return CULIPX_OK;
+    GUARD_END
+}
+
+CULIPX_API int culipx_batch_destroy(culipx_batch b)
+{
+    if (b) {
+        cudaSetDevice(b->h->device);
+        delete b;
+    }
+    return CULIPX_OK;
+}
+
+CULIPX_API int culipx_batch_sqmr_solve(culipx_batch b, culipx_csr A, culipx_factor M, const double* d_b, double* d_x,
+                                       double tol, int max_it, double* h_residual, int* h_iterations, int* h_status)
+{
+    if (!b) return fail(CULIPX_INVALID_ARG, "null batch");
+    GUARD_BEGIN
+    CULIPX_TRY(use_device(b->h));
+    return batch_sqmr_solve(b, A, M, d_b, d_x, tol, max_it, h_residual, h_iterations, h_status, b->h->sqmr);
+    GUARD_END
 }
 
 CULIPX_API int culipx_sqmr_refine(culipx_handle h, culipx_csr A, culipx_factor M, const double* d_b, double* d_x,

@@ -4,6 +4,8 @@
 #include "device.h"
 #include "spmv.h"
 
+#include <vector>
+
 namespace culipx {
 
 struct Factor;
@@ -23,6 +25,22 @@ struct Sqmr {
     }
 };
 
+// Independent systems stored as one block-diagonal union pattern: row ranges
+// and, per system and level, the positions of its block rows in the level lists.
+struct Pattern;
+struct Batch {
+    culipx_handle_t* h = nullptr;
+    const Pattern* pat = nullptr;
+    int num = 0, nl = 0;
+    std::vector<int> row_off;                 // num + 1
+    DeviceBuffer d_row_off, d_qb, d_qe;       // num + 1, num x nl, num x nl
+    DeviceBuffer d_out, d_next;               // num x 8 results, system counter
+};
+
+int batch_create(culipx_handle_t* h, const Pattern* p, int num, const int* h_row_off, Batch** out);
+int batch_sqmr_solve(Batch* bt, Csr* A, Factor* M, const double* b, double* x, double tol, int max_it,
+                     double* h_res, int* h_its, int* h_status, Sqmr* w);
+
 int sqmr_workspace(Sqmr* w, culipx_handle_t* h, int n);
 int sqmr_solve(culipx_handle_t* h, Csr* A, Factor* M, const double* b, double* x, double tol, int max_it,
                double* residual, int* iterations, Sqmr* w);
@@ -34,3 +52,5 @@ int sqmr_solve_noalloc(culipx_handle_t* h, Csr* A, Factor* M, const double* b, d
                        double* residual, int* iterations);
 
 }  // namespace culipx
+
+struct culipx_batch_t : culipx::Batch {};

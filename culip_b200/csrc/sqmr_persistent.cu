@@ -50,6 +50,7 @@
 // computes for a 1x1 pivot) and tri / is_piv for the others, and 9 vectors.
 #include "sqmr.h"
 #include "factor.h"
+#include "pattern.h"
 #include "kernels_common.cuh"
 
 #include <cooperative_groups.h>
@@ -416,18 +417,72 @@ __device__ void sym_ortho(double a, double b, double& c, double& s, double& r)
     }
 }
 
-template <class TF, int CTAS>
-__global__ void __launch_bounds__(kT, CTAS) k_sqmr_persistent(PArgs<TF> a)
+// Fixed-order sum over one CTA: thread 0 gets the totals (same protocol as
+// grid_reduce).
+template <int NV>
+__device__ void cta_reduce(double (&v)[NV], double (*sh)[kW])
 {
-    cg::grid_group grid = cg::this_grid();
-    __shared__ Scal S;
-    __shared__ double sh[kMaxNV][kW];
+    const int lane = (int)lane_id(), w = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < NV; ++k)
+        for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(kFull, v[k], o);
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) sh[k][w] = v[k];
+    __syncthreads();
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            double t = 0.0;
+            for (int i = 0; i < kW; ++i) t += sh[k][i];
+            v[k] = t;
+        }
+}
+
+// Where one solve runs: the whole grid of a cooperative launch (one system)
+// or one CTA of a batched launch (one system per CTA at a time).  Work items
+// go to warps wid, wid + nwarps, ...; vector loops to threads g0, g0 + gstride.
+struct GridCtx {
+    cg::grid_group grid;
+    double* partials;
+    int red;
+    int wid, nwarps, g0, gstride;
+    __device__ void sync() { grid.sync(); }
+    template <int NV>
+    __device__ void reduce(double (&v)[NV], double (*sh)[kW])
+    {
+        grid_reduce<NV>(v, partials, red, sh, grid);
+    }
+};
+
+struct CtaCtx {
+    int wid, nwarps, g0, gstride;
+    __device__ void sync() const { __syncthreads(); }
+    template <int NV>
+    __device__ void reduce(double (&v)[NV], double (*sh)[kW])
+    {
+        cta_reduce<NV>(v, sh);
+    }
+};
+
+// The system a solve works on: its rows [row0, row1) and, for each level L,
+// its block rows' positions [qb[L], qe[L]) in the level lists; out receives
+// [0] gamma/norm_pb, [1] iterations, [2] breakdown, [3] converged,
+// [4] norm_pb, [5] it.
+struct SysView {
+    int row0, row1;
+    const int* qb;
+    const int* qe;
+    double* out;
+};
+
+// The whole preconditioned SQMR solve of one system (see the top of the file).
+template <class TF, class Ctx>
+__device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal& S, double (*sh)[kW])
+{
     const int tid = threadIdx.x, lane = (int)lane_id();
-    const int n = a.n, G = gridDim.x;
-    const int g0 = blockIdx.x * kT + tid, gstride = G * kT;
-    const int wid = (tid >> 5) * G + blockIdx.x;  // work items interleaved across CTAs
-    const int nwarps = G * kW;
-    int red = 0;
+    const int wid = ctx.wid, nwarps = ctx.nwarps;
+    const int row0 = sv.row0, row1 = sv.row1;
     if (tid == 0) {
         memset(&S, 0, sizeof(S));
         S.c[0] = -1.0;
@@ -436,18 +491,18 @@ __global__ void __launch_bounds__(kT, CTAS) k_sqmr_persistent(PArgs<TF> a)
 
     // ---- init: v0 = U'^-1 P' b; ||v0|| ----
     for (int L = 0; L < a.nl; ++L) {
-        const int r0 = __ldg(a.lvl_off + L), nr = __ldg(a.lvl_off + L + 1) - r0;
+        const int r0 = __ldg(sv.qb + L), nr = __ldg(sv.qe + L) - r0;
         for (int t = wid; t < nr; t += nwarps) {
             const int I = __ldg(a.lvl_rows + r0 + t);
             const int fr = __ldg(a.bs + I), h = __ldg(a.bs + I + 1) - fr;
             ut_item<TF, false>(a, I, fr, h, __ldg(a.rowflags + I), a.b, 1.0, a.v[0]);
         }
-        grid.sync();
+        ctx.sync();
     }
     {
         double r[1] = {0.0};
-        for (int g = g0; g < n; g += gstride) r[0] = fma_rn(a.v[0][g], a.v[0][g], r[0]);
-        grid_reduce<1>(r, a.partials, red, sh, grid);
+        for (int g = row0 + ctx.g0; g < row1; g += ctx.gstride) r[0] = fma_rn(a.v[0][g], a.v[0][g], r[0]);
+        ctx.template reduce<1>(r, sh);
         if (tid == 0) {
             S.norm_pb = sqrt(r[0]);
             S.gamma = S.norm_pb;
@@ -460,7 +515,7 @@ __global__ void __launch_bounds__(kT, CTAS) k_sqmr_persistent(PArgs<TF> a)
     {
         const double inv_pb = S.inv_pb;
         for (int L = a.nl - 1; L >= 0; --L) {
-            const int r0 = __ldg(a.lvl_off + L), nr = __ldg(a.lvl_off + L + 1) - r0;
+            const int r0 = __ldg(sv.qb + L), nr = __ldg(sv.qe + L) - r0;
             for (int t = wid; t < nr; t += nwarps) {
                 const int I = __ldg(a.lvl_rows + r0 + t);
                 const int fr = __ldg(a.bs + I), h = __ldg(a.bs + I + 1) - fr;
@@ -472,14 +527,14 @@ __global__ void __launch_bounds__(kT, CTAS) k_sqmr_persistent(PArgs<TF> a)
                 const double d = u_item<TF>(a, I, fr, h, y, a.ev);
                 ww = fma_rn(d, d, ww);
             }
-            grid.sync();
+            ctx.sync();
         }
     }
     // Av = U'^-1 P' K ev; alpha's dots for iteration 0; eta_0 = 1/||D^-1 v0||
     {
         double r[3] = {ww, 0.0, 0.0};
         for (int L = 0; L < a.nl; ++L) {
-            const int r0 = __ldg(a.lvl_off + L), nr = __ldg(a.lvl_off + L + 1) - r0;
+            const int r0 = __ldg(sv.qb + L), nr = __ldg(sv.qe + L) - r0;
             for (int t = wid; t < nr; t += nwarps) {
                 const int I = __ldg(a.lvl_rows + r0 + t);
                 const int fr = __ldg(a.bs + I), h = __ldg(a.bs + I + 1) - fr;
@@ -494,9 +549,9 @@ __global__ void __launch_bounds__(kT, CTAS) k_sqmr_persistent(PArgs<TF> a)
                     r[2] = fma_rn(vs, dv, r[2]);
                 }
             }
-            if (L < a.nl - 1) grid.sync();
+            if (L < a.nl - 1) ctx.sync();
         }
-        grid_reduce<3>(r, a.partials, red, sh, grid);
+        ctx.template reduce<3>(r, sh);
         if (tid == 0) {
             S.eta = 1.0 / sqrt(r[0]);
             S.alpha_next = r[1] / r[2];
@@ -522,7 +577,7 @@ __global__ void __launch_bounds__(kT, CTAS) k_sqmr_persistent(PArgs<TF> a)
         {
             double r[1] = {0.0};
             for (int L = a.nl - 1; L >= 0; --L) {
-                const int q0 = __ldg(a.lvl_off + L), q1 = __ldg(a.lvl_off + L + 1);
+                const int q0 = __ldg(sv.qb + L), q1 = __ldg(sv.qe + L);
                 // block rows with a pivot tile, swaps or 2x2 pivots: warp per block row
                 const int c1 = __ldg(a.scan_c + q1);
                 for (int t = __ldg(a.scan_c + q0) + wid; t < c1; t += nwarps) {
@@ -542,7 +597,7 @@ __global__ void __launch_bounds__(kT, CTAS) k_sqmr_persistent(PArgs<TF> a)
                 // rows of simple block rows: thread per row (u_item with D = d,
                 // an identity tile and no swaps)
                 const int s1 = __ldg(a.scan_s + q1);
-                for (int i = __ldg(a.scan_s + q0) + g0; i < s1; i += gstride) {
+                for (int i = __ldg(a.scan_s + q0) + ctx.g0; i < s1; i += ctx.gstride) {
                     const int g = __ldg(a.simple_rows + i);
                     double y = a.Av[g];
                     y = fma_rn(na, vk[g], y);
@@ -554,11 +609,11 @@ __global__ void __launch_bounds__(kT, CTAS) k_sqmr_persistent(PArgs<TF> a)
                                                   a.ev);
                 }
                 if (L > 0) {
-                    grid.sync();
+                    ctx.sync();
                     if (L == a.nl - 1) stamp(a.ts, it, 1);
                 }
             }
-            grid_reduce<1>(r, a.partials, red, sh, grid);
+            ctx.template reduce<1>(r, sh);
             if (tid == 0) {
                 S.alpha = alpha;
                 const double bk = S.beta[k0];
@@ -593,7 +648,7 @@ __global__ void __launch_bounds__(kT, CTAS) k_sqmr_persistent(PArgs<TF> a)
             const double* const pkm1 = a.p[(it + 1) & 1];
             const double* const pkm2 = pk;  // read, then overwritten element by element
             for (int L = 0; L < a.nl; ++L) {
-                const int q0 = __ldg(a.lvl_off + L), q1 = __ldg(a.lvl_off + L + 1);
+                const int q0 = __ldg(sv.qb + L), q1 = __ldg(sv.qe + L);
                 const int c1 = __ldg(a.scan_c + q1);
                 for (int t = __ldg(a.scan_c + q0) + wid; t < c1; t += nwarps) {
                     const int I = __ldg(a.cplx + t);
@@ -626,7 +681,7 @@ __global__ void __launch_bounds__(kT, CTAS) k_sqmr_persistent(PArgs<TF> a)
                     }
                 }
                 const int s1 = __ldg(a.scan_s + q1);
-                for (int i = __ldg(a.scan_s + q0) + g0; i < s1; i += gstride) {
+                for (int i = __ldg(a.scan_s + q0) + ctx.g0; i < s1; i += ctx.gstride) {
                     const int g = __ldg(a.simple_rows + i);
                     const double y = spmv_row(a, g, a.ev) * sc;
                     const double av = (double)row_sub<TF>((TF)y, __ldg(a.ut_off + g), __ldg(a.ut_off + g + 1), a.ut_col,
@@ -650,11 +705,11 @@ __global__ void __launch_bounds__(kT, CTAS) k_sqmr_persistent(PArgs<TF> a)
                     r[2] = fma_rn(vs, dv, r[2]);
                 }
                 if (L < a.nl - 1) {
-                    grid.sync();
+                    ctx.sync();
                     if (L == 0) stamp(a.ts, it, 4);
                 }
             }
-            grid_reduce<4>(r, a.partials, red, sh, grid);
+            ctx.template reduce<4>(r, sh);
             if (tid == 0) {
                 const double bt = r[0] / S.vdv;
                 S.beta[k1] = bt;
@@ -692,25 +747,70 @@ __global__ void __launch_bounds__(kT, CTAS) k_sqmr_persistent(PArgs<TF> a)
     if (tid == 0 && !S.done) S.iters = it;
     __syncthreads();
     // ---- x = P U^-1 D^-1 x~ ----
-    for (int g = g0; g < n; g += gstride) a.tmp[g] = a.x[g];
-    grid.sync();
+    for (int g = row0 + ctx.g0; g < row1; g += ctx.gstride) a.tmp[g] = a.x[g];
+    ctx.sync();
     for (int L = a.nl - 1; L >= 0; --L) {
-        const int r0 = __ldg(a.lvl_off + L), nr = __ldg(a.lvl_off + L + 1) - r0;
+        const int r0 = __ldg(sv.qb + L), nr = __ldg(sv.qe + L) - r0;
         for (int t = wid; t < nr; t += nwarps) {
             const int I = __ldg(a.lvl_rows + r0 + t);
             const int fr = __ldg(a.bs + I), h = __ldg(a.bs + I + 1) - fr;
             const double y = (lane < h) ? a.tmp[fr + lane] : 0.0;
             u_item<TF>(a, I, fr, h, y, a.x);
         }
-        if (L > 0) grid.sync();
+        if (L > 0) ctx.sync();
     }
-    if (blockIdx.x == 0 && tid == 0) {
-        a.out[0] = S.gamma / S.norm_pb;
-        a.out[1] = S.iters;
-        a.out[2] = S.breakdown;
-        a.out[3] = (S.snap0 || S.snap1) ? 1 : 0;
-        a.out[4] = S.norm_pb;
-        a.out[5] = it;
+    if (sv.out && tid == 0) {
+        sv.out[0] = S.gamma / S.norm_pb;
+        sv.out[1] = S.iters;
+        sv.out[2] = S.breakdown;
+        sv.out[3] = (S.snap0 || S.snap1) ? 1 : 0;
+        sv.out[4] = S.norm_pb;
+        sv.out[5] = it;
+    }
+    __syncthreads();
+}
+
+template <class TF, int CTAS>
+__global__ void __launch_bounds__(kT, CTAS) k_sqmr_persistent(PArgs<TF> a)
+{
+    __shared__ Scal S;
+    __shared__ double sh[kMaxNV][kW];
+    const int G = gridDim.x;
+    GridCtx ctx{cg::this_grid(), a.partials, 0, (int)(threadIdx.x >> 5) * G + (int)blockIdx.x,  // items interleaved
+                G * kW, (int)(blockIdx.x * kT + threadIdx.x), G * kT};
+    const SysView sv{0, a.n, a.lvl_off, a.lvl_off + 1, blockIdx.x == 0 ? a.out : nullptr};
+    sqmr_body<TF>(a, ctx, sv, S, sh);
+}
+
+// Batched solves of independent systems stored as one block-diagonal union
+// (one pattern, one factor): each CTA takes the next unsolved system from a
+// counter and runs its whole SQMR with CTA barriers only.  A system's result
+// does not depend on the others or on which CTA solves it.
+struct BatchArgs {
+    int num;
+    const int* row_off;  // num + 1
+    const int* qb;       // num x nl
+    const int* qe;
+    double* out;         // num x 8
+    int* next;           // counter, 0 at launch
+};
+
+template <class TF>
+__global__ void __launch_bounds__(kT, kCtasPerSm) k_sqmr_batched(PArgs<TF> a, BatchArgs bt)
+{
+    __shared__ Scal S;
+    __shared__ double sh[kMaxNV][kW];
+    __shared__ int sys;
+    CtaCtx ctx{(int)(threadIdx.x >> 5), kW, (int)threadIdx.x, kT};
+    for (;;) {
+        if (threadIdx.x == 0) sys = atomicAdd(bt.next, 1);
+        __syncthreads();
+        const int s = sys;
+        __syncthreads();
+        if (s >= bt.num) break;
+        const SysView sv{__ldg(bt.row_off + s), __ldg(bt.row_off + s + 1), bt.qb + (size_t)s * a.nl,
+                         bt.qe + (size_t)s * a.nl, bt.out + (size_t)s * 8};
+        sqmr_body<TF>(a, ctx, sv, S, sh);
     }
 }
 
@@ -841,6 +941,129 @@ int launch_persistent(culipx_handle_t* h, Csr* A, Factor* M, const double* b, do
 }
 
 }  // namespace
+
+// ---------------------------------------------------------------------------
+// Batched solves (no counterpart in the reference, which solves one system
+// per SQMR object): systems given as consecutive row ranges of one
+// block-diagonal union pattern.
+namespace {
+
+template <class TF>
+int launch_batched(Batch* bt, Csr* A, Factor* M, const double* b, double* x, double tol, int max_it, Sqmr* w)
+{
+    culipx_handle_t* h = bt->h;
+    cudaStream_t s = h->stream;
+    const int n = A->m;
+    CULIPX_TRY(sqmr_workspace(w, h, n));
+    static int grid_cache[2] = {0, 0};
+    int& G = grid_cache[sizeof(TF) == 8 ? 0 : 1];
+    if (G == 0) {
+        int dev = 0, per_sm = 0, sms = 0;
+        CULIPX_CUDA(cudaGetDevice(&dev));
+        CULIPX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        CULIPX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sqmr_batched<TF>, kT, 0));
+        if (per_sm < 1) return fail(CULIPX_NOT_SUPPORTED, "batched SQMR kernel does not fit on an SM");
+        G = sms * std::min(per_sm, kCtasPerSm);
+    }
+    PArgs<TF> a = make_args<TF>(A, M, w->vecs.as<double>(), w->partials.as<double>(), b, x, tol, max_it);
+    BatchArgs ba;
+    ba.num = bt->num;
+    ba.row_off = bt->d_row_off.as<int>();
+    ba.qb = bt->d_qb.as<int>();
+    ba.qe = bt->d_qe.as<int>();
+    ba.out = bt->d_out.as<double>();
+    ba.next = bt->d_next.as<int>();
+    CULIPX_CUDA(cudaMemsetAsync(a.v[0], 0, (size_t)kVecs * n * sizeof(double), s));
+    CULIPX_CUDA(cudaMemsetAsync(x, 0, (size_t)n * sizeof(double), s));
+    CULIPX_CUDA(cudaMemsetAsync(ba.next, 0, sizeof(int), s));
+    k_sqmr_batched<TF><<<std::min(G, bt->num), kT, 0, s>>>(a, ba);
+    h->launches += 1;
+    return launch_check("k_sqmr_batched");
+}
+
+}  // namespace
+
+int batch_create(culipx_handle_t* h, const Pattern* p, int num, const int* h_row_off, Batch** out)
+{
+    if (!p || !h_row_off || !out || num < 1) return fail(CULIPX_INVALID_ARG, "culipx_batch_create: bad argument");
+    if (h_row_off[0] != 0 || h_row_off[num] != p->n)
+        return fail(CULIPX_INVALID_ARG, "culipx_batch_create: row offsets must run from 0 to n");
+    const int cm = p->num_blocks, nl = p->num_levels;
+    // system of every block row; every system boundary must be a block boundary
+    std::vector<int> sys(cm);
+    int s = 0;
+    for (int I = 0; I < cm; ++I) {
+        while (s < num && h_row_off[s + 1] <= p->bs[I]) ++s;
+        if (s >= num || h_row_off[s] > p->bs[I] || p->bs[I + 1] > h_row_off[s + 1])
+            return fail(CULIPX_INVALID_ARG, "culipx_batch_create: a system boundary splits block row %d", I);
+        sys[I] = s;
+    }
+    for (int k = 0; k < num; ++k)
+        if (h_row_off[k + 1] <= h_row_off[k]) return fail(CULIPX_INVALID_ARG, "culipx_batch_create: empty system %d", k);
+    // the systems must be independent: no block of the (filled) pattern couples two of them
+    for (int b = 0; b < p->coarse_nnz; ++b)
+        if (sys[p->blk_row[b]] != sys[p->blk_col[b]])
+            return fail(CULIPX_INVALID_ARG, "culipx_batch_create: block (%d, %d) couples systems %d and %d",
+                        p->blk_row[b], p->blk_col[b], sys[p->blk_row[b]], sys[p->blk_col[b]]);
+    // per system and level: its (contiguous) run in the level's ascending block list
+    std::vector<int> qb((size_t)num * std::max(nl, 1), 0), qe((size_t)num * std::max(nl, 1), 0);
+    for (int L = 0; L < nl; ++L)
+        for (int q = p->lvl_off[L]; q < p->lvl_off[L + 1]; ++q) {
+            const int k = sys[p->lvl_rows[q]];
+            int& b0 = qb[(size_t)k * nl + L];
+            int& e0 = qe[(size_t)k * nl + L];
+            if (e0 == b0) b0 = q;
+            else if (e0 != q) return fail(CULIPX_INVALID_ARG, "culipx_batch_create: level list not grouped by system");
+            e0 = q + 1;
+        }
+    auto* bt = new culipx_batch_t();
+    bt->h = h;
+    bt->pat = p;
+    bt->num = num;
+    bt->nl = nl;
+    bt->row_off.assign(h_row_off, h_row_off + num + 1);
+    int st = bt->d_row_off.upload(h, h_row_off, (size_t)(num + 1) * sizeof(int));
+    if (st == CULIPX_OK) st = bt->d_qb.upload(h, qb.data(), qb.size() * sizeof(int));
+    if (st == CULIPX_OK) st = bt->d_qe.upload(h, qe.data(), qe.size() * sizeof(int));
+    if (st == CULIPX_OK) st = bt->d_out.alloc(h, (size_t)num * 8 * sizeof(double));
+    if (st == CULIPX_OK) st = bt->d_next.alloc(h, sizeof(int));
+    if (st != CULIPX_OK) {
+        delete bt;
+        return st;
+    }
+    *out = bt;
+    return CULIPX_OK;
+}
+
+int batch_sqmr_solve(Batch* bt, Csr* A, Factor* M, const double* b, double* x, double tol, int max_it,
+                     double* h_res, int* h_its, int* h_status, Sqmr* w)
+{
+    if (!bt || !A || !M || !b || !x || !w) return fail(CULIPX_INVALID_ARG, "culipx_batch_sqmr_solve: null argument");
+    if (A->precision != CULIPX_F64 || A->m != A->n || A->m != bt->pat->n)
+        return fail(CULIPX_INVALID_ARG, "culipx_batch_sqmr_solve: A must be the FP64 union matrix of the batch");
+    if (!M->computed || M->pat != bt->pat)
+        return fail(CULIPX_INVALID_ARG, "culipx_batch_sqmr_solve: M must be a computed factor of the batch's pattern");
+    if (M->solve_algorithm == CULIPX_SOLVE_JACOBI)
+        return fail(CULIPX_NOT_SUPPORTED, "culipx_batch_sqmr_solve: SOLVE_JACOBI is not batched");
+    if (max_it < 0) return fail(CULIPX_INVALID_ARG, "culipx_batch_sqmr_solve: max_it < 0");
+    const int st = (M->precision == CULIPX_F64) ? launch_batched<double>(bt, A, M, b, x, tol, max_it, w)
+                                                : launch_batched<float>(bt, A, M, b, x, tol, max_it, w);
+    if (st != CULIPX_OK) return st;
+    std::vector<double> out((size_t)bt->num * 8);
+    CULIPX_CUDA(cudaMemcpyAsync(out.data(), bt->d_out.get(), out.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                                bt->h->stream));
+    CULIPX_CUDA(cudaStreamSynchronize(bt->h->stream));
+    for (int k = 0; k < bt->num; ++k) {
+        const double* o = out.data() + (size_t)k * 8;
+        if (h_res) h_res[k] = o[0];
+        if (h_its) h_its[k] = (int)o[1];
+        if (h_status)
+            h_status[k] = (o[2] != 0.0) ? CULIPX_BREAKDOWN
+                          : (o[3] == 0.0 && max_it > 0 && (int)o[1] >= max_it) ? CULIPX_MAXIT
+                                                                               : CULIPX_OK;
+    }
+    return CULIPX_OK;
+}
 
 int sqmr_solve_persistent(culipx_handle_t* h, Csr* A, Factor* M, const double* b, double* x, double tol, int max_it,
                           double* residual, int* iterations, Sqmr* w)

@@ -163,7 +163,8 @@ int culipx_factor_stats(culipx_factor f, double *ms, int *launches);
  * off-diagonal entries of U, [1] block rows with a non-identity pivot tile,
  * [2] upper-triangle entries of those tiles, [3] fine rows of simple block
  * rows (identity tile, no swaps, 1x1 pivots), [4] block rows with a 2x2
- * pivot, [5] bytes per value, [6..7] 0 */
+ * pivot, [5] bytes per value, [6] blocks that drew extra capacity from the
+ * dual-dropping pass's leftover pool (got_extra > 0), [7] 0 */
 int culipx_factor_info(culipx_factor f, long long *info8);
 
 /* set_solve_algorithm (block_ildlt.impl.cuh:253-258): algorithm one of
@@ -219,6 +220,27 @@ int culipx_spmv(culipx_csr A, const void *d_x, void *d_y, double alpha, double b
  * the reference returns; iterations as the reference counts them. */
 int culipx_sqmr_solve(culipx_handle h, culipx_csr A, culipx_factor M, const double *d_b,
                       double *d_x, double tol, int max_it, double *residual, int *iterations);
+
+/* Batched solves of independent systems (no counterpart in the reference,
+ * which solves one system per SQMR object).  The systems are stored as one
+ * block-diagonal union: consecutive row ranges h_row_offsets[k] ..
+ * h_row_offsets[k + 1] of one pattern / factor / CSR / b / x, each range a
+ * whole number of block rows and no block coupling two ranges (checked).
+ * One launch solves them all, each system by one CTA with its own SQMR
+ * scalars and stopping test (tol, max_it as culipx_sqmr_solve); a system's
+ * result does not depend on which other systems share the batch.  Per
+ * system: h_residual (gamma / ||M_L^-1 b||), h_iterations, h_status (OK,
+ * MAXIT or BREAKDOWN); any of the three may be NULL.  The factor of a union
+ * equals the systems' separate factors when no block draws extra capacity
+ * from the dual-dropping pass's leftover pool, which is one pool per
+ * factorization as in the reference (culipx_factor_info[6] == 0; always the
+ * case at level-0 fill of natural-order KKT systems, whose off-diagonal
+ * blocks keep K's pattern). */
+typedef struct culipx_batch_t *culipx_batch;
+int culipx_batch_create(culipx_pattern p, int num_systems, const int *h_row_offsets, culipx_batch *out);
+int culipx_batch_destroy(culipx_batch b);
+int culipx_batch_sqmr_solve(culipx_batch b, culipx_csr A, culipx_factor M, const double *d_b, double *d_x,
+                            double tol, int max_it, double *h_residual, int *h_iterations, int *h_status);
 
 /* FP64 iterative refinement around SQMR (no counterpart in the reference,
  * whose SQMR solves once in the factor's precision): x = 0, r = b; while
