@@ -379,6 +379,18 @@ def batch_sqmr_solve(batch: Batch, A: CsrOperator, M: Factor, b, x, tol=1e-8, ma
     return res, its, st
 
 
+def batch_sqmr_refine(batch: Batch, A: CsrOperator, M: Factor, b, x, tol=1e-8, inner_tol=1e-6, inner_max_it=1000,
+                      max_refine=20):
+    """Per-system (relres, iterations, corrections, status) numpy arrays."""
+    rel = np.zeros(batch.num)
+    its = np.zeros(batch.num, np.int32)
+    steps = np.zeros(batch.num, np.int32)
+    st = np.zeros(batch.num, np.int32)
+    capi.call("culipx_batch_sqmr_refine", batch._h, A._h, M._h, _dptr(b), _dptr(x), float(tol), float(inner_tol),
+              int(inner_max_it), int(max_refine), _p(rel), _p(its), _p(steps), _p(st))
+    return rel, its, steps, st
+
+
 def sqmr_refine(handle: Handle, A: CsrOperator, M: Factor, b, x, tol=1e-8, inner_tol=1e-6, inner_max_it=1000,
                 max_refine=20):
     """FP64 iterative refinement around SQMR (mixed precision with an FP32

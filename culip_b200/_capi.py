@@ -80,6 +80,7 @@ _SIGS = {
     "culipx_batch_create": [vp, i32, vp, ctypes.POINTER(vp)],
     "culipx_batch_destroy": [vp],
     "culipx_batch_sqmr_solve": [vp, vp, vp, vp, vp, f64, i32, vp, vp, vp],
+    "culipx_batch_sqmr_refine": [vp, vp, vp, vp, vp, f64, f64, i32, i32, vp, vp, vp, vp],
     "culipx_sqmr_refine": [vp, vp, vp, vp, vp, f64, f64, i32, i32, ctypes.POINTER(f64), ctypes.POINTER(i32),
                            ctypes.POINTER(i32)],
     "culipx_sqmr_profile": [vp, i32],

@@ -493,6 +493,18 @@ CULIPX_API int culipx_batch_sqmr_solve(culipx_batch b, culipx_csr A, culipx_fact
     GUARD_END
 }
 
+CULIPX_API int culipx_batch_sqmr_refine(culipx_batch b, culipx_csr A, culipx_factor M, const double* d_b,
+                                        double* d_x, double tol, double inner_tol, int inner_max_it, int max_refine,
+                                        double* h_relres, int* h_iterations, int* h_steps, int* h_status)
+{
+    if (!b) return fail(CULIPX_INVALID_ARG, "null batch");
+    GUARD_BEGIN
+    CULIPX_TRY(use_device(b->h));
+    return batch_sqmr_refine(b, A, M, d_b, d_x, tol, inner_tol, inner_max_it, max_refine, h_relres, h_iterations,
+                             h_steps, h_status, b->h->sqmr);
+    GUARD_END
+}
+
 CULIPX_API int culipx_sqmr_refine(culipx_handle h, culipx_csr A, culipx_factor M, const double* d_b, double* d_x,
                                   double tol, double inner_tol, int inner_max_it, int max_refine, double* relres,
                                   int* iterations, int* steps)

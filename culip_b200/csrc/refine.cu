@@ -16,6 +16,7 @@
 #include "factor.h"
 #include "kernels_common.cuh"
 
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -59,7 +60,119 @@ int norm2(const double* v, int n, double* part_d, double* part_h, cudaStream_t s
     return CULIPX_OK;
 }
 
+// per system k: sum of squares of v over rows row_off[k] .. row_off[k+1]
+// (one CTA per system, fixed order)
+__global__ void k_seg_sumsq(const double* __restrict__ v, const int* __restrict__ row_off, int num,
+                            double* __restrict__ out)
+{
+    __shared__ double sh[kRT / 32];
+    for (int k = blockIdx.x; k < num; k += gridDim.x) {
+        double s = 0.0;
+        for (int g = row_off[k] + threadIdx.x; g < row_off[k + 1]; g += kRT) s = fma_rn(v[g], v[g], s);
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+        if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double t = 0.0;
+            for (int i = 0; i < kRT / 32; ++i) t += sh[i];
+            out[k] = t;
+        }
+        __syncthreads();
+    }
+}
+
+// rows of the systems with keep[k] == 0 set to zero
+__global__ void k_seg_mask(double* __restrict__ v, const int* __restrict__ row_off, int num,
+                           const int* __restrict__ keep)
+{
+    for (int k = blockIdx.x; k < num; k += gridDim.x)
+        if (!keep[k])
+            for (int g = row_off[k] + threadIdx.x; g < row_off[k + 1]; g += kRT) v[g] = 0.0;
+}
+
+int seg_norms(const double* v, Batch* bt, double* d_out, std::vector<double>& h_out, cudaStream_t s)
+{
+    k_seg_sumsq<<<std::min(bt->num, 148 * 8), kRT, 0, s>>>(v, bt->d_row_off.as<int>(), bt->num, d_out);
+    bt->h->launches += 1;
+    CULIPX_TRY(launch_check("k_seg_sumsq"));
+    CULIPX_CUDA(cudaMemcpyAsync(h_out.data(), d_out, bt->num * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CULIPX_CUDA(cudaStreamSynchronize(s));
+    for (double& t : h_out) t = std::sqrt(t);
+    return CULIPX_OK;
+}
+
 }  // namespace
+
+// Batched refinement: the loop above per system, all systems' corrections in
+// one batched SQMR launch per step; systems that reached tol get a zero
+// right-hand side (their correction is zero) and stop counting steps.
+int batch_sqmr_refine(Batch* bt, Csr* A, Factor* M, const double* b, double* x, double tol, double inner_tol,
+                      int inner_max_it, int max_refine, double* h_relres, int* h_its, int* h_steps, int* h_status,
+                      Sqmr* w)
+{
+    if (!bt || !A || !M || !b || !x || !w) return fail(CULIPX_INVALID_ARG, "culipx_batch_sqmr_refine: null argument");
+    if (!(tol >= 0.0) || !(inner_tol >= 0.0) || inner_max_it < 0 || max_refine < 0)
+        return fail(CULIPX_INVALID_ARG, "culipx_batch_sqmr_refine: bad tolerance or limit");
+    culipx_handle_t* h = bt->h;
+    const int n = A->m, num = bt->num;
+    cudaStream_t s = h->stream;
+    const size_t vb = (size_t)n * sizeof(double);
+    if (w->ref_r.bytes() < vb + 16) CULIPX_TRY(w->ref_r.alloc(h, vb + 16));
+    if (w->ref_d.bytes() < vb + 16) CULIPX_TRY(w->ref_d.alloc(h, vb + 16));
+    const size_t pb = std::max<size_t>((size_t)num * (sizeof(double) + sizeof(int)), kRGrid * sizeof(double));
+    if (w->ref_part.bytes() < pb) CULIPX_TRY(w->ref_part.alloc(h, pb));
+    double* r = w->ref_r.as<double>();
+    double* d = w->ref_d.as<double>();
+    double* sums = w->ref_part.as<double>();
+    int* keep_d = reinterpret_cast<int*>(sums + num);
+    std::vector<double> nb(num), nr(num);
+    std::vector<int> keep(num), its(num, 0), steps(num, 0), st(num, CULIPX_OK), it_k(num), st_k(num);
+    CULIPX_CUDA(cudaMemsetAsync(x, 0, vb, s));
+    CULIPX_TRY(seg_norms(b, bt, sums, nb, s));
+    std::vector<double> rel(num);
+    for (int k = 0; k < num; ++k) rel[k] = nb[k] > 0.0 ? 1.0 : 0.0;
+    for (int step = 0; step < max_refine; ++step) {
+        int active = 0;
+        for (int k = 0; k < num; ++k) {
+            keep[k] = rel[k] > tol && st[k] != CULIPX_BREAKDOWN;
+            active += keep[k];
+        }
+        if (!active) break;
+        // r = b - K x on the active systems, zero elsewhere
+        CULIPX_CUDA(cudaMemcpyAsync(r, b, vb, cudaMemcpyDeviceToDevice, s));
+        if (step > 0) {
+            CULIPX_TRY(csr_spmv(A, x, r, -1.0, 1.0, 0, s));
+            h->launches += 1;
+        }
+        CULIPX_CUDA(cudaMemcpyAsync(keep_d, keep.data(), num * sizeof(int), cudaMemcpyHostToDevice, s));
+        k_seg_mask<<<std::min(num, 148 * 8), kRT, 0, s>>>(r, bt->d_row_off.as<int>(), num, keep_d);
+        h->launches += 1;
+        CULIPX_TRY(launch_check("k_seg_mask"));
+        CULIPX_TRY(batch_sqmr_solve(bt, A, M, r, d, inner_tol, inner_max_it, nullptr, it_k.data(), st_k.data(), w));
+        k_add<<<kRGrid, kRT, 0, s>>>(x, d, n);
+        h->launches += 1;
+        CULIPX_TRY(launch_check("k_add"));
+        CULIPX_CUDA(cudaMemcpyAsync(r, b, vb, cudaMemcpyDeviceToDevice, s));
+        CULIPX_TRY(csr_spmv(A, x, r, -1.0, 1.0, 0, s));
+        h->launches += 1;
+        CULIPX_TRY(seg_norms(r, bt, sums, nr, s));
+        for (int k = 0; k < num; ++k) {
+            if (!keep[k]) continue;
+            its[k] += it_k[k];
+            steps[k] += 1;
+            rel[k] = nr[k] / nb[k];
+            if (st_k[k] == CULIPX_BREAKDOWN || !std::isfinite(rel[k])) st[k] = CULIPX_BREAKDOWN;
+        }
+    }
+    for (int k = 0; k < num; ++k) {
+        if (st[k] != CULIPX_BREAKDOWN) st[k] = rel[k] <= tol ? CULIPX_OK : CULIPX_MAXIT;
+        if (h_relres) h_relres[k] = rel[k];
+        if (h_its) h_its[k] = its[k];
+        if (h_steps) h_steps[k] = steps[k];
+        if (h_status) h_status[k] = st[k];
+    }
+    return CULIPX_OK;
+}
 
 int sqmr_refine(culipx_handle_t* h, Csr* A, Factor* M, const double* b, double* x, double tol, double inner_tol,
                 int inner_max_it, int max_refine, double* relres, int* iterations, int* steps, Sqmr* w)

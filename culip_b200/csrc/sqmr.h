@@ -41,6 +41,10 @@ int batch_create(culipx_handle_t* h, const Pattern* p, int num, const int* h_row
 int batch_sqmr_solve(Batch* bt, Csr* A, Factor* M, const double* b, double* x, double tol, int max_it,
                      double* h_res, int* h_its, int* h_status, Sqmr* w);
 
+int batch_sqmr_refine(Batch* bt, Csr* A, Factor* M, const double* b, double* x, double tol, double inner_tol,
+                      int inner_max_it, int max_refine, double* h_relres, int* h_its, int* h_steps, int* h_status,
+                      Sqmr* w);
+
 int sqmr_workspace(Sqmr* w, culipx_handle_t* h, int n);
 int sqmr_solve(culipx_handle_t* h, Csr* A, Factor* M, const double* b, double* x, double tol, int max_it,
                double* residual, int* iterations, Sqmr* w);

@@ -242,6 +242,14 @@ int culipx_batch_destroy(culipx_batch b);
 int culipx_batch_sqmr_solve(culipx_batch b, culipx_csr A, culipx_factor M, const double *d_b, double *d_x,
                             double tol, int max_it, double *h_residual, int *h_iterations, int *h_status);
 
+/* culipx_sqmr_refine per system of a batch: every step solves all systems
+ * still above tol in one batched launch (the others get a zero right-hand
+ * side); per system the true relative residual, the SQMR iterations summed,
+ * the corrections taken and a status (OK, MAXIT, BREAKDOWN). */
+int culipx_batch_sqmr_refine(culipx_batch b, culipx_csr A, culipx_factor M, const double *d_b, double *d_x,
+                             double tol, double inner_tol, int inner_max_it, int max_refine, double *h_relres,
+                             int *h_iterations, int *h_steps, int *h_status);
+
 /* FP64 iterative refinement around SQMR (no counterpart in the reference,
  * whose SQMR solves once in the factor's precision): x = 0, r = b; while
  * ||r|| > tol ||b|| and fewer than max_refine corrections: d = SQMR(K, M, r,
