@@ -140,7 +140,7 @@ class Pattern:
     """Symbolic analysis of one sparsity pattern (BlockiLDLt ctor + symbolic part of compute())."""
 
     def __init__(self, handle: Handle, rowptr, colidx, block_starts, fill_level=0, fill_factor=1.0,
-                 precision=F64):
+                 precision=F64, system_row_offsets=None):
         self.handle = handle
         self.rowptr = np.ascontiguousarray(rowptr, np.int32)
         self.colidx = np.ascontiguousarray(colidx, np.int32)
@@ -151,8 +151,14 @@ class Pattern:
         self.num_blocks = len(bs)
         self.precision = precision
         p = ctypes.c_void_p()
-        capi.call("culipx_pattern_analyze", handle._h, self.n, _p(self.rowptr), _p(self.colidx), self.num_blocks,
-                  _p(bs), int(fill_level), float(fill_factor), int(precision), ctypes.byref(p))
+        if system_row_offsets is None:
+            capi.call("culipx_pattern_analyze", handle._h, self.n, _p(self.rowptr), _p(self.colidx), self.num_blocks,
+                      _p(bs), int(fill_level), float(fill_factor), int(precision), ctypes.byref(p))
+        else:
+            so = np.ascontiguousarray(system_row_offsets, np.int32)
+            capi.call("culipx_pattern_analyze_systems", handle._h, self.n, _p(self.rowptr), _p(self.colidx),
+                      self.num_blocks, _p(bs), int(fill_level), float(fill_factor), int(precision), len(so) - 1,
+                      _p(so), ctypes.byref(p))
         self._h = p
 
     def info(self) -> dict:

@@ -54,6 +54,7 @@ _SIGS = {
     "culipx_handle_synchronize": [vp],
     "culipx_handle_launch_count": [vp, ctypes.POINTER(i64), i32],
     "culipx_pattern_analyze": [vp, i32, vp, vp, i32, vp, i32, f64, i32, ctypes.POINTER(vp)],
+    "culipx_pattern_analyze_systems": [vp, i32, vp, vp, i32, vp, i32, f64, i32, i32, vp, ctypes.POINTER(vp)],
     "culipx_pattern_destroy": [vp],
     "culipx_pattern_info": [vp, vp],
     "culipx_pattern_export": [vp] * 12,

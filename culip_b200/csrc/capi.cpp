@@ -131,6 +131,23 @@ CULIPX_API int culipx_pattern_analyze(culipx_handle h, int n, const int* h_rowpt
     GUARD_END
 }
 
+CULIPX_API int culipx_pattern_analyze_systems(culipx_handle h, int n, const int* h_rowptr, const int* h_colidx,
+                                              int num_blocks, const int* h_block_starts, int fill_level,
+                                              double fill_factor, int precision, int num_systems,
+                                              const int* h_row_offsets, culipx_pattern* out)
+{
+    if (!h) return fail(CULIPX_INVALID_ARG, "null handle");
+    if (num_systems < 1 || !h_row_offsets) return fail(CULIPX_INVALID_ARG, "culipx_pattern_analyze_systems: bad systems");
+    GUARD_BEGIN
+    CULIPX_TRY(use_device(h));
+    Pattern* p = nullptr;
+    CULIPX_TRY(analyze_pattern(h, n, h_rowptr, h_colidx, num_blocks, h_block_starts, fill_level, fill_factor,
+                               precision, &p, num_systems, h_row_offsets));
+    *out = static_cast<culipx_pattern>(p);
+    return CULIPX_OK;
+    GUARD_END
+}
+
 CULIPX_API int culipx_pattern_destroy(culipx_pattern p)
 {
     if (p) {

@@ -64,7 +64,7 @@ struct Pattern {
 // Builds the analysis on the host and uploads the device mirror.
 int analyze_pattern(culipx_handle_t* h, int n, const int* rowptr, const int* colidx,
                     int num_blocks, const int* block_starts, int fill_level, double fill_factor,
-                    int precision, Pattern** out);
+                    int precision, Pattern** out, int num_systems = 1, const int* system_row_offsets = nullptr);
 
 }  // namespace culipx
 

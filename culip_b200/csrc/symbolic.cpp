@@ -125,7 +125,7 @@ void coarse_pattern(Pattern& p, const int* rowptr, const int* colidx)
 
 int analyze_pattern(culipx_handle_t* h, int n, const int* rowptr, const int* colidx,
                     int num_blocks, const int* block_starts, int fill_level, double fill_factor,
-                    int precision, Pattern** out)
+                    int precision, Pattern** out, int num_systems, const int* system_row_offsets)
 {
     if (!out || !rowptr || !colidx || !block_starts || n <= 0 || num_blocks <= 0 || num_blocks > n)
         return fail(CULIPX_INVALID_ARG, "culipx_pattern_analyze: bad arguments");
@@ -157,6 +157,29 @@ int analyze_pattern(culipx_handle_t* h, int n, const int* rowptr, const int* col
         }
     }
     if (p.bs[0] != 0) { delete pp; return fail(CULIPX_INVALID_ARG, "culipx_pattern_analyze: block_starts[0] != 0"); }
+    // systems of a block-diagonal union (default: one system): per block row
+    // its system's first block row and block count, for the format rule
+    std::vector<int> sys_first(cm, 0), sys_blocks(cm, cm);
+    if (num_systems > 1 && system_row_offsets) {
+        if (system_row_offsets[0] != 0 || system_row_offsets[num_systems] != n) {
+            delete pp;
+            return fail(CULIPX_INVALID_ARG, "culipx_pattern_analyze_systems: row offsets must run from 0 to n");
+        }
+        int b0 = 0;
+        for (int k = 0; k < num_systems; ++k) {
+            int b1 = b0;
+            while (b1 < cm && p.bs[b1] < system_row_offsets[k + 1]) ++b1;
+            if (p.bs[b0] != system_row_offsets[k] || p.bs[b1] != system_row_offsets[k + 1] || b1 == b0) {
+                delete pp;
+                return fail(CULIPX_INVALID_ARG, "culipx_pattern_analyze_systems: system %d does not start and end on block boundaries", k);
+            }
+            for (int I = b0; I < b1; ++I) {
+                sys_first[I] = b0;
+                sys_blocks[I] = b1 - b0;
+            }
+            b0 = b1;
+        }
+    }
     for (int i = 0; i < n; ++i)
         for (int q = rowptr[i]; q < rowptr[i + 1]; ++q)
             if (colidx[q] < 0 || colidx[q] >= n || (q > rowptr[i] && colidx[q] <= colidx[q - 1])) {
@@ -278,7 +301,8 @@ int analyze_pattern(culipx_handle_t* h, int n, const int* rowptr, const int* col
             const size_t vb = dbl ? 8 : 4;
             const double lhs = (double)((4 + vb) * (size_t)(long long)mx);
             const double rhs = dbl ? 0.5 * 8.0 * (double)r * (double)c : (double)(0.5f * 4.0f * (float)r * (float)c);
-            const bool sparse = (I != J) && ((double)I < 0.9 * (double)cm) && (lhs < rhs);
+            // the last 10 % of a system's block rows keep dense blocks
+            const bool sparse = (I != J) && ((double)(I - sys_first[I]) < 0.9 * (double)sys_blocks[I]) && (lhs < rhs);
             p.fmt[q] = sparse ? kSparse : kDense;
             if (sparse) ++p.num_sparse; else ++p.num_dense;
         }

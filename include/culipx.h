@@ -119,6 +119,15 @@ int culipx_handle_launch_count(culipx_handle h, long long *count, int reset);
 int culipx_pattern_analyze(culipx_handle h, int n, const int *h_rowptr, const int *h_colidx,
                            int num_blocks, const int *h_block_starts, int fill_level,
                            double fill_factor, int precision, culipx_pattern *out);
+/* The same for a block-diagonal union of independent systems (rows
+ * h_row_offsets[k] .. h_row_offsets[k + 1], each on block boundaries): the
+ * reference's rule that the last 10 % of block rows keep dense blocks
+ * (build_blocks, block_ildlt.impl.cuh:1015-1280) is applied per system, so
+ * block formats equal those of the separate analyses.  For culipx_batch_*. */
+int culipx_pattern_analyze_systems(culipx_handle h, int n, const int *h_rowptr, const int *h_colidx,
+                                   int num_blocks, const int *h_block_starts, int fill_level,
+                                   double fill_factor, int precision, int num_systems,
+                                   const int *h_row_offsets, culipx_pattern *out);
 int culipx_pattern_destroy(culipx_pattern p);
 /* info[0..15]: n, nnz, num_blocks, coarse_nnz, fill_nnz, num_levels, num_sparse,
  * num_dense, val_slots, idx_slots, max_level_blocks, max_level_rows,

@@ -42,7 +42,7 @@ def _solve_batch(handle, syst, precision=cb.F64, tol=1e-8, max_it=1000, rhs=None
     import torch
 
     rp, ci, v, bs, off = cb.union_systems(syst)
-    P = cb.Pattern(handle, rp, ci, bs, 0, 1.0, precision)
+    P = cb.Pattern(handle, rp, ci, bs, 0, 1.0, precision, system_row_offsets=off)
     F = cb.Factor(P)
     dt = np.float64 if precision == cb.F64 else np.float32
     F.compute(torch.from_numpy(v.astype(dt)).cuda())
@@ -159,7 +159,7 @@ def test_batch_refine_fp32_reaches_tol():
     h = cb.Handle(0)
     syst = _systems(6, seed=21)
     rp, ci, v, bs, off = cb.union_systems(syst)
-    P = cb.Pattern(h, rp, ci, bs, 0, 1.0, cb.F32)
+    P = cb.Pattern(h, rp, ci, bs, 0, 1.0, cb.F32, system_row_offsets=off)
     F = cb.Factor(P)
     F.compute(torch.from_numpy(v.astype(np.float32)).cuda())
     A = cb.CsrOperator(h, torch.from_numpy(rp).cuda(), torch.from_numpy(ci).cuda(), torch.from_numpy(v).cuda())
@@ -174,3 +174,29 @@ def test_batch_refine_fp32_reaches_tol():
         true_rel = np.linalg.norm(bk - K @ xs[off[k]:off[k + 1]]) / np.linalg.norm(bk)
         assert st[k] == capi.OK and rel[k] <= 1e-10 and steps[k] >= 1
         assert abs(true_rel - rel[k]) <= 1e-3 * rel[k] + 1e-15
+
+
+def test_union_analysis_formats_equal_separate_analyses():
+    """With system boundaries, the union's block formats and fill caps are the
+    concatenation of the separate analyses' (host-only handle, no GPU)."""
+    import ctypes
+
+    class HostHandle:
+        def __init__(self):
+            self._h = ctypes.c_void_p()
+            capi.call("culipx_handle_create", ctypes.byref(self._h), -1, None)
+
+    hh = HostHandle()
+    syst = _systems(4, seed=5)
+    rp, ci, v, bs, off = cb.union_systems(syst)
+    U = cb.Pattern(hh, rp, ci, bs, 0, 1.0, cb.F32, system_row_offsets=off).export()
+    fmts, mx = [], []
+    for s in syst:
+        E = cb.Pattern(hh, s[0], s[1], s[3], 0, 1.0, cb.F32).export()
+        fmts.append(E["fmt"])
+        mx.append(E["max_nnz"])
+    assert np.array_equal(U["fmt"], np.concatenate(fmts))
+    assert np.array_equal(U["max_nnz"], np.concatenate(mx))
+    with pytest.raises(cb.CulipxError):
+        cb.Pattern(hh, rp, ci, bs, 0, 1.0, cb.F32, system_row_offsets=[0, off[1] + 1, off[-1]])
+    capi.load().culipx_handle_destroy(hh._h)
