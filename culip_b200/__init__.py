@@ -385,6 +385,91 @@ def batch_sqmr_solve(batch: Batch, A: CsrOperator, M: Factor, b, x, tol=1e-8, ma
     return res, its, st
 
 
+class Server:
+    """Continuous-batching request server (culipx_server_*): patterns analysed
+    once, requests (K's values + right-hand sides, host numpy) admitted by
+    device memory into batched launches on several streams."""
+
+    def __init__(self, device=0, memory_budget=0, slots=2, max_batch=256, tol=1e-8, max_it=1000):
+        h = ctypes.c_void_p()
+        capi.call("culipx_server_create", int(device), int(memory_budget), int(slots), int(max_batch), float(tol),
+                  int(max_it), ctypes.byref(h))
+        self._h = h
+        self.patterns = []
+
+    def add_pattern(self, rowptr, colidx, block_starts, precision=F64) -> int:
+        rp = np.ascontiguousarray(rowptr, np.int32)
+        ci = np.ascontiguousarray(colidx, np.int32)
+        bs = np.ascontiguousarray(block_starts, np.int32)
+        n = len(rp) - 1
+        if bs[-1] == n:
+            bs = bs[:-1]
+        pid = ctypes.c_int()
+        capi.call("culipx_server_add_pattern", self._h, n, _p(rp), _p(ci), len(bs), _p(bs), int(precision),
+                  ctypes.byref(pid))
+        self.patterns.append((n, len(ci)))
+        return pid.value
+
+    def submit(self, pid, vals, b) -> int:
+        v = np.ascontiguousarray(vals, np.float64)
+        b = np.asarray(b, np.float64)
+        nrhs = 1 if b.ndim == 1 else b.shape[1]
+        bb = np.ascontiguousarray(b.reshape(-1, nrhs).T if b.ndim == 2 else b)
+        rid = ctypes.c_int()
+        capi.call("culipx_server_submit", self._h, int(pid), _p(v), nrhs, _p(bb), ctypes.byref(rid))
+        self._meta = getattr(self, "_meta", {})
+        self._meta[rid.value] = (pid, nrhs)
+        return rid.value
+
+    def progress(self, wait=False) -> int:
+        c = ctypes.c_int()
+        capi.call("culipx_server_progress", self._h, 1 if wait else 0, ctypes.byref(c))
+        return c.value
+
+    def result(self, rid):
+        """None while pending, else (x (n x nrhs), iterations, status, latency_ms)."""
+        pid, nrhs = self._meta[rid]
+        n = self.patterns[pid][0]
+        x = np.zeros(n * nrhs)
+        its = np.zeros(nrhs, np.int32)
+        st = np.zeros(nrhs, np.int32)
+        lat = ctypes.c_double()
+        s = capi.call("culipx_server_result", self._h, int(rid), _p(x), _p(its), _p(st), ctypes.byref(lat),
+                      allow=(capi.OK, capi.PENDING))
+        if s == capi.PENDING:
+            return None
+        return x.reshape(nrhs, n).T, its, st, lat.value
+
+    def release(self, rid):
+        capi.call("culipx_server_release", self._h, int(rid))
+        self._meta.pop(rid, None)
+
+    def stats(self) -> dict:
+        v = np.zeros(8, np.int64)
+        capi.call("culipx_server_stats", self._h, _p(v))
+        keys = ["queued", "running", "done", "batches", "running_bytes", "held_bytes", "patterns"]
+        return {k: int(x) for k, x in zip(keys, v)}
+
+    def __del__(self):
+        try:
+            _release(self, "culipx_server_destroy")
+        except Exception:  # interpreter shutdown
+            pass
+
+
+def sqmr_solve_many(handle: Handle, As, Ms, bs, xs, tol=1e-8, max_it=1000):
+    """Independent systems with their own factors, one launch; per-system
+    (residual, iterations, status) numpy arrays."""
+    num = len(As)
+    arr = lambda objs: (ctypes.c_void_p * num)(*[o._h.value if hasattr(o, "_h") else o for o in objs])
+    res = np.zeros(num)
+    its = np.zeros(num, np.int32)
+    st = np.zeros(num, np.int32)
+    capi.call("culipx_sqmr_solve_many", handle._h, num, arr(As), arr(Ms), arr([t.data_ptr() for t in bs]),
+              arr([t.data_ptr() for t in xs]), float(tol), int(max_it), _p(res), _p(its), _p(st))
+    return res, its, st
+
+
 def batch_sqmr_refine(batch: Batch, A: CsrOperator, M: Factor, b, x, tol=1e-8, inner_tol=1e-6, inner_max_it=1000,
                       max_refine=20):
     """Per-system (relres, iterations, corrections, status) numpy arrays."""

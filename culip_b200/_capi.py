@@ -12,14 +12,14 @@ import os
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "lib", "libculipx.so")
 
-OK, INVALID_ARG, OOM, BREAKDOWN, MAXIT, TIMEOUT, CUDA_ERROR, NOT_SUPPORTED = range(8)
+OK, INVALID_ARG, OOM, BREAKDOWN, MAXIT, TIMEOUT, CUDA_ERROR, NOT_SUPPORTED, PENDING = range(9)
 F64, F32 = 0, 1
 PIV_STATIC, PIV_BK, PIV_ROOK = 0, 1, 2
 LEFT, MIDDLE, RIGHT = 0, 1, 2
 SOLVE_STRIPE, SOLVE_BLOCK, SOLVE_SCALAR, SOLVE_JACOBI = 0, 1, 2, 3
 
 STATUS_NAMES = {0: "OK", 1: "INVALID_ARG", 2: "OOM", 3: "BREAKDOWN", 4: "MAXIT", 5: "TIMEOUT", 6: "CUDA_ERROR",
-                7: "NOT_SUPPORTED"}
+                7: "NOT_SUPPORTED", 8: "PENDING"}
 
 
 class CulipxError(RuntimeError):
@@ -81,6 +81,15 @@ _SIGS = {
     "culipx_batch_create": [vp, i32, vp, ctypes.POINTER(vp)],
     "culipx_batch_destroy": [vp],
     "culipx_batch_sqmr_solve": [vp, vp, vp, vp, vp, f64, i32, vp, vp, vp],
+    "culipx_sqmr_solve_many": [vp, i32, vp, vp, vp, vp, f64, i32, vp, vp, vp],
+    "culipx_server_create": [i32, i64, i32, i32, f64, i32, ctypes.POINTER(vp)],
+    "culipx_server_destroy": [vp],
+    "culipx_server_add_pattern": [vp, i32, vp, vp, i32, vp, i32, ctypes.POINTER(i32)],
+    "culipx_server_submit": [vp, i32, vp, i32, vp, ctypes.POINTER(i32)],
+    "culipx_server_progress": [vp, i32, ctypes.POINTER(i32)],
+    "culipx_server_result": [vp, i32, vp, vp, vp, ctypes.POINTER(f64)],
+    "culipx_server_release": [vp, i32],
+    "culipx_server_stats": [vp, vp],
     "culipx_batch_sqmr_refine": [vp, vp, vp, vp, vp, f64, f64, i32, i32, vp, vp, vp, vp],
     "culipx_sqmr_refine": [vp, vp, vp, vp, vp, f64, f64, i32, i32, ctypes.POINTER(f64), ctypes.POINTER(i32),
                            ctypes.POINTER(i32)],

@@ -2,6 +2,7 @@
 #include "factor.h"
 #include "pattern.h"
 #include "permute.h"
+#include "server.h"
 #include "spmv.h"
 #include "sqmr.h"
 
@@ -508,6 +509,84 @@ CULIPX_API int culipx_batch_sqmr_solve(culipx_batch b, culipx_csr A, culipx_fact
     CULIPX_TRY(use_device(b->h));
     return batch_sqmr_solve(b, A, M, d_b, d_x, tol, max_it, h_residual, h_iterations, h_status, b->h->sqmr);
     GUARD_END
+}
+
+CULIPX_API int culipx_sqmr_solve_many(culipx_handle h, int num, const culipx_csr* A, const culipx_factor* M,
+                                      const double* const* d_b, double* const* d_x, double tol, int max_it,
+                                      double* h_residual, int* h_iterations, int* h_status)
+{
+    if (!h) return fail(CULIPX_INVALID_ARG, "null handle");
+    GUARD_BEGIN
+    CULIPX_TRY(use_device(h));
+    std::vector<Csr*> a(num > 0 ? num : 0);
+    std::vector<Factor*> m(num > 0 ? num : 0);
+    for (int k = 0; k < num; ++k) {
+        a[k] = A ? A[k] : nullptr;
+        m[k] = M ? M[k] : nullptr;
+    }
+    return sqmr_solve_many(h, num, a.data(), m.data(), d_b, d_x, tol, max_it, h_residual, h_iterations, h_status,
+                           h->sqmr);
+    GUARD_END
+}
+
+CULIPX_API int culipx_server_create(int device, long long memory_budget, int slots, int max_batch, double tol,
+                                    int max_it, culipx_server* out)
+{
+    GUARD_BEGIN
+    Server* s = nullptr;
+    CULIPX_TRY(server_create(device, memory_budget, slots, max_batch, tol, max_it, &s));
+    *out = static_cast<culipx_server>(s);
+    return CULIPX_OK;
+    GUARD_END
+}
+
+CULIPX_API int culipx_server_destroy(culipx_server s)
+{
+    delete s;
+    return CULIPX_OK;
+}
+
+CULIPX_API int culipx_server_add_pattern(culipx_server s, int n, const int* h_rowptr, const int* h_colidx,
+                                         int num_blocks, const int* h_block_starts, int precision, int* pattern_id)
+{
+    GUARD_BEGIN
+    return server_add_pattern(s, n, h_rowptr, h_colidx, num_blocks, h_block_starts, precision, pattern_id);
+    GUARD_END
+}
+
+CULIPX_API int culipx_server_submit(culipx_server s, int pattern_id, const double* h_vals, int nrhs,
+                                    const double* h_b, int* request_id)
+{
+    GUARD_BEGIN
+    return server_submit(s, pattern_id, h_vals, nrhs, h_b, request_id);
+    GUARD_END
+}
+
+CULIPX_API int culipx_server_progress(culipx_server s, int wait, int* completed)
+{
+    GUARD_BEGIN
+    return server_progress(s, wait, completed);
+    GUARD_END
+}
+
+CULIPX_API int culipx_server_result(culipx_server s, int request_id, double* h_x, int* h_iterations, int* h_status,
+                                    double* latency_ms)
+{
+    GUARD_BEGIN
+    return server_result(s, request_id, h_x, h_iterations, h_status, latency_ms);
+    GUARD_END
+}
+
+CULIPX_API int culipx_server_release(culipx_server s, int request_id)
+{
+    GUARD_BEGIN
+    return server_release(s, request_id);
+    GUARD_END
+}
+
+CULIPX_API int culipx_server_stats(culipx_server s, long long* stats8)
+{
+    return server_stats(s, stats8);
 }
 
 CULIPX_API int culipx_batch_sqmr_refine(culipx_batch b, culipx_csr A, culipx_factor M, const double* d_b,

@@ -1,0 +1,450 @@
+// Request server for streams of KKT solves (no counterpart in the reference,
+// whose driver solves one system per process run, apps/block_ildlt).
+//
+// A request is one IPM iteration on a registered sparsity pattern: new
+// values of K and 1..k right-hand sides.  The server
+//   * analyses each pattern once (symbolic phase, device mirror, K's
+//     structure on the device) and keeps a pool of factor objects per
+//     pattern, reused across requests;
+//   * admits queued requests in arrival order while the device-memory budget
+//     allows (request buffers come from the stream-ordered allocator, so
+//     admission and release never synchronize the device);
+//   * runs admitted requests as a batch on one of several slots, each with
+//     its own stream and workspace: per request the values' upload and the
+//     numeric factor, then ONE launch solving every (request, right-hand
+//     side) pair, one CTA each (k_sqmr_many); results come back through
+//     pinned buffers;
+//   * keeps up to `slots` batches in flight, so requests that arrive while
+//     others run are admitted into the next slot and overlap on the device.
+// Latency is measured from submit to the progress() call that sees the
+// batch's completion event.
+#include "server.h"
+#include "factor.h"
+#include "pattern.h"
+#include "kernels_common.cuh"
+
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+
+namespace culipx {
+
+namespace {
+
+__global__ void k_to_f32(const double* __restrict__ in, float* __restrict__ out, long long n)
+{
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += stride) out[i] = (float)in[i];
+}
+
+double now_ms()
+{
+    using namespace std::chrono;
+    return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
+}
+
+long long request_bytes(const ServerPattern& sp, int nrhs)
+{
+    const long long n = sp.n;
+    long long b = sp.nnz * 8 + 2 * n * nrhs * 8 + (long long)(7 * n + 8) * nrhs * 8 + 4096;
+    if (sp.precision == CULIPX_F32) b += sp.nnz * 4;
+    return b;
+}
+
+}  // namespace
+
+int server_create(int device, long long budget, int slots, int max_batch, double tol, int max_it, Server** out)
+{
+    if (!out || slots < 1 || slots > 8 || max_batch < 1 || !(tol >= 0.0) || max_it < 0)
+        return fail(CULIPX_INVALID_ARG, "culipx_server_create: bad argument");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+        cudaGetLastError();
+        return fail(CULIPX_INVALID_ARG, "culipx_server_create: bad device %d", device);
+    }
+    CULIPX_CUDA(cudaSetDevice(device));
+    {
+        // keep freed request buffers in the process's pool (no OS round trips)
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+            unsigned long long keep = ~0ull;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+        cudaGetLastError();
+    }
+    auto* s = new culipx_server_t();
+    s->device = device;
+    s->budget = budget;
+    s->max_batch = max_batch;
+    s->tol = tol;
+    s->max_it = max_it;
+    s->base = new culipx_handle_t();
+    s->base->device = device;
+    s->base->sqmr = new Sqmr();
+    if (cudaEventCreate(&s->base->ev_start) != cudaSuccess || cudaEventCreate(&s->base->ev_stop) != cudaSuccess) {
+        delete s;
+        return fail(CULIPX_CUDA_ERROR, "culipx_server_create: event creation failed");
+    }
+    s->slots.resize(slots);
+    for (auto& sl : s->slots) {
+        sl.h = new culipx_handle_t();
+        sl.h->device = device;
+        sl.h->sqmr = new Sqmr();
+        if (cudaStreamCreateWithFlags(&sl.h->stream, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreate(&sl.h->ev_start) != cudaSuccess || cudaEventCreate(&sl.h->ev_stop) != cudaSuccess) {
+            delete s;
+            return fail(CULIPX_CUDA_ERROR, "culipx_server_create: stream / event creation failed");
+        }
+    }
+    *out = s;
+    return CULIPX_OK;
+}
+
+Server::~Server()
+{
+    cudaSetDevice(device);
+    for (auto& sl : slots) {
+        if (sl.h && sl.h->stream) cudaStreamSynchronize(sl.h->stream);
+    }
+    for (auto& r : requests)
+        for (void* p : {r.second.d_vals, r.second.d_vals32, r.second.d_b, r.second.d_x})
+            if (p) cudaFree(p);
+    for (auto& sp : patterns) {
+        for (Factor* f : sp.free_factors) delete static_cast<culipx_factor_t*>(f);
+        delete static_cast<culipx_pattern_t*>(sp.pat);
+    }
+    for (auto& sl : slots) {
+        if (sl.out_host) cudaFreeHost(sl.out_host);
+        if (sl.x_host) cudaFreeHost(sl.x_host);
+        if (sl.done) cudaEventDestroy(sl.done);
+        if (sl.h) {
+            delete sl.h->sqmr;
+            if (sl.h->stream) cudaStreamDestroy(sl.h->stream);
+            if (sl.h->ev_start) cudaEventDestroy(sl.h->ev_start);
+            if (sl.h->ev_stop) cudaEventDestroy(sl.h->ev_stop);
+            delete sl.h;
+        }
+    }
+    if (base) {
+        delete base->sqmr;
+        if (base->ev_start) cudaEventDestroy(base->ev_start);
+        if (base->ev_stop) cudaEventDestroy(base->ev_stop);
+        delete base;
+    }
+}
+
+int server_add_pattern(Server* s, int n, const int* rowptr, const int* colidx, int num_blocks, const int* block_starts,
+                       int precision, int* pattern_id)
+{
+    if (!s || !pattern_id) return fail(CULIPX_INVALID_ARG, "culipx_server_add_pattern: null argument");
+    CULIPX_CUDA(cudaSetDevice(s->device));
+    Pattern* p = nullptr;
+    CULIPX_TRY(analyze_pattern(s->base, n, rowptr, colidx, num_blocks, block_starts, 0, 1.0, precision, &p));
+    ServerPattern sp;
+    sp.pat = p;
+    sp.n = n;
+    sp.nnz = p->nnz;
+    sp.precision = precision;
+    int st = sp.d_rowptr.upload(s->base, rowptr, (size_t)(n + 1) * sizeof(int));
+    if (st == CULIPX_OK) st = sp.d_colidx.upload(s->base, colidx, (size_t)std::max<long long>(sp.nnz, 1) * sizeof(int));
+    if (st != CULIPX_OK) {
+        delete static_cast<culipx_pattern_t*>(p);
+        return st;
+    }
+    s->patterns.push_back(std::move(sp));
+    *pattern_id = (int)s->patterns.size() - 1;
+    return CULIPX_OK;
+}
+
+int server_submit(Server* s, int pid, const double* vals, int nrhs, const double* b, int* request_id)
+{
+    if (!s || !vals || !b || !request_id || nrhs < 1) return fail(CULIPX_INVALID_ARG, "culipx_server_submit: bad argument");
+    if (pid < 0 || pid >= (int)s->patterns.size()) return fail(CULIPX_INVALID_ARG, "culipx_server_submit: unknown pattern %d", pid);
+    const ServerPattern& sp = s->patterns[pid];
+    if (s->budget > 0 && request_bytes(sp, nrhs) > s->budget)
+        return fail(CULIPX_OOM, "culipx_server_submit: the request alone exceeds the memory budget");
+    ServerRequest r;
+    r.id = s->next_id++;
+    r.pid = pid;
+    r.nrhs = nrhs;
+    r.vals.assign(vals, vals + sp.nnz);
+    r.b.assign(b, b + (size_t)sp.n * nrhs);
+    r.t_submit = now_ms();
+    const int id = r.id;
+    s->queue.push_back(id);
+    s->requests.emplace(id, std::move(r));
+    *request_id = id;
+    return CULIPX_OK;
+}
+
+long long Server::fixed_bytes() const
+{
+    long long t = 0;
+    for (const auto& sp : patterns) t += sp.pat->device_bytes + sp.d_rowptr.bytes() + sp.d_colidx.bytes() + sp.pool_bytes;
+    return t;
+}
+
+namespace {
+
+int finish_slot(Server* s, ServerSlot& sl)
+{
+    const double t = now_ms();
+    int k = 0;
+    size_t xo = 0;
+    for (int id : sl.reqs) {
+        ServerRequest& r = s->requests.at(id);
+        const ServerPattern& sp = s->patterns[r.pid];
+        r.its.resize(r.nrhs);
+        r.status.resize(r.nrhs);
+        many_results(r.nrhs, s->max_it, sl.out_host + (size_t)k * 8, nullptr, r.its.data(), r.status.data());
+        k += r.nrhs;
+        r.x.assign(sl.x_host + xo, sl.x_host + xo + (size_t)sp.n * r.nrhs);
+        xo += (size_t)sp.n * r.nrhs;
+        r.t_done = t;
+        r.state = 2;
+        s->patterns[r.pid].free_factors.push_back(r.F);
+        r.F = nullptr;
+        s->in_use -= r.bytes;
+        r.vals.clear();
+        r.vals.shrink_to_fit();
+        r.b.clear();
+        r.b.shrink_to_fit();
+        ++s->done;
+    }
+    sl.reqs.clear();
+    sl.busy = false;
+    return CULIPX_OK;
+}
+
+int launch_slot(Server* s, ServerSlot& sl)
+{
+    cudaStream_t st = sl.h->stream;
+    // admit in arrival order while the budget allows
+    std::vector<int> admit;
+    int systems = 0;
+    while (!s->queue.empty() && (int)admit.size() < s->max_batch) {
+        ServerRequest& r = s->requests.at(s->queue.front());
+        const ServerPattern& sp = s->patterns[r.pid];
+        const long long need = request_bytes(sp, r.nrhs);
+        const long long fbytes = sp.free_factors.empty() ? sp.factor_bytes_estimate() : 0;
+        const bool fits = s->budget <= 0 || s->fixed_bytes() + s->in_use + need + fbytes <= s->budget;
+        // over the budget: wait for running batches to free memory (a request
+        // that fits alone always runs once the device is idle)
+        if (!fits && (!admit.empty() || s->running_slots() > 0)) break;
+        r.bytes = need;
+        s->in_use += need;
+        admit.push_back(r.id);
+        systems += r.nrhs;
+        s->queue.pop_front();
+    }
+    if (admit.empty()) return CULIPX_OK;
+    // pinned result buffers
+    size_t xtot = 0;
+    for (int id : admit) xtot += (size_t)s->patterns[s->requests.at(id).pid].n * s->requests.at(id).nrhs;
+    if (sl.out_cap < systems) {
+        if (sl.out_host) cudaFreeHost(sl.out_host);
+        CULIPX_CUDA(cudaMallocHost(&sl.out_host, (size_t)systems * 8 * sizeof(double)));
+        sl.out_cap = systems;
+    }
+    if (sl.x_cap < xtot) {
+        if (sl.x_host) cudaFreeHost(sl.x_host);
+        CULIPX_CUDA(cudaMallocHost(&sl.x_host, std::max<size_t>(xtot, 1) * sizeof(double)));
+        sl.x_cap = xtot;
+    }
+    std::vector<Csr*> As;
+    std::vector<Factor*> Ms;
+    std::vector<const double*> bs;
+    std::vector<double*> xs;
+    sl.csrs.clear();
+    sl.csrs.reserve(admit.size());
+    for (int id : admit) {
+        ServerRequest& r = s->requests.at(id);
+        ServerPattern& sp = s->patterns[r.pid];
+        if (sp.free_factors.empty()) {
+            Factor* f = nullptr;
+            CULIPX_TRY(factor_create(sp.pat, &f));
+            sp.pool_bytes += sp.factor_bytes_estimate();
+            r.F = f;
+        } else {
+            r.F = sp.free_factors.back();
+            sp.free_factors.pop_back();
+        }
+        const size_t nv = (size_t)sp.nnz, nb = (size_t)sp.n * r.nrhs;
+        CULIPX_CUDA(cudaMallocAsync(&r.d_vals, std::max<size_t>(nv, 1) * sizeof(double), st));
+        CULIPX_CUDA(cudaMallocAsync(&r.d_b, nb * sizeof(double), st));
+        CULIPX_CUDA(cudaMallocAsync(&r.d_x, nb * sizeof(double), st));
+        CULIPX_CUDA(cudaMemcpyAsync(r.d_vals, r.vals.data(), nv * sizeof(double), cudaMemcpyHostToDevice, st));
+        CULIPX_CUDA(cudaMemcpyAsync(r.d_b, r.b.data(), nb * sizeof(double), cudaMemcpyHostToDevice, st));
+        const void* fv = r.d_vals;
+        if (sp.precision == CULIPX_F32) {
+            CULIPX_CUDA(cudaMallocAsync(&r.d_vals32, std::max<size_t>(nv, 1) * sizeof(float), st));
+            k_to_f32<<<148 * 4, 256, 0, st>>>(static_cast<const double*>(r.d_vals), static_cast<float*>(r.d_vals32),
+                                              (long long)nv);
+            fv = r.d_vals32;
+        }
+        // the factor runs on this slot's stream
+        cudaStream_t keep = sp.pat->handle->stream;
+        sp.pat->handle->stream = st;
+        const int fs = factor_compute(r.F, fv, nullptr, CULIPX_PIV_BK, 0.0);
+        sp.pat->handle->stream = keep;
+        CULIPX_TRY(fs);
+        sl.csrs.emplace_back();
+        Csr& A = sl.csrs.back();
+        A.h = sl.h;
+        A.m = A.n = sp.n;
+        A.nnz = sp.nnz;
+        A.rowptr = sp.d_rowptr.as<int>();
+        A.colidx = sp.d_colidx.as<int>();
+        A.val = r.d_vals;
+        A.precision = CULIPX_F64;
+        r.state = 1;
+    }
+    for (size_t q = 0; q < admit.size(); ++q) {
+        ServerRequest& r = s->requests.at(admit[q]);
+        const int n = s->patterns[r.pid].n;
+        for (int k = 0; k < r.nrhs; ++k) {
+            As.push_back(&sl.csrs[q]);
+            Ms.push_back(r.F);
+            bs.push_back(static_cast<const double*>(r.d_b) + (size_t)k * n);
+            xs.push_back(static_cast<double*>(r.d_x) + (size_t)k * n);
+        }
+    }
+    // one launch for every (request, right-hand side); FP32 and FP64 factors go in separate launches
+    std::vector<int> order(As.size());
+    for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return Ms[a]->precision < Ms[b]->precision; });
+    size_t g0 = 0;
+    while (g0 < order.size()) {
+        size_t g1 = g0;
+        while (g1 < order.size() && Ms[order[g1]]->precision == Ms[order[g0]]->precision) ++g1;
+        std::vector<Csr*> a;
+        std::vector<Factor*> m;
+        std::vector<const double*> bb;
+        std::vector<double*> xx;
+        for (size_t i = g0; i < g1; ++i) {
+            a.push_back(As[order[i]]);
+            m.push_back(Ms[order[i]]);
+            bb.push_back(bs[order[i]]);
+            xx.push_back(xs[order[i]]);
+        }
+        CULIPX_TRY(sqmr_solve_many_async(sl.h, (int)(g1 - g0), a.data(), m.data(), bb.data(), xx.data(), s->tol,
+                                         s->max_it, sl.h->sqmr, sl.out_host + g0 * 8));
+        g0 = g1;
+    }
+    // the groups' results were written in sorted order; keep the permutation to undo it
+    sl.order = order;
+    size_t xo = 0;
+    for (int id : admit) {
+        ServerRequest& r = s->requests.at(id);
+        const size_t nb = (size_t)s->patterns[r.pid].n * r.nrhs;
+        CULIPX_CUDA(cudaMemcpyAsync(sl.x_host + xo, r.d_x, nb * sizeof(double), cudaMemcpyDeviceToHost, st));
+        xo += nb;
+        for (void** p : {&r.d_vals, &r.d_vals32, &r.d_b, &r.d_x})
+            if (*p) {
+                CULIPX_CUDA(cudaFreeAsync(*p, st));
+                *p = nullptr;
+            }
+    }
+    CULIPX_CUDA(cudaEventRecord(sl.done, st));
+    sl.reqs = admit;
+    sl.busy = true;
+    ++s->batches;
+    return CULIPX_OK;
+}
+
+}  // namespace
+
+int Server::running_slots() const
+{
+    int r = 0;
+    for (const auto& sl : slots) r += sl.busy;
+    return r;
+}
+
+long long ServerPattern::factor_bytes_estimate() const
+{
+    const Pattern& p = *pat;
+    const long long vb = (precision == CULIPX_F64) ? 8 : 4;
+    const long long slots = p.val_slots + 2 * p.sparse_slots;
+    return slots * (vb + 4) * 2 + (long long)p.n * 64 + (long long)p.coarse_nnz * 24 + (long long)p.num_blocks * 64;
+}
+
+int server_progress(Server* s, int wait, int* completed)
+{
+    if (!s) return fail(CULIPX_INVALID_ARG, "null server");
+    CULIPX_CUDA(cudaSetDevice(s->device));
+    const long long done0 = s->done;
+    for (;;) {
+        // completions
+        for (auto& sl : s->slots)
+            if (sl.busy) {
+                const cudaError_t e = cudaEventQuery(sl.done);
+                if (e == cudaSuccess) {
+                    CULIPX_TRY(launch_check("server batch"));
+                    // undo the precision-group order of the results
+                    std::vector<double> tmp(sl.order.size() * 8);
+                    for (size_t i = 0; i < sl.order.size(); ++i)
+                        std::memcpy(tmp.data() + (size_t)sl.order[i] * 8, sl.out_host + i * 8, 8 * sizeof(double));
+                    std::memcpy(sl.out_host, tmp.data(), tmp.size() * sizeof(double));
+                    CULIPX_TRY(finish_slot(s, sl));
+                } else if (e != cudaErrorNotReady) {
+                    return fail(CULIPX_CUDA_ERROR, "server batch failed: %s", cudaGetErrorString(e));
+                }
+            }
+        // admissions into free slots
+        for (auto& sl : s->slots)
+            if (!sl.busy && !s->queue.empty()) CULIPX_TRY(launch_slot(s, sl));
+        if (!wait || s->done > done0 || s->running_slots() == 0) break;
+        // block on the oldest busy slot
+        for (auto& sl : s->slots)
+            if (sl.busy) {
+                CULIPX_CUDA(cudaEventSynchronize(sl.done));
+                break;
+            }
+    }
+    if (completed) *completed = (int)(s->done - done0);
+    return CULIPX_OK;
+}
+
+int server_result(Server* s, int id, double* x, int* its, int* status, double* latency_ms)
+{
+    if (!s) return fail(CULIPX_INVALID_ARG, "null server");
+    auto it = s->requests.find(id);
+    if (it == s->requests.end()) return fail(CULIPX_INVALID_ARG, "culipx_server_result: unknown request %d", id);
+    const ServerRequest& r = it->second;
+    if (r.state != 2) return CULIPX_PENDING;
+    if (x) std::memcpy(x, r.x.data(), r.x.size() * sizeof(double));
+    if (its) std::memcpy(its, r.its.data(), r.its.size() * sizeof(int));
+    if (status) std::memcpy(status, r.status.data(), r.status.size() * sizeof(int));
+    if (latency_ms) *latency_ms = r.t_done - r.t_submit;
+    return CULIPX_OK;
+}
+
+int server_release(Server* s, int id)
+{
+    if (!s) return fail(CULIPX_INVALID_ARG, "null server");
+    auto it = s->requests.find(id);
+    if (it == s->requests.end()) return fail(CULIPX_INVALID_ARG, "culipx_server_release: unknown request %d", id);
+    if (it->second.state != 2) return fail(CULIPX_INVALID_ARG, "culipx_server_release: request %d not finished", id);
+    s->requests.erase(it);
+    return CULIPX_OK;
+}
+
+int server_stats(Server* s, long long* st8)
+{
+    if (!s || !st8) return fail(CULIPX_INVALID_ARG, "null argument");
+    long long running = 0;
+    for (const auto& sl : s->slots) running += (long long)sl.reqs.size();
+    st8[0] = (long long)s->queue.size();
+    st8[1] = running;
+    st8[2] = s->done;
+    st8[3] = s->batches;
+    st8[4] = s->in_use;
+    st8[5] = s->fixed_bytes();
+    st8[6] = (long long)s->patterns.size();
+    st8[7] = 0;
+    return CULIPX_OK;
+}
+
+}  // namespace culipx

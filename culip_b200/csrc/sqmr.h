@@ -18,6 +18,7 @@ struct Sqmr {
     DeviceBuffer ts;                  // 64 iterations x 8 phase stamps (ns, %globaltimer)
     DeviceBuffer vecs, partials, scal;
     DeviceBuffer ref_r, ref_d, ref_part;  // iterative refinement: residual, correction, norm partials
+    DeviceBuffer many;                    // sqmr_solve_many: vectors, argument blocks, counter
     void* host_flags = nullptr;  // pinned
     ~Sqmr()
     {
@@ -44,6 +45,13 @@ int batch_sqmr_solve(Batch* bt, Csr* A, Factor* M, const double* b, double* x, d
 int batch_sqmr_refine(Batch* bt, Csr* A, Factor* M, const double* b, double* x, double tol, double inner_tol,
                       int inner_max_it, int max_refine, double* h_relres, int* h_its, int* h_steps, int* h_status,
                       Sqmr* w);
+
+int sqmr_solve_many(culipx_handle_t* h, int num, Csr* const* A, Factor* const* M, const double* const* b,
+                    double* const* x, double tol, int max_it, double* h_res, int* h_its, int* h_status, Sqmr* w);
+
+int sqmr_solve_many_async(culipx_handle_t* h, int num, Csr* const* A, Factor* const* M, const double* const* b,
+                          double* const* x, double tol, int max_it, Sqmr* w, double* out_host);
+void many_results(int num, int max_it, const double* out, double* h_res, int* h_its, int* h_status);
 
 int sqmr_workspace(Sqmr* w, culipx_handle_t* h, int n);
 int sqmr_solve(culipx_handle_t* h, Csr* A, Factor* M, const double* b, double* x, double tol, int max_it,

@@ -814,6 +814,33 @@ __global__ void __launch_bounds__(kT, kCtasPerSm) k_sqmr_batched(PArgs<TF> a, Ba
     }
 }
 
+// Batched solves of independent systems that each have their own pattern,
+// factor, matrix and vectors (the serving path): the CTA copies system s's
+// argument block into shared memory and runs the same body over its rows.
+template <class TF>
+__global__ void __launch_bounds__(kT, kCtasPerSm) k_sqmr_many(const PArgs<TF>* __restrict__ sys_args, int num,
+                                                             int* next)
+{
+    __shared__ Scal S;
+    __shared__ double sh[kMaxNV][kW];
+    __shared__ int sys;
+    __shared__ PArgs<TF> pa;
+    static_assert(sizeof(PArgs<TF>) % 8 == 0, "argument block copied in 8-byte words");
+    CtaCtx ctx{(int)(threadIdx.x >> 5), kW, (int)threadIdx.x, kT};
+    for (;;) {
+        if (threadIdx.x == 0) sys = atomicAdd(next, 1);
+        __syncthreads();
+        const int s = sys;
+        if (s >= num) break;
+        const unsigned long long* src = reinterpret_cast<const unsigned long long*>(sys_args + s);
+        unsigned long long* dst = reinterpret_cast<unsigned long long*>(&pa);
+        for (int i = threadIdx.x; i < (int)(sizeof(PArgs<TF>) / 8); i += kT) dst[i] = src[i];
+        __syncthreads();
+        const SysView sv{0, pa.n, pa.lvl_off, pa.lvl_off + 1, pa.out};
+        sqmr_body<TF>(pa, ctx, sv, S, sh);
+    }
+}
+
 // kernel arguments over a work area of kVecs n doubles + 6 (vectors, then out)
 template <class TF>
 PArgs<TF> make_args(Csr* A, Factor* M, double* base, double* partials, const double* b, double* x, double tol,
@@ -1062,6 +1089,99 @@ int batch_sqmr_solve(Batch* bt, Csr* A, Factor* M, const double* b, double* x, d
                           : (o[3] == 0.0 && max_it > 0 && (int)o[1] >= max_it) ? CULIPX_MAXIT
                                                                                : CULIPX_OK;
     }
+    return CULIPX_OK;
+}
+
+namespace {
+
+// Enqueues the launch on h's stream; each system's 6 result values are
+// copied to out_host + 8 k (pinned memory for a truly asynchronous call)
+template <class TF>
+int launch_many(culipx_handle_t* h, int num, Csr* const* A, Factor* const* M, const double* const* b,
+                double* const* x, double tol, int max_it, Sqmr* w, double* out_host)
+{
+    cudaStream_t s = h->stream;
+    size_t total = 0;
+    for (int k = 0; k < num; ++k) total += (size_t)kVecs * A[k]->m + 8;
+    const size_t need = total * sizeof(double) + (size_t)num * sizeof(PArgs<TF>) + 64;
+    if (w->many.bytes() < need) CULIPX_TRY(w->many.alloc(h, need));
+    double* base = w->many.as<double>();
+    std::vector<PArgs<TF>> args(num);
+    size_t o = 0;
+    for (int k = 0; k < num; ++k) {
+        args[k] = make_args<TF>(A[k], M[k], base + o, nullptr, b[k], x[k], tol, max_it);
+        o += (size_t)kVecs * A[k]->m + 8;
+        CULIPX_CUDA(cudaMemsetAsync(args[k].v[0], 0, (size_t)kVecs * A[k]->m * sizeof(double), s));
+        CULIPX_CUDA(cudaMemsetAsync(x[k], 0, (size_t)A[k]->m * sizeof(double), s));
+    }
+    // argument blocks after the vectors (8-byte aligned), then the counter
+    PArgs<TF>* d_args = reinterpret_cast<PArgs<TF>*>(base + o);
+    int* d_next = reinterpret_cast<int*>(d_args + num);
+    CULIPX_CUDA(cudaMemcpyAsync(d_args, args.data(), (size_t)num * sizeof(PArgs<TF>), cudaMemcpyHostToDevice, s));
+    CULIPX_CUDA(cudaMemsetAsync(d_next, 0, sizeof(int), s));
+    static int grid_cache[2] = {0, 0};
+    int& G = grid_cache[sizeof(TF) == 8 ? 0 : 1];
+    if (G == 0) {
+        int dev = 0, per_sm = 0, sms = 0;
+        CULIPX_CUDA(cudaGetDevice(&dev));
+        CULIPX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        CULIPX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sqmr_many<TF>, kT, 0));
+        if (per_sm < 1) return fail(CULIPX_NOT_SUPPORTED, "batched SQMR kernel does not fit on an SM");
+        G = sms * std::min(per_sm, kCtasPerSm);
+    }
+    k_sqmr_many<TF><<<std::min(G, num), kT, 0, s>>>(d_args, num, d_next);
+    h->launches += 1;
+    CULIPX_TRY(launch_check("k_sqmr_many"));
+    for (int k = 0; k < num; ++k)
+        CULIPX_CUDA(cudaMemcpyAsync(out_host + (size_t)k * 8, args[k].out, 6 * sizeof(double),
+                                    cudaMemcpyDeviceToHost, s));
+    return CULIPX_OK;
+}
+
+}  // namespace
+
+int sqmr_solve_many_async(culipx_handle_t* h, int num, Csr* const* A, Factor* const* M, const double* const* b,
+                          double* const* x, double tol, int max_it, Sqmr* w, double* out_host)
+{
+    if (num == 0) return CULIPX_OK;
+    return (M[0]->precision == CULIPX_F64) ? launch_many<double>(h, num, A, M, b, x, tol, max_it, w, out_host)
+                                           : launch_many<float>(h, num, A, M, b, x, tol, max_it, w, out_host);
+}
+
+void many_results(int num, int max_it, const double* out, double* h_res, int* h_its, int* h_status)
+{
+    for (int k = 0; k < num; ++k) {
+        const double* o = out + (size_t)k * 8;
+        if (h_res) h_res[k] = o[0];
+        if (h_its) h_its[k] = (int)o[1];
+        if (h_status)
+            h_status[k] = (o[2] != 0.0) ? CULIPX_BREAKDOWN
+                          : (o[3] == 0.0 && max_it > 0 && (int)o[1] >= max_it) ? CULIPX_MAXIT
+                                                                               : CULIPX_OK;
+    }
+}
+
+int sqmr_solve_many(culipx_handle_t* h, int num, Csr* const* A, Factor* const* M, const double* const* b,
+                    double* const* x, double tol, int max_it, double* h_res, int* h_its, int* h_status, Sqmr* w)
+{
+    if (num < 0 || (num > 0 && (!A || !M || !b || !x)) || !w)
+        return fail(CULIPX_INVALID_ARG, "culipx_sqmr_solve_many: bad argument");
+    if (max_it < 0) return fail(CULIPX_INVALID_ARG, "culipx_sqmr_solve_many: max_it < 0");
+    if (num == 0) return CULIPX_OK;
+    const int prec = M[0] ? M[0]->precision : CULIPX_F64;
+    for (int k = 0; k < num; ++k) {
+        if (!A[k] || !M[k] || !b[k] || !x[k]) return fail(CULIPX_INVALID_ARG, "culipx_sqmr_solve_many: null system %d", k);
+        if (A[k]->precision != CULIPX_F64 || A[k]->m != A[k]->n || !M[k]->computed || M[k]->pat->n != A[k]->m)
+            return fail(CULIPX_INVALID_ARG, "culipx_sqmr_solve_many: system %d: A must be square FP64 and M its computed factor", k);
+        if (M[k]->precision != prec)
+            return fail(CULIPX_NOT_SUPPORTED, "culipx_sqmr_solve_many: all factors of one call must share a precision");
+        if (M[k]->solve_algorithm == CULIPX_SOLVE_JACOBI)
+            return fail(CULIPX_NOT_SUPPORTED, "culipx_sqmr_solve_many: SOLVE_JACOBI is not batched");
+    }
+    std::vector<double> out((size_t)num * 8, 0.0);
+    CULIPX_TRY(sqmr_solve_many_async(h, num, A, M, b, x, tol, max_it, w, out.data()));
+    CULIPX_CUDA(cudaStreamSynchronize(h->stream));
+    many_results(num, max_it, out.data(), h_res, h_its, h_status);
     return CULIPX_OK;
 }
 

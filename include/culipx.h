@@ -37,6 +37,7 @@ extern "C" {
 #define CULIPX_TIMEOUT       5  /* a bounded device wait gave up */
 #define CULIPX_CUDA_ERROR    6
 #define CULIPX_NOT_SUPPORTED 7
+#define CULIPX_PENDING       8  /* a server request has not finished yet */
 
 /* ---- value precision (the reference's T = double / float) ---- */
 #define CULIPX_F64 0
@@ -250,6 +251,45 @@ int culipx_batch_create(culipx_pattern p, int num_systems, const int *h_row_offs
 int culipx_batch_destroy(culipx_batch b);
 int culipx_batch_sqmr_solve(culipx_batch b, culipx_csr A, culipx_factor M, const double *d_b, double *d_x,
                             double tol, int max_it, double *h_residual, int *h_iterations, int *h_status);
+
+/* Many independent systems, each with its own pattern, factor, matrix and
+ * vectors (no union), solved in one launch, one CTA per system; all factors
+ * of one call share a precision.  Same per-system outputs as
+ * culipx_batch_sqmr_solve.  No counterpart in the reference. */
+int culipx_sqmr_solve_many(culipx_handle h, int num, const culipx_csr *A, const culipx_factor *M,
+                           const double *const *d_b, double *const *d_x, double tol, int max_it,
+                           double *h_residual, int *h_iterations, int *h_status);
+
+/* ------------------------------------------------------------------------ */
+/* Request server for streams of KKT solves (no counterpart in the reference).
+ * Patterns are analysed once; each request brings K's values (host FP64, the
+ * pattern's CSR order) and nrhs right-hand sides (host, n x nrhs column-major),
+ * copied at submit.  progress() completes finished batches and admits queued
+ * requests, in arrival order and within memory_budget device bytes (<= 0:
+ * unlimited), into free slots: per request the values' upload and the numeric
+ * factor (BK, level-0 fill), then one launch solving every (request,
+ * right-hand side) with SQMR(tol, max_it), one CTA each.  Up to `slots`
+ * batches run concurrently on their own streams; at most max_batch requests
+ * per batch.  A request's results do not depend on the other requests.
+ * result() returns CULIPX_PENDING until the request is done; latency_ms runs
+ * from submit to the progress() call that saw it finish. */
+typedef struct culipx_server_t *culipx_server;
+int culipx_server_create(int device, long long memory_budget, int slots, int max_batch, double tol, int max_it,
+                         culipx_server *out);
+int culipx_server_destroy(culipx_server s);
+int culipx_server_add_pattern(culipx_server s, int n, const int *h_rowptr, const int *h_colidx, int num_blocks,
+                              const int *h_block_starts, int precision, int *pattern_id);
+int culipx_server_submit(culipx_server s, int pattern_id, const double *h_vals, int nrhs, const double *h_b,
+                         int *request_id);
+/* wait != 0: block until at least one request finishes (or nothing runs) */
+int culipx_server_progress(culipx_server s, int wait, int *completed);
+int culipx_server_result(culipx_server s, int request_id, double *h_x, int *h_iterations, int *h_status,
+                         double *latency_ms);
+/* forget a finished request */
+int culipx_server_release(culipx_server s, int request_id);
+/* stats[0..7]: queued, running, done, batches launched, device bytes of
+ * running requests, device bytes held by patterns and factor pools, patterns, 0 */
+int culipx_server_stats(culipx_server s, long long *stats8);
 
 /* culipx_sqmr_refine per system of a batch: every step solves all systems
  * still above tol in one batched launch (the others get a zero right-hand
