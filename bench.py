@@ -47,7 +47,10 @@ def _parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="culipx", choices=["culipx", "reference"])
-    ap.add_argument("--config", default="scale", choices=["small", "scale", "batch"])
+    ap.add_argument("--config", default="scale", choices=["small", "scale", "batch", "served"])
+    ap.add_argument("--rate", type=float, default=2000.0, help="--config served: arrivals per second")
+    ap.add_argument("--duration", type=float, default=0.25, help="--config served: seconds of arrivals")
+    ap.add_argument("--patterns", type=int, default=64, help="--config served: sparsity patterns")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--max-it", type=int, default=1000, help="SQMR iteration cap (1000 = the driver's setting)")
     ap.add_argument("--batch", type=int, default=512, help="systems in --config batch")
@@ -494,11 +497,123 @@ def run_batch(args):
         print(json.dumps(out), flush=True)
 
 
+def served_workload(num_patterns, seed_base):
+    """Config 5: num_patterns KKT patterns, pattern j from sub-seed
+    seed_base + j, n log-uniform in [1e3, 5e5], m = n // 2, A with 6 nonzeros
+    per column (half in a band of half-width 32), initial H log-uniform in
+    [1e-6, 1e6], delta = gamma = 1e-8, 32-row blocks."""
+    import culip_b200 as cb
+
+    rng = np.random.default_rng(seed_base)
+    pats = []
+    for j in range(num_patterns):
+        n = int(round(10 ** rng.uniform(3, np.log10(5e5))))
+        m = n // 2
+        rp, ci, v = cb.kkt_generate(n, m, 6, 32, 1e-6, 1e6, seed=seed_base + j)
+        pats.append((rp, ci, v, cb.kkt_blocking(n, m, 32), n))
+    return pats
+
+
+def run_served(args):
+    """Served IPM stream: Poisson arrivals at --rate over the patterns for
+    --duration seconds; request = the pattern's next IPM iteration (H times
+    10^U(-1, 1), clipped to [1e-8, 1e8]) with 1-8 N(0,1) right-hand sides,
+    submitted to the server when its arrival time has passed (host wall
+    clock), solved to SQMR tol 1e-8.  value = requests completed / (time from
+    the first arrival to the last completion); latency = submit to completion."""
+    import culip_b200 as cb
+
+    import torch
+
+    world, rank, local = _dist()
+    torch.cuda.set_device(local)
+    seed_base = cb.SEED + 5000
+    pats = served_workload(args.patterns, seed_base)
+    rng = np.random.default_rng(seed_base + 999)
+    # arrival trace
+    t, arrivals = 0.0, []
+    while True:
+        t += rng.exponential(1.0 / args.rate)
+        if t > args.duration:
+            break
+        arrivals.append((t, int(rng.integers(0, len(pats))), int(rng.integers(1, 9))))
+    # per-pattern IPM state: the diagonal of H evolves request by request
+    state = []
+    for rp, ci, v, bs, n in pats:
+        rows = np.repeat(np.arange(len(rp) - 1), np.diff(rp))
+        d = np.nonzero((rows == ci) & (rows < n))[0]
+        state.append([v.copy(), d])
+
+    def make_request(j, nrhs):
+        v, d = state[j]
+        h = np.clip((v[d] - 1e-8) * 10.0 ** rng.uniform(-1, 1, len(d)), 1e-8, 1e8)
+        v = v.copy()
+        v[d] = h + 1e-8
+        state[j][0] = v
+        return v, rng.standard_normal((len(pats[j][0]) - 1, nrhs))
+
+    srv = cb.Server(local, 0, 3, 512, 1e-8, args.max_it)
+    t0 = time.perf_counter()
+    pids = [srv.add_pattern(rp, ci, bs) for rp, ci, v, bs, n in pats]
+    analysis_s = time.perf_counter() - t0
+    # warm-up: one request per pattern (factor pools, workspaces)
+    for j in range(len(pats)):
+        srv.submit(pids[j], pats[j][2], np.zeros(len(pats[j][0]) - 1) + 1.0)
+    while srv.stats()["done"] < len(pats):
+        srv.progress(wait=True)
+    clocks = ClockSampler(local)
+    clocks.start()
+    ids = []
+    start = time.perf_counter()
+    k = 0
+    reqs = arrivals
+    while k < len(reqs) or srv.stats()["done"] < len(pats) + len(reqs):
+        now = time.perf_counter() - start
+        while k < len(reqs) and reqs[k][0] <= now:
+            v, b = make_request(reqs[k][1], reqs[k][2])  # the request's values are built as it arrives
+            ids.append(srv.submit(pids[reqs[k][1]], v, b))
+            k += 1
+        if srv.progress(wait=False) == 0 and k < len(reqs):
+            time.sleep(min(0.0005, max(0.0, reqs[k][0] - (time.perf_counter() - start))))
+        elif k >= len(reqs):
+            srv.progress(wait=True)
+    elapsed = time.perf_counter() - start
+    ck = clocks.stop()
+    lat, its, conv, nrhs_tot = [], [], 0, 0
+    for i in ids:
+        x, it, st, l = srv.result(i)
+        lat.append(l)
+        its.extend(it.tolist())
+        conv += int(np.sum(st == 0))
+        nrhs_tot += len(st)
+    lat = np.array(lat)
+    out = {
+        "metric": "KKT solves/s and p50/p99 latency (served IPM stream, FP64 plain method per request)",
+        "value": len(ids) / elapsed, "unit": "requests/s", "n_gpus": world, "steps": len(ids), "warmup": len(pats),
+        "ms_per_step": 1e3 * elapsed / max(len(ids), 1), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded KKT generator, Poisson arrivals)",
+        "config": {"workload": f"{len(pats)} patterns, n log-U[1e3,5e5], m=n/2, A 6/col (band_half=32), "
+                               f"Poisson {args.rate:g} req/s for {args.duration:g} s ({len(ids)} requests), "
+                               f"1-8 RHS, H *= 10^U(-1,1) clipped [1e-8,1e8] per request",
+                   "solver": f"server: 3 slots, batched SQMR (one CTA per right-hand side), tol 1e-8, "
+                             f"max_it {args.max_it}", "parallelism": "one GPU"},
+        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                       "mean": float(lat.mean()), "max": float(lat.max())},
+        "right_hand_sides": nrhs_tot, "converged_fraction": conv / max(nrhs_tot, 1),
+        "median_iterations": int(np.median(its)) if its else None, "pattern_analysis_s_once": analysis_s,
+        "clocks": ck, "gpu_launches": None,
+    }
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
 if __name__ == "__main__":
     a = _parse()
     if a.impl == "reference":
         run_reference(a)
     elif a.config == "batch":
         run_batch(a)
+    elif a.config == "served":
+        run_served(a)
     else:
         run_culipx(a)
