@@ -476,6 +476,33 @@ struct SysView {
     double* out;
 };
 
+// Per-row tail of the U' sweep for a row of a simple block row (1x1 pivot
+// d): v+ scaled in place, beta's numerator v_k' D^-1 Av, the next alpha's
+// dots v+' D^-1 Av and v+' D^-1 v+, and p_k = (v_k - beta_rr p_k-1 -
+// epsilon p_k-2) / rho, x += tau p_k with ||x||^2.
+template <class TF>
+__device__ __forceinline__ void simple_epilogue(const PArgs<TF>& a, int g, double av, const double* vk, double* vk1,
+                                                const double* pkm1, const double* pkm2, double* pk, double sc,
+                                                double nbrr, double ne, double ir, double tau, double (&r)[4])
+{
+    const double vkr = vk[g];
+    const double vs = vk1[g] * sc;
+    vk1[g] = vs;
+    double p = vkr;
+    p = fma_rn(nbrr, pkm1[g], p);
+    p = fma_rn(ne, pkm2[g], p);
+    p = p * ir;
+    pk[g] = p;
+    const double xv = fma_rn(tau, p, a.x[g]);
+    a.x[g] = xv;
+    r[3] = fma_rn(xv, xv, r[3]);
+    const double dd = (double)__ldg(a.dg + g);
+    const double da = av / dd, dv = vs / dd;
+    r[0] = fma_rn(vkr, da, r[0]);
+    r[1] = fma_rn(vs, da, r[1]);
+    r[2] = fma_rn(vs, dv, r[2]);
+}
+
 // The whole preconditioned SQMR solve of one system (see the top of the file).
 template <class TF, class Ctx>
 __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal& S, double (*sh)[kW])
@@ -680,6 +707,10 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal&
                         r[2] = fma_rn(vs, dv, r[2]);
                     }
                 }
+                // simple rows of this level: Av; their dots and the p / x
+                // update wait for the next level's phase, whose threads are
+                // mostly free (the last level does them at once)
+                const bool last = (L == a.nl - 1);
                 const int s1 = __ldg(a.scan_s + q1);
                 for (int i = __ldg(a.scan_s + q0) + ctx.g0; i < s1; i += ctx.gstride) {
                     const int g = __ldg(a.simple_rows + i);
@@ -687,22 +718,23 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal&
                     const double av = (double)row_sub<TF>((TF)y, __ldg(a.ut_off + g), __ldg(a.ut_off + g + 1), a.ut_col,
                                                           a.ut_val, a.Av);
                     a.Av[g] = av;
-                    const double vkr = vk[g];
-                    const double vs = vk1[g] * sc;
-                    vk1[g] = vs;
-                    double p = vkr;
-                    p = fma_rn(nbrr, pkm1[g], p);
-                    p = fma_rn(ne, pkm2[g], p);
-                    p = p * ir;
-                    pk[g] = p;
-                    const double xv = fma_rn(tau, p, a.x[g]);
-                    a.x[g] = xv;
-                    r[3] = fma_rn(xv, xv, r[3]);
-                    const double dd = (double)__ldg(a.dg + g);
-                    const double da = av / dd, dv = vs / dd;
-                    r[0] = fma_rn(vkr, da, r[0]);
-                    r[1] = fma_rn(vs, da, r[1]);
-                    r[2] = fma_rn(vs, dv, r[2]);
+                    if (last) simple_epilogue(a, g, av, vk, vk1, pkm1, pkm2, pk, sc, nbrr, ne, ir, tau, r);
+                }
+                if (L > 0) {
+                    // warps without a block row in this level take the tails;
+                    // if every warp has one, all threads do, after their items
+                    const int p0 = __ldg(sv.qb + L - 1), p1 = __ldg(sv.qe + L - 1);
+                    const int e1 = __ldg(a.scan_s + p1);
+                    const int items = c1 - __ldg(a.scan_c + q0);
+                    const bool spare = items < nwarps;
+                    if (!spare || wid >= items) {
+                        const int t0 = spare ? (wid - items) * 32 + lane : ctx.g0;
+                        const int ts = spare ? (nwarps - items) * 32 : ctx.gstride;
+                        for (int i = __ldg(a.scan_s + p0) + t0; i < e1; i += ts) {
+                            const int g = __ldg(a.simple_rows + i);
+                            simple_epilogue(a, g, a.Av[g], vk, vk1, pkm1, pkm2, pk, sc, nbrr, ne, ir, tau, r);
+                        }
+                    }
                 }
                 if (L < a.nl - 1) {
                     ctx.sync();
