@@ -457,6 +457,19 @@ class Server:
             pass
 
 
+def sqmr_solve_multi(handle: Handle, A: CsrOperator, M: Factor, B, X, tol=1e-8, max_it=1000):
+    """Several right-hand sides of one system: B, X torch float64 CUDA tensors
+    of shape (nrhs, n) (row k = right-hand side k, i.e. n x nrhs column-major).
+    Returns per-RHS (residual, iterations, status) numpy arrays."""
+    nrhs = int(B.shape[0])
+    res = np.zeros(nrhs)
+    its = np.zeros(nrhs, np.int32)
+    st = np.zeros(nrhs, np.int32)
+    capi.call("culipx_sqmr_solve_multi", handle._h, A._h, M._h, nrhs, _dptr(B), _dptr(X), float(tol), int(max_it),
+              _p(res), _p(its), _p(st))
+    return res, its, st
+
+
 def sqmr_solve_many(handle: Handle, As, Ms, bs, xs, tol=1e-8, max_it=1000):
     """Independent systems with their own factors, one launch; per-system
     (residual, iterations, status) numpy arrays."""

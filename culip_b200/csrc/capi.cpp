@@ -511,6 +511,17 @@ CULIPX_API int culipx_batch_sqmr_solve(culipx_batch b, culipx_csr A, culipx_fact
     GUARD_END
 }
 
+CULIPX_API int culipx_sqmr_solve_multi(culipx_handle h, culipx_csr A, culipx_factor M, int nrhs, const double* d_B,
+                                       double* d_X, double tol, int max_it, double* h_residual, int* h_iterations,
+                                       int* h_status)
+{
+    if (!h) return fail(CULIPX_INVALID_ARG, "null handle");
+    GUARD_BEGIN
+    CULIPX_TRY(use_device(h));
+    return sqmr_solve_multi(h, A, M, nrhs, d_B, d_X, tol, max_it, h_residual, h_iterations, h_status, h->sqmr);
+    GUARD_END
+}
+
 CULIPX_API int culipx_sqmr_solve_many(culipx_handle h, int num, const culipx_csr* A, const culipx_factor* M,
                                       const double* const* d_b, double* const* d_x, double tol, int max_it,
                                       double* h_residual, int* h_iterations, int* h_status)

@@ -53,6 +53,9 @@ int sqmr_solve_many_async(culipx_handle_t* h, int num, Csr* const* A, Factor* co
                           double* const* x, double tol, int max_it, Sqmr* w, double* out_host);
 void many_results(int num, int max_it, const double* out, double* h_res, int* h_its, int* h_status);
 
+int sqmr_solve_multi(culipx_handle_t* h, Csr* A, Factor* M, int nrhs, const double* B, double* X, double tol,
+                     int max_it, double* h_res, int* h_its, int* h_status, Sqmr* w);
+
 int sqmr_workspace(Sqmr* w, culipx_handle_t* h, int n);
 int sqmr_solve(culipx_handle_t* h, Csr* A, Factor* M, const double* b, double* x, double tol, int max_it,
                double* residual, int* iterations, Sqmr* w);

@@ -68,7 +68,8 @@ namespace {
 constexpr int kT = 512;          // threads per CTA
 constexpr int kW = kT / 32;      // warps per CTA
 constexpr int kCtasPerSm = 2;    // 32 resident warps per SM
-constexpr int kMaxNV = 4;        // values per grid reduction
+constexpr int kMaxNR = 4;        // right-hand sides per launch
+constexpr int kMaxNV = 4 * kMaxNR;  // values per grid reduction
 constexpr int kBatch = 8;        // loads issued ahead in row sums and tile solves
 constexpr int kVecs = 7;         // work vectors of n doubles
 constexpr unsigned kFull = 0xffffffffu;
@@ -106,9 +107,9 @@ struct PArgs {
     double* p[2];              // p_k-1 and p_k-2, p_k overwrites p_k-2 in place
     double* Av;
     double* ev;    // P U^-1 D^-1 (...)
-    double* tmp;
-    double* x;
-    const double* b;
+    double* xt;    // the iterate x~ (interleaved)
+    double* x;     // the caller's solutions, column-major n x NR
+    const double* b;  // the caller's right-hand sides, column-major n x NR
     double* partials;  // 2 buffers x kMaxNV x gridDim
     double* out;       // [0] gamma/norm_pb, [1] iterations, [2] breakdown, [3] converged, [4] norm_pb, [5] it
     unsigned long long* ts;  // optional phase timestamps: [it * 8 + phase], it < kTsIters
@@ -135,7 +136,7 @@ struct Scal {
     double norm_A, epsilon, beta_rr, tau, rho, gamma, norm_pb, norm_x, eta;
     double inv_pb, inv_delta, inv_beta, inv_rho;
     double vdv;  // v_k' D^-1 v_k
-    int test0, test1, snap0, snap1, done, iters, breakdown;
+    int test0, test1, snap0, snap1, done, iters, breakdown, stop_it;
 };
 
 __host__ __device__ __forceinline__ int acc3(int r) { return (r % 3) + ((r < 0) ? 3 : 0); }
@@ -235,166 +236,248 @@ struct DBlock {
     }
 };
 
-// acc - sum_k val[k] x[col[k]] in increasing k (x is written during the
-// kernel: plain loads); kBatch index / value loads, then kBatch gathers
-template <class TF>
-__device__ __forceinline__ TF row_sub(TF acc, int k0, int k1, const int* __restrict__ col,
-                                      const TF* __restrict__ val, const double* x)
+// acc[j] - sum_k val[k] x[col[k] NR + j] in increasing k for the NR
+// interleaved right-hand sides (x is written during the kernel: plain loads);
+// index / value loads of a batch, then its gathers (the NR values of one
+// column are adjacent: 16-byte loads for even NR)
+template <class TF, int NR>
+__device__ __forceinline__ void row_sub(TF (&acc)[NR], int k0, int k1, const int* __restrict__ col,
+                                        const TF* __restrict__ val, const double* x)
 {
-    for (int k = k0; k < k1; k += kBatch) {
-        int c[kBatch];
-        TF v[kBatch];
+    constexpr int B = (NR == 1) ? kBatch : (NR == 2 ? 4 : 2);
+    for (int k = k0; k < k1; k += B) {
+        int c[B];
+        TF v[B];
 #pragma unroll
-        for (int j = 0; j < kBatch; ++j) {
+        for (int j = 0; j < B; ++j) {
             c[j] = (k + j < k1) ? __ldg(col + k + j) : -1;
             v[j] = (k + j < k1) ? __ldg(val + k + j) : TF(0);
         }
-        double xv[kBatch];
+        double xv[B][NR];
 #pragma unroll
-        for (int j = 0; j < kBatch; ++j) xv[j] = (c[j] >= 0) ? x[c[j]] : 0.0;
+        for (int j = 0; j < B; ++j) {
+            if (NR % 2 == 0) {
 #pragma unroll
-        for (int j = 0; j < kBatch; ++j)
-            if (k + j < k1) acc = fma_rn(-v[j], (TF)xv[j], acc);
+                for (int r = 0; r < NR; r += 2) {
+                    double2 q = make_double2(0.0, 0.0);
+                    if (c[j] >= 0) q = *reinterpret_cast<const double2*>(x + (size_t)c[j] * NR + r);
+                    xv[j][r] = q.x;
+                    xv[j][r + 1] = q.y;
+                }
+            } else {
+#pragma unroll
+                for (int r = 0; r < NR; ++r) xv[j][r] = (c[j] >= 0) ? x[(size_t)c[j] * NR + r] : 0.0;
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < B; ++j)
+            if (k + j < k1)
+#pragma unroll
+                for (int r = 0; r < NR; ++r) acc[r] = fma_rn(-v[j], (TF)xv[j][r], acc[r]);
     }
-    return acc;
 }
 
-// (K x)_q, entries in increasing column order
-template <class TF>
-__device__ __forceinline__ double spmv_row(const PArgs<TF>& a, int q, const double* x)
+// (K x)_q for the NR interleaved vectors, entries in increasing column order
+template <class TF, int NR>
+__device__ __forceinline__ void spmv_row(const PArgs<TF>& a, int q, const double* x, double (&acc)[NR])
 {
+    constexpr int B = (NR == 1) ? kBatch : (NR == 2 ? 4 : 2);
     const int k0 = __ldg(a.rowptr + q), k1 = __ldg(a.rowptr + q + 1);
-    double acc = 0.0;
-    for (int k = k0; k < k1; k += kBatch) {
-        int c[kBatch];
-        double v[kBatch];
 #pragma unroll
-        for (int j = 0; j < kBatch; ++j) {
+    for (int r = 0; r < NR; ++r) acc[r] = 0.0;
+    for (int k = k0; k < k1; k += B) {
+        int c[B];
+        double v[B];
+#pragma unroll
+        for (int j = 0; j < B; ++j) {
             c[j] = (k + j < k1) ? __ldg(a.colidx + k + j) : -1;
             v[j] = (k + j < k1) ? __ldg(a.kval + k + j) : 0.0;
         }
-        double xv[kBatch];
+        double xv[B][NR];
 #pragma unroll
-        for (int j = 0; j < kBatch; ++j) xv[j] = (c[j] >= 0) ? x[c[j]] : 0.0;
+        for (int j = 0; j < B; ++j) {
+            if (NR % 2 == 0) {
 #pragma unroll
-        for (int j = 0; j < kBatch; ++j)
-            if (k + j < k1) acc = fma_rn(v[j], xv[j], acc);
+                for (int r = 0; r < NR; r += 2) {
+                    double2 q2 = make_double2(0.0, 0.0);
+                    if (c[j] >= 0) q2 = *reinterpret_cast<const double2*>(x + (size_t)c[j] * NR + r);
+                    xv[j][r] = q2.x;
+                    xv[j][r + 1] = q2.y;
+                }
+            } else {
+#pragma unroll
+                for (int r = 0; r < NR; ++r) xv[j][r] = (c[j] >= 0) ? x[(size_t)c[j] * NR + r] : 0.0;
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < B; ++j)
+            if (k + j < k1)
+#pragma unroll
+                for (int r = 0; r < NR; ++r) acc[r] = fma_rn(v[j], xv[j][r], acc[r]);
     }
-    return acc;
 }
 
 // Back substitution with the block row's pivot tile, upper triangle packed
 // column by column (U sweep; d_left_solve_row_major,
 // block_ildlt_kernels.impl.cuh:2087-2113): for c = h-1 .. 0:
-// x_c = t_c / U_cc, t_r -= U_rc x_c (r < c).  The division is taken only
-// where bit c of nd says U_cc != 1 (t / 1 == t exactly); with nd == 0 the
-// chain is shuffle + fma per step.
-template <class TF, bool DIV>
-__device__ __forceinline__ TF tile_upper_t(TF t, const TF* P, int h, unsigned nd)
+// x_c = t_c / U_cc, t_r -= U_rc x_c (r < c), for each right-hand side.  The
+// division is taken only where bit c of nd says U_cc != 1 (t / 1 == t
+// exactly); with nd == 0 the chain is shuffle + fma per step.
+template <class TF, int NR, bool DIV>
+__device__ __forceinline__ void tile_upper_t(TF (&t)[NR], const TF* __restrict__ P, int h, unsigned nd)
 {
     const int lane = (int)lane_id();
-    for (int c0 = h - 1; c0 >= 0; c0 -= kBatch) {
-        TF u[kBatch];
+    constexpr int B = (NR == 1) ? kBatch : 4;
+    for (int c0 = h - 1; c0 >= 0; c0 -= B) {
+        TF u[B];
 #pragma unroll
-        for (int j = 0; j < kBatch; ++j) {
+        for (int j = 0; j < B; ++j) {
             const int c = c0 - j;
-            u[j] = (c >= 0 && lane <= c) ? P[c * (c + 1) / 2 + lane] : TF(0);
+            u[j] = (c >= 0 && lane <= c) ? __ldg(P + c * (c + 1) / 2 + lane) : TF(0);
         }
 #pragma unroll
-        for (int j = 0; j < kBatch; ++j) {
+        for (int j = 0; j < B; ++j) {
             const int c = c0 - j;
             if (c >= 0) {
                 if (DIV && ((nd >> c) & 1u)) {
-                    if (lane == c) t = t / u[j];
+                    if (lane == c)
+#pragma unroll
+                        for (int r = 0; r < NR; ++r) t[r] = t[r] / u[j];
                 }
-                const TF xc = __shfl_sync(kFull, t, c);
-                if (lane < c) t = fma_rn(-u[j], xc, t);
+#pragma unroll
+                for (int r = 0; r < NR; ++r) {
+                    const TF xc = __shfl_sync(kFull, t[r], c);
+                    if (lane < c) t[r] = fma_rn(-u[j], xc, t[r]);
+                }
             }
         }
     }
-    return t;
-}
-
-template <class TF>
-__device__ __forceinline__ double tile_upper(double in, const TF* P, int h, unsigned nd)
-{
-    return (double)(nd ? tile_upper_t<TF, true>((TF)in, P, h, nd) : tile_upper_t<TF, false>((TF)in, P, h, 0u));
 }
 
 // Forward substitution with the upper triangle packed row by row (U'
 // sweep): for r = 0 .. h-1: x_r = t_r / U_rr, t_c -= U_rc x_r (r < c < h);
 // divisions as in tile_upper_t
-template <class TF, bool DIV>
-__device__ __forceinline__ TF tile_lower_t(TF t, const TF* P, int h, unsigned nd)
+template <class TF, int NR, bool DIV>
+__device__ __forceinline__ void tile_lower_t(TF (&t)[NR], const TF* __restrict__ P, int h, unsigned nd)
 {
     const int lane = (int)lane_id();
-    for (int r0 = 0; r0 < h; r0 += kBatch) {
-        TF u[kBatch];
+    constexpr int B = (NR == 1) ? kBatch : 4;
+    for (int r0 = 0; r0 < h; r0 += B) {
+        TF u[B];
 #pragma unroll
-        for (int j = 0; j < kBatch; ++j) {
+        for (int j = 0; j < B; ++j) {
             const int r = r0 + j;
-            u[j] = (r < h && lane >= r && lane < h) ? P[r * h - r * (r - 1) / 2 + lane - r] : TF(0);
+            u[j] = (r < h && lane >= r && lane < h) ? __ldg(P + r * h - r * (r - 1) / 2 + lane - r) : TF(0);
         }
 #pragma unroll
-        for (int j = 0; j < kBatch; ++j) {
+        for (int j = 0; j < B; ++j) {
             const int r = r0 + j;
             if (r < h) {
                 if (DIV && ((nd >> r) & 1u)) {
-                    if (lane == r) t = t / u[j];
+                    if (lane == r)
+#pragma unroll
+                        for (int q = 0; q < NR; ++q) t[q] = t[q] / u[j];
                 }
-                const TF xr = __shfl_sync(kFull, t, r);
-                if (lane > r && lane < h) t = fma_rn(-u[j], xr, t);
+#pragma unroll
+                for (int q = 0; q < NR; ++q) {
+                    const TF xr = __shfl_sync(kFull, t[q], r);
+                    if (lane > r && lane < h) t[q] = fma_rn(-u[j], xr, t[q]);
+                }
             }
         }
     }
-    return t;
 }
 
-template <class TF>
-__device__ __forceinline__ double tile_lower(double in, const TF* P, int h, unsigned nd)
+template <class TF, int NR>
+__device__ __forceinline__ void tile_upper(double (&v)[NR], const TF* P, int h, unsigned nd)
 {
-    return (double)(nd ? tile_lower_t<TF, true>((TF)in, P, h, nd) : tile_lower_t<TF, false>((TF)in, P, h, 0u));
+    TF t[NR];
+#pragma unroll
+    for (int r = 0; r < NR; ++r) t[r] = (TF)v[r];
+    if (nd) tile_upper_t<TF, NR, true>(t, P, h, nd);
+    else tile_upper_t<TF, NR, false>(t, P, h, 0u);
+#pragma unroll
+    for (int r = 0; r < NR; ++r) v[r] = (double)t[r];
+}
+
+template <class TF, int NR>
+__device__ __forceinline__ void tile_lower(double (&v)[NR], const TF* P, int h, unsigned nd)
+{
+    TF t[NR];
+#pragma unroll
+    for (int r = 0; r < NR; ++r) t[r] = (TF)v[r];
+    if (nd) tile_lower_t<TF, NR, true>(t, P, h, nd);
+    else tile_lower_t<TF, NR, false>(t, P, h, 0u);
+#pragma unroll
+    for (int r = 0; r < NR; ++r) v[r] = (double)t[r];
 }
 
 // One U-sweep work item: block row I (rows fr .. fr+h-1), lane's right-hand
-// side y: d = D^-1 y; t = U_II^-1 (d - U_I* t); out[perm[r]] = t.  The
-// gathers of the later levels' t read out through the permuted columns.
-// Returns d (0 on lanes >= h).
-template <class TF>
-__device__ __forceinline__ double u_item(const PArgs<TF>& a, int I, int fr, int h, double y, double* out)
+// sides y: d = D^-1 y; t = U_II^-1 (d - U_I* t); out[perm[r]] = t (NR
+// interleaved).  The gathers of the later levels' t read out through the
+// permuted columns.  d receives D^-1 y (0 on lanes >= h).
+template <class TF, int NR>
+__device__ __forceinline__ void u_item(const PArgs<TF>& a, int I, int fr, int h, const double (&y)[NR], double* out,
+                                       double (&d)[NR])
 {
     const int lane = (int)lane_id();
     const int flags = __ldg(a.rowflags + I);
     DBlock<TF> D;
     D.load(a, fr, h, flags);
-    const double d = D.apply(y, h);
-    double t = d;
-    if (lane < h)
-        t = (double)row_sub<TF>((TF)d, __ldg(a.u_off + fr + lane), __ldg(a.u_off + fr + lane + 1), a.u_colp,
-                                a.u_val, out);
-    if (!(flags & kRowIdentity)) t = tile_upper<TF>(t, a.pk_col + __ldg(a.pk_off + I), h, __ldg(a.ndmask + I));
-    if (lane < h) out[(flags & kRowPermIdentity) ? fr + lane : __ldg(a.perm + fr + lane)] = t;
-    return d;
-}
-
-// One U'-sweep work item: lane's right-hand side is src[perm[r]] or, with
-// SPMV, sc * (K src)[perm[r]]; dst[r] = U_II'^-1 (rhs - U'_I* dst).  Returns
-// the lane's result (0 for lanes >= h).
-template <class TF, bool SPMV>
-__device__ __forceinline__ double ut_item(const PArgs<TF>& a, int I, int fr, int h, int flags, const double* src,
-                                          double sc, double* dst)
-{
-    const int lane = (int)lane_id();
-    double t = 0.0;
+#pragma unroll
+    for (int r = 0; r < NR; ++r) d[r] = D.apply(y[r], h);
+    double t[NR];
+#pragma unroll
+    for (int r = 0; r < NR; ++r) t[r] = d[r];
+    if (lane < h) {
+        TF acc[NR];
+#pragma unroll
+        for (int r = 0; r < NR; ++r) acc[r] = (TF)d[r];
+        row_sub<TF, NR>(acc, __ldg(a.u_off + fr + lane), __ldg(a.u_off + fr + lane + 1), a.u_colp, a.u_val, out);
+#pragma unroll
+        for (int r = 0; r < NR; ++r) t[r] = (double)acc[r];
+    }
+    if (!(flags & kRowIdentity)) tile_upper<TF, NR>(t, a.pk_col + __ldg(a.pk_off + I), h, __ldg(a.ndmask + I));
     if (lane < h) {
         const int q = (flags & kRowPermIdentity) ? fr + lane : __ldg(a.perm + fr + lane);
-        const double y = SPMV ? spmv_row(a, q, src) * sc : src[q];
-        t = (double)row_sub<TF>((TF)y, __ldg(a.ut_off + fr + lane), __ldg(a.ut_off + fr + lane + 1), a.ut_col,
-                                a.ut_val, dst);
+#pragma unroll
+        for (int r = 0; r < NR; ++r) out[(size_t)q * NR + r] = t[r];
     }
-    if (!(flags & kRowIdentity)) t = tile_lower<TF>(t, a.pk_row + __ldg(a.pk_off + I), h, __ldg(a.ndmask + I));
-    if (lane < h) dst[fr + lane] = t;
-    return t;
+}
+
+// One U'-sweep work item.  The lane's right-hand sides are, with SPMV,
+// sc[r] * (K src)[perm[row]] (src interleaved), else b[r n + perm[row]] of the
+// caller's column-major right-hand sides; dst[row] = U_II'^-1 (rhs - U'_I*
+// dst) (interleaved).  t receives the lane's results (0 for lanes >= h).
+template <class TF, int NR, bool SPMV>
+__device__ __forceinline__ void ut_item(const PArgs<TF>& a, int I, int fr, int h, int flags, const double* src,
+                                        const double (&sc)[NR], double* dst, double (&t)[NR])
+{
+    const int lane = (int)lane_id();
+#pragma unroll
+    for (int r = 0; r < NR; ++r) t[r] = 0.0;
+    if (lane < h) {
+        const int q = (flags & kRowPermIdentity) ? fr + lane : __ldg(a.perm + fr + lane);
+        double y[NR];
+        if (SPMV) {
+            spmv_row<TF, NR>(a, q, src, y);
+#pragma unroll
+            for (int r = 0; r < NR; ++r) y[r] *= sc[r];
+        } else {
+#pragma unroll
+            for (int r = 0; r < NR; ++r) y[r] = src[(size_t)r * a.n + q];
+        }
+        TF acc[NR];
+#pragma unroll
+        for (int r = 0; r < NR; ++r) acc[r] = (TF)y[r];
+        row_sub<TF, NR>(acc, __ldg(a.ut_off + fr + lane), __ldg(a.ut_off + fr + lane + 1), a.ut_col, a.ut_val, dst);
+#pragma unroll
+        for (int r = 0; r < NR; ++r) t[r] = (double)acc[r];
+    }
+    if (!(flags & kRowIdentity)) tile_lower<TF, NR>(t, a.pk_row + __ldg(a.pk_off + I), h, __ldg(a.ndmask + I));
+    if (lane < h)
+#pragma unroll
+        for (int r = 0; r < NR; ++r) dst[(size_t)(fr + lane) * NR + r] = t[r];
 }
 
 __device__ double sgn(double v) { return v < 0 ? -1.0 : 1.0; }
@@ -467,8 +550,8 @@ struct CtaCtx {
 
 // The system a solve works on: its rows [row0, row1) and, for each level L,
 // its block rows' positions [qb[L], qe[L]) in the level lists; out receives
-// [0] gamma/norm_pb, [1] iterations, [2] breakdown, [3] converged,
-// [4] norm_pb, [5] it.
+// per right-hand side r at out + 8 r: [0] gamma/norm_pb, [1] iterations,
+// [2] breakdown, [3] converged, [4] norm_pb, [5] it.
 struct SysView {
     int row0, row1;
     const int* qb;
@@ -476,133 +559,195 @@ struct SysView {
     double* out;
 };
 
+// Per-RHS coefficients of the p / x update and of the dots' scaling
+template <int NR>
+struct Coef {
+    double sc[NR], nbrr[NR], ne[NR], ir[NR], tau[NR];
+    bool act[NR];  // right-hand sides still iterating (x of the others is final)
+};
+
 // Per-row tail of the U' sweep for a row of a simple block row (1x1 pivot
 // d): v+ scaled in place, beta's numerator v_k' D^-1 Av, the next alpha's
 // dots v+' D^-1 Av and v+' D^-1 v+, and p_k = (v_k - beta_rr p_k-1 -
-// epsilon p_k-2) / rho, x += tau p_k with ||x||^2.
-template <class TF>
-__device__ __forceinline__ void simple_epilogue(const PArgs<TF>& a, int g, double av, const double* vk, double* vk1,
-                                                const double* pkm1, const double* pkm2, double* pk, double sc,
-                                                double nbrr, double ne, double ir, double tau, double (&r)[4])
+// epsilon p_k-2) / rho, x += tau p_k with ||x||^2 (r[k NR + rhs]).
+template <class TF, int NR>
+__device__ __forceinline__ void simple_epilogue(const PArgs<TF>& a, int g, const double (&av)[NR], const double* vk,
+                                                double* vk1, const double* pkm1, const double* pkm2, double* pk,
+                                                const Coef<NR>& cf, double (&r)[4 * NR])
 {
-    const double vkr = vk[g];
-    const double vs = vk1[g] * sc;
-    vk1[g] = vs;
-    double p = vkr;
-    p = fma_rn(nbrr, pkm1[g], p);
-    p = fma_rn(ne, pkm2[g], p);
-    p = p * ir;
-    pk[g] = p;
-    const double xv = fma_rn(tau, p, a.x[g]);
-    a.x[g] = xv;
-    r[3] = fma_rn(xv, xv, r[3]);
     const double dd = (double)__ldg(a.dg + g);
-    const double da = av / dd, dv = vs / dd;
-    r[0] = fma_rn(vkr, da, r[0]);
-    r[1] = fma_rn(vs, da, r[1]);
-    r[2] = fma_rn(vs, dv, r[2]);
+#pragma unroll
+    for (int j = 0; j < NR; ++j) {
+        const size_t o = (size_t)g * NR + j;
+        const double vkr = vk[o];
+        const double vs = vk1[o] * cf.sc[j];
+        vk1[o] = vs;
+        if (cf.act[j]) {
+            double p = vkr;
+            p = fma_rn(cf.nbrr[j], pkm1[o], p);
+            p = fma_rn(cf.ne[j], pkm2[o], p);
+            p = p * cf.ir[j];
+            pk[o] = p;
+            const double xv = fma_rn(cf.tau[j], p, a.xt[o]);
+            a.xt[o] = xv;
+            r[3 * NR + j] = fma_rn(xv, xv, r[3 * NR + j]);
+        }
+        const double da = av[j] / dd, dv = vs / dd;
+        r[j] = fma_rn(vkr, da, r[j]);
+        r[NR + j] = fma_rn(vs, da, r[NR + j]);
+        r[2 * NR + j] = fma_rn(vs, dv, r[2 * NR + j]);
+    }
 }
 
-// The whole preconditioned SQMR solve of one system (see the top of the file).
-template <class TF, class Ctx>
-__device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal& S, double (*sh)[kW])
+// The whole preconditioned SQMR solve of one system for NR right-hand sides
+// at once (see the top of the file): every work item loads the factor and
+// K once for all of them; each right-hand side has its own scalars and stops
+// on its own test (its x is final from then on).
+template <class TF, int NR, class Ctx>
+__device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal (&S)[NR], double (*sh)[kW])
 {
     const int tid = threadIdx.x, lane = (int)lane_id();
     const int wid = ctx.wid, nwarps = ctx.nwarps;
     const int row0 = sv.row0, row1 = sv.row1;
-    if (tid == 0) {
-        memset(&S, 0, sizeof(S));
-        S.c[0] = -1.0;
-    }
+    if (tid == 0)
+        for (int j = 0; j < NR; ++j) {
+            memset(&S[j], 0, sizeof(Scal));
+            S[j].c[0] = -1.0;
+        }
     __syncthreads();
 
     // ---- init: v0 = U'^-1 P' b; ||v0|| ----
-    for (int L = 0; L < a.nl; ++L) {
-        const int r0 = __ldg(sv.qb + L), nr = __ldg(sv.qe + L) - r0;
-        for (int t = wid; t < nr; t += nwarps) {
-            const int I = __ldg(a.lvl_rows + r0 + t);
-            const int fr = __ldg(a.bs + I), h = __ldg(a.bs + I + 1) - fr;
-            ut_item<TF, false>(a, I, fr, h, __ldg(a.rowflags + I), a.b, 1.0, a.v[0]);
+    {
+        double one[NR];
+#pragma unroll
+        for (int j = 0; j < NR; ++j) one[j] = 1.0;
+        for (int L = 0; L < a.nl; ++L) {
+            const int r0 = __ldg(sv.qb + L), nr = __ldg(sv.qe + L) - r0;
+            for (int t = wid; t < nr; t += nwarps) {
+                const int I = __ldg(a.lvl_rows + r0 + t);
+                const int fr = __ldg(a.bs + I), h = __ldg(a.bs + I + 1) - fr;
+                double tt[NR];
+                ut_item<TF, NR, false>(a, I, fr, h, __ldg(a.rowflags + I), a.b, one, a.v[0], tt);
+            }
+            ctx.sync();
         }
-        ctx.sync();
     }
     {
-        double r[1] = {0.0};
-        for (int g = row0 + ctx.g0; g < row1; g += ctx.gstride) r[0] = fma_rn(a.v[0][g], a.v[0][g], r[0]);
-        ctx.template reduce<1>(r, sh);
-        if (tid == 0) {
-            S.norm_pb = sqrt(r[0]);
-            S.gamma = S.norm_pb;
-            S.inv_pb = 1.0 / S.norm_pb;
-        }
+        double r[NR];
+#pragma unroll
+        for (int j = 0; j < NR; ++j) r[j] = 0.0;
+        for (int g = row0 + ctx.g0; g < row1; g += ctx.gstride)
+#pragma unroll
+            for (int j = 0; j < NR; ++j) r[j] = fma_rn(a.v[0][(size_t)g * NR + j], a.v[0][(size_t)g * NR + j], r[j]);
+        ctx.template reduce<NR>(r, sh);
+        if (tid == 0)
+            for (int j = 0; j < NR; ++j) {
+                S[j].norm_pb = sqrt(r[j]);
+                S[j].gamma = S[j].norm_pb;
+                S[j].inv_pb = 1.0 / S[j].norm_pb;
+            }
         __syncthreads();
     }
     // v0 /= ||v0|| (in place), ev = P U^-1 D^-1 v0, ||D^-1 v0||^2
-    double ww = 0.0;
+    double ww[NR];
+#pragma unroll
+    for (int j = 0; j < NR; ++j) ww[j] = 0.0;
     {
-        const double inv_pb = S.inv_pb;
+        double inv_pb[NR];
+#pragma unroll
+        for (int j = 0; j < NR; ++j) inv_pb[j] = S[j].inv_pb;
         for (int L = a.nl - 1; L >= 0; --L) {
             const int r0 = __ldg(sv.qb + L), nr = __ldg(sv.qe + L) - r0;
             for (int t = wid; t < nr; t += nwarps) {
                 const int I = __ldg(a.lvl_rows + r0 + t);
                 const int fr = __ldg(a.bs + I), h = __ldg(a.bs + I + 1) - fr;
-                double y = 0.0;
-                if (lane < h) {
-                    y = a.v[0][fr + lane] * inv_pb;
-                    a.v[0][fr + lane] = y;
+                double y[NR], d[NR];
+#pragma unroll
+                for (int j = 0; j < NR; ++j) {
+                    y[j] = 0.0;
+                    if (lane < h) {
+                        const size_t o = (size_t)(fr + lane) * NR + j;
+                        y[j] = a.v[0][o] * inv_pb[j];
+                        a.v[0][o] = y[j];
+                    }
                 }
-                const double d = u_item<TF>(a, I, fr, h, y, a.ev);
-                ww = fma_rn(d, d, ww);
+                u_item<TF, NR>(a, I, fr, h, y, a.ev, d);
+#pragma unroll
+                for (int j = 0; j < NR; ++j) ww[j] = fma_rn(d[j], d[j], ww[j]);
             }
             ctx.sync();
         }
     }
     // Av = U'^-1 P' K ev; alpha's dots for iteration 0; eta_0 = 1/||D^-1 v0||
     {
-        double r[3] = {ww, 0.0, 0.0};
+        double r[3 * NR];
+        double one[NR];
+#pragma unroll
+        for (int j = 0; j < NR; ++j) {
+            r[j] = ww[j];
+            r[NR + j] = 0.0;
+            r[2 * NR + j] = 0.0;
+            one[j] = 1.0;
+        }
         for (int L = 0; L < a.nl; ++L) {
             const int r0 = __ldg(sv.qb + L), nr = __ldg(sv.qe + L) - r0;
             for (int t = wid; t < nr; t += nwarps) {
                 const int I = __ldg(a.lvl_rows + r0 + t);
                 const int fr = __ldg(a.bs + I), h = __ldg(a.bs + I + 1) - fr;
                 const int flags = __ldg(a.rowflags + I);
-                const double av = ut_item<TF, true>(a, I, fr, h, flags, a.ev, 1.0, a.Av);
-                const double vs = (lane < h) ? a.v[0][fr + lane] : 0.0;
+                double av[NR];
+                ut_item<TF, NR, true>(a, I, fr, h, flags, a.ev, one, a.Av, av);
                 DBlock<TF> D;
                 D.load(a, fr, h, flags);
-                const double da = D.apply(av, h), dv = D.apply(vs, h);
-                if (lane < h) {
-                    r[1] = fma_rn(vs, da, r[1]);
-                    r[2] = fma_rn(vs, dv, r[2]);
+#pragma unroll
+                for (int j = 0; j < NR; ++j) {
+                    const double vs = (lane < h) ? a.v[0][(size_t)(fr + lane) * NR + j] : 0.0;
+                    const double da = D.apply(av[j], h), dv = D.apply(vs, h);
+                    if (lane < h) {
+                        r[NR + j] = fma_rn(vs, da, r[NR + j]);
+                        r[2 * NR + j] = fma_rn(vs, dv, r[2 * NR + j]);
+                    }
                 }
             }
             if (L < a.nl - 1) ctx.sync();
         }
-        ctx.template reduce<3>(r, sh);
-        if (tid == 0) {
-            S.eta = 1.0 / sqrt(r[0]);
-            S.alpha_next = r[1] / r[2];
-            S.vdv = r[2];
-            if (!isfinite(S.inv_pb) || !isfinite(S.eta)) {
-                S.breakdown = 1;
-                S.done = 1;
+        ctx.template reduce<3 * NR>(r, sh);
+        if (tid == 0)
+            for (int j = 0; j < NR; ++j) {
+                S[j].eta = 1.0 / sqrt(r[j]);
+                S[j].alpha_next = r[NR + j] / r[2 * NR + j];
+                S[j].vdv = r[2 * NR + j];
+                if (!isfinite(S[j].inv_pb) || !isfinite(S[j].eta)) {
+                    S[j].breakdown = 1;
+                    S[j].done = 1;
+                }
             }
-        }
         __syncthreads();
     }
 
     int it = 0;
-    while (!S.done && it < a.max_it) {
+    for (;;) {
+        bool any = false;
+#pragma unroll
+        for (int j = 0; j < NR; ++j) any |= !S[j].done;
+        if (!any || it >= a.max_it) break;
         const int k0 = acc3(it), k1 = acc3(it + 1), km1 = acc3(it - 1);
-        stamp(a.ts, it, 0);
-        const double alpha = S.alpha_next, na = -alpha, nb = -S.beta[k0];
+        if (NR == 1) stamp(a.ts, it, 0);
+        double na[NR], nb[NR];
+#pragma unroll
+        for (int j = 0; j < NR; ++j) {
+            na[j] = -S[j].alpha_next;
+            nb[j] = -S[j].beta[k0];
+        }
         const double* const vk = a.v[it & 1];
         double* const vk1 = a.v[(it + 1) & 1];
         const double* const vkm1 = vk1;  // read, then overwritten element by element
         // ---- U sweep on v+ = Av - alpha v - beta v- (each item computes and
         //      stores its rows' v+, kept unscaled), ||v+||^2 ----
         {
-            double r[1] = {0.0};
+            double r[NR];
+#pragma unroll
+            for (int j = 0; j < NR; ++j) r[j] = 0.0;
             for (int L = a.nl - 1; L >= 0; --L) {
                 const int q0 = __ldg(sv.qb + L), q1 = __ldg(sv.qe + L);
                 // block rows with a pivot tile, swaps or 2x2 pivots: warp per block row
@@ -610,67 +755,95 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal&
                 for (int t = __ldg(a.scan_c + q0) + wid; t < c1; t += nwarps) {
                     const int I = __ldg(a.cplx + t);
                     const int fr = __ldg(a.bs + I), h = __ldg(a.bs + I + 1) - fr;
-                    double y = 0.0;
-                    if (lane < h) {
-                        const int g = fr + lane;
-                        y = a.Av[g];
-                        y = fma_rn(na, vk[g], y);
-                        y = fma_rn(nb, vkm1[g], y);
-                        vk1[g] = y;
-                        r[0] = fma_rn(y, y, r[0]);
+                    double y[NR], d[NR];
+#pragma unroll
+                    for (int j = 0; j < NR; ++j) {
+                        y[j] = 0.0;
+                        if (lane < h) {
+                            const size_t o = (size_t)(fr + lane) * NR + j;
+                            double v = a.Av[o];
+                            v = fma_rn(na[j], vk[o], v);
+                            v = fma_rn(nb[j], vkm1[o], v);
+                            vk1[o] = v;
+                            r[j] = fma_rn(v, v, r[j]);
+                            y[j] = v;
+                        }
                     }
-                    u_item<TF>(a, I, fr, h, y, a.ev);
+                    u_item<TF, NR>(a, I, fr, h, y, a.ev, d);
                 }
                 // rows of simple block rows: thread per row (u_item with D = d,
                 // an identity tile and no swaps)
                 const int s1 = __ldg(a.scan_s + q1);
                 for (int i = __ldg(a.scan_s + q0) + ctx.g0; i < s1; i += ctx.gstride) {
                     const int g = __ldg(a.simple_rows + i);
-                    double y = a.Av[g];
-                    y = fma_rn(na, vk[g], y);
-                    y = fma_rn(nb, vkm1[g], y);
-                    vk1[g] = y;
-                    r[0] = fma_rn(y, y, r[0]);
-                    const double d = y / (double)__ldg(a.dg + g);
-                    a.ev[g] = (double)row_sub<TF>((TF)d, __ldg(a.u_off + g), __ldg(a.u_off + g + 1), a.u_colp, a.u_val,
-                                                  a.ev);
+                    const double dd = (double)__ldg(a.dg + g);
+                    TF acc[NR];
+#pragma unroll
+                    for (int j = 0; j < NR; ++j) {
+                        const size_t o = (size_t)g * NR + j;
+                        double v = a.Av[o];
+                        v = fma_rn(na[j], vk[o], v);
+                        v = fma_rn(nb[j], vkm1[o], v);
+                        vk1[o] = v;
+                        r[j] = fma_rn(v, v, r[j]);
+                        acc[j] = (TF)(v / dd);
+                    }
+                    row_sub<TF, NR>(acc, __ldg(a.u_off + g), __ldg(a.u_off + g + 1), a.u_colp, a.u_val, a.ev);
+#pragma unroll
+                    for (int j = 0; j < NR; ++j) a.ev[(size_t)g * NR + j] = (double)acc[j];
                 }
                 if (L > 0) {
                     ctx.sync();
-                    if (L == a.nl - 1) stamp(a.ts, it, 1);
+                    if (NR == 1 && L == a.nl - 1) stamp(a.ts, it, 1);
                 }
             }
-            ctx.template reduce<1>(r, sh);
-            if (tid == 0) {
-                S.alpha = alpha;
-                const double bk = S.beta[k0];
-                const double dl = sqrt(r[0]);
-                S.delta[k1] = dl;
-                S.inv_delta = 1.0 / dl;
-                const double nA = sqrt(fma_rn(dl, dl, fma_rn(alpha, alpha, bk * bk)));
-                S.norm_A = fmax(S.norm_A, nA);
-                S.epsilon = S.s[km1] * bk;
-                const double beta_rot = (-S.c[km1]) * bk;
-                S.beta_rr = fma_rn(S.c[k0], beta_rot, S.s[k0] * alpha);
-                const double alpha_rot = fma_rn(S.s[k0], beta_rot, (-S.c[k0]) * alpha);
-                double c, s, rr;
-                sym_ortho(alpha_rot, dl, c, s, rr);
-                S.c[k1] = c;
-                S.s[k1] = s;
-                S.rho = rr;
-                S.inv_rho = 1.0 / rr;
-                S.tau = c * S.gamma;
-                S.gamma = s * S.gamma;
-            }
+            ctx.template reduce<NR>(r, sh);
+            if (tid == 0)
+                for (int j = 0; j < NR; ++j) {
+                    if (S[j].done) continue;
+                    Scal& Q = S[j];
+                    const double alpha = Q.alpha_next;
+                    Q.alpha = alpha;
+                    const double bk = Q.beta[k0];
+                    const double dl = sqrt(r[j]);
+                    Q.delta[k1] = dl;
+                    Q.inv_delta = 1.0 / dl;
+                    const double nA = sqrt(fma_rn(dl, dl, fma_rn(alpha, alpha, bk * bk)));
+                    Q.norm_A = fmax(Q.norm_A, nA);
+                    Q.epsilon = Q.s[km1] * bk;
+                    const double beta_rot = (-Q.c[km1]) * bk;
+                    Q.beta_rr = fma_rn(Q.c[k0], beta_rot, Q.s[k0] * alpha);
+                    const double alpha_rot = fma_rn(Q.s[k0], beta_rot, (-Q.c[k0]) * alpha);
+                    double c, s, rr;
+                    sym_ortho(alpha_rot, dl, c, s, rr);
+                    Q.c[k1] = c;
+                    Q.s[k1] = s;
+                    Q.rho = rr;
+                    Q.inv_rho = 1.0 / rr;
+                    Q.tau = c * Q.gamma;
+                    Q.gamma = s * Q.gamma;
+                }
             __syncthreads();
         }
-        if (a.nl == 1) stamp(a.ts, it, 1);
-        stamp(a.ts, it, 2);
-        // ---- P3: U' sweep with the fused SpMV; beta's and alpha's dots; p, x ----
+        if (NR == 1) {
+            if (a.nl == 1) stamp(a.ts, it, 1);
+            stamp(a.ts, it, 2);
+        }
+        // ---- U' sweep with the fused SpMV; beta's and alpha's dots; p, x ----
         {
-            double r[4] = {0.0, 0.0, 0.0, 0.0};
-            const double sc = S.inv_delta;
-            const double nbrr = -S.beta_rr, ne = -S.epsilon, ir = S.inv_rho, tau = S.tau;
+            double r[4 * NR];
+#pragma unroll
+            for (int j = 0; j < 4 * NR; ++j) r[j] = 0.0;
+            Coef<NR> cf;
+#pragma unroll
+            for (int j = 0; j < NR; ++j) {
+                cf.sc[j] = S[j].inv_delta;
+                cf.nbrr[j] = -S[j].beta_rr;
+                cf.ne[j] = -S[j].epsilon;
+                cf.ir[j] = S[j].inv_rho;
+                cf.tau[j] = S[j].tau;
+                cf.act[j] = !S[j].done;
+            }
             double* const pk = a.p[it & 1];
             const double* const pkm1 = a.p[(it + 1) & 1];
             const double* const pkm2 = pk;  // read, then overwritten element by element
@@ -681,30 +854,36 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal&
                     const int I = __ldg(a.cplx + t);
                     const int fr = __ldg(a.bs + I), h = __ldg(a.bs + I + 1) - fr;
                     const int flags = __ldg(a.rowflags + I);
-                    const double av = ut_item<TF, true>(a, I, fr, h, flags, a.ev, sc, a.Av);
-                    double vkr = 0.0, vs = 0.0;
-                    if (lane < h) {
-                        const int g = fr + lane;
-                        vkr = vk[g];
-                        vs = vk1[g] * sc;
-                        vk1[g] = vs;
-                        // p_k = (v_k - beta_rr p_k-1 - epsilon p_k-2) / rho, x += tau p_k
-                        double p = vkr;
-                        p = fma_rn(nbrr, pkm1[g], p);
-                        p = fma_rn(ne, pkm2[g], p);
-                        p = p * ir;
-                        pk[g] = p;
-                        const double xv = fma_rn(tau, p, a.x[g]);
-                        a.x[g] = xv;
-                        r[3] = fma_rn(xv, xv, r[3]);
-                    }
+                    double av[NR];
+                    ut_item<TF, NR, true>(a, I, fr, h, flags, a.ev, cf.sc, a.Av, av);
                     DBlock<TF> D;
                     D.load(a, fr, h, flags);
-                    const double da = D.apply(av, h), dv = D.apply(vs, h);
-                    if (lane < h) {
-                        r[0] = fma_rn(vkr, da, r[0]);
-                        r[1] = fma_rn(vs, da, r[1]);
-                        r[2] = fma_rn(vs, dv, r[2]);
+#pragma unroll
+                    for (int j = 0; j < NR; ++j) {
+                        double vkr = 0.0, vs = 0.0;
+                        if (lane < h) {
+                            const size_t o = (size_t)(fr + lane) * NR + j;
+                            vkr = vk[o];
+                            vs = vk1[o] * cf.sc[j];
+                            vk1[o] = vs;
+                            if (cf.act[j]) {
+                                // p_k = (v_k - beta_rr p_k-1 - epsilon p_k-2) / rho, x += tau p_k
+                                double p = vkr;
+                                p = fma_rn(cf.nbrr[j], pkm1[o], p);
+                                p = fma_rn(cf.ne[j], pkm2[o], p);
+                                p = p * cf.ir[j];
+                                pk[o] = p;
+                                const double xv = fma_rn(cf.tau[j], p, a.xt[o]);
+                                a.xt[o] = xv;
+                                r[3 * NR + j] = fma_rn(xv, xv, r[3 * NR + j]);
+                            }
+                        }
+                        const double da = D.apply(av[j], h), dv = D.apply(vs, h);
+                        if (lane < h) {
+                            r[j] = fma_rn(vkr, da, r[j]);
+                            r[NR + j] = fma_rn(vs, da, r[NR + j]);
+                            r[2 * NR + j] = fma_rn(vs, dv, r[2 * NR + j]);
+                        }
                     }
                 }
                 // simple rows of this level: Av; their dots and the p / x
@@ -714,11 +893,19 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal&
                 const int s1 = __ldg(a.scan_s + q1);
                 for (int i = __ldg(a.scan_s + q0) + ctx.g0; i < s1; i += ctx.gstride) {
                     const int g = __ldg(a.simple_rows + i);
-                    const double y = spmv_row(a, g, a.ev) * sc;
-                    const double av = (double)row_sub<TF>((TF)y, __ldg(a.ut_off + g), __ldg(a.ut_off + g + 1), a.ut_col,
-                                                          a.ut_val, a.Av);
-                    a.Av[g] = av;
-                    if (last) simple_epilogue(a, g, av, vk, vk1, pkm1, pkm2, pk, sc, nbrr, ne, ir, tau, r);
+                    double y[NR];
+                    spmv_row<TF, NR>(a, g, a.ev, y);
+                    TF acc[NR];
+#pragma unroll
+                    for (int j = 0; j < NR; ++j) acc[j] = (TF)(y[j] * cf.sc[j]);
+                    row_sub<TF, NR>(acc, __ldg(a.ut_off + g), __ldg(a.ut_off + g + 1), a.ut_col, a.ut_val, a.Av);
+                    double av[NR];
+#pragma unroll
+                    for (int j = 0; j < NR; ++j) {
+                        av[j] = (double)acc[j];
+                        a.Av[(size_t)g * NR + j] = av[j];
+                    }
+                    if (last) simple_epilogue<TF, NR>(a, g, av, vk, vk1, pkm1, pkm2, pk, cf, r);
                 }
                 if (L > 0) {
                     // warps without a block row in this level take the tails;
@@ -732,86 +919,103 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal&
                         const int ts = spare ? (nwarps - items) * 32 : ctx.gstride;
                         for (int i = __ldg(a.scan_s + p0) + t0; i < e1; i += ts) {
                             const int g = __ldg(a.simple_rows + i);
-                            simple_epilogue(a, g, a.Av[g], vk, vk1, pkm1, pkm2, pk, sc, nbrr, ne, ir, tau, r);
+                            double av[NR];
+#pragma unroll
+                            for (int j = 0; j < NR; ++j) av[j] = a.Av[(size_t)g * NR + j];
+                            simple_epilogue<TF, NR>(a, g, av, vk, vk1, pkm1, pkm2, pk, cf, r);
                         }
                     }
                 }
                 if (L < a.nl - 1) {
                     ctx.sync();
-                    if (L == 0) stamp(a.ts, it, 4);
+                    if (NR == 1 && L == 0) stamp(a.ts, it, 4);
                 }
             }
-            ctx.template reduce<4>(r, sh);
-            if (tid == 0) {
-                const double bt = r[0] / S.vdv;
-                S.beta[k1] = bt;
-                S.inv_beta = 1.0 / bt;
-                S.eta = (S.delta[k1] / bt) * S.eta;
-                S.alpha_next = r[1] / r[2];
-                S.vdv = r[2];
-                S.norm_x = sqrt(r[3]);
-                S.test0 |= (fabs(S.delta[k1]) <= a.tol);
-                S.test1 |= (S.gamma / fma_rn(S.norm_A, S.norm_x, S.norm_pb) <= a.tol);
-                bool stop = false;
-                if (it > 0 && (it % 4) == 0) {
-                    if (S.snap0 || S.snap1) {
-                        stop = true;
-                        S.iters = it;
+            ctx.template reduce<4 * NR>(r, sh);
+            if (tid == 0)
+                for (int j = 0; j < NR; ++j) {
+                    Scal& Q = S[j];
+                    if (Q.done) continue;
+                    const double bt = r[j] / Q.vdv;
+                    Q.beta[k1] = bt;
+                    Q.inv_beta = 1.0 / bt;
+                    Q.eta = (Q.delta[k1] / bt) * Q.eta;
+                    Q.alpha_next = r[NR + j] / r[2 * NR + j];
+                    Q.vdv = r[2 * NR + j];
+                    Q.norm_x = sqrt(r[3 * NR + j]);
+                    Q.test0 |= (fabs(Q.delta[k1]) <= a.tol);
+                    Q.test1 |= (Q.gamma / fma_rn(Q.norm_A, Q.norm_x, Q.norm_pb) <= a.tol);
+                    bool stop = false;
+                    if (it > 0 && (it % 4) == 0) {
+                        if (Q.snap0 || Q.snap1) {
+                            stop = true;
+                            Q.iters = it;
+                        }
+                    } else if (((it + 1) % 4) == 0) {
+                        Q.snap0 = Q.test0;
+                        Q.snap1 = Q.test1;
                     }
-                } else if (((it + 1) % 4) == 0) {
-                    S.snap0 = S.test0;
-                    S.snap1 = S.test1;
+                    if (!isfinite(Q.inv_beta) || !isfinite(Q.inv_rho) || !isfinite(Q.eta) ||
+                        !isfinite(Q.inv_delta) || !isfinite(Q.alpha)) {
+                        Q.breakdown = 1;
+                        stop = true;
+                        Q.iters = it;
+                    }
+                    if (!stop && it + 1 >= a.max_it) Q.iters = a.max_it;
+                    if (stop) {
+                        Q.done = 1;
+                        Q.stop_it = it;
+                    }
                 }
-                if (!isfinite(S.inv_beta) || !isfinite(S.inv_rho) || !isfinite(S.eta) || !isfinite(S.inv_delta) ||
-                    !isfinite(S.alpha)) {
-                    S.breakdown = 1;
-                    stop = true;
-                    S.iters = it;
-                }
-                if (!stop && it + 1 >= a.max_it) S.iters = a.max_it;
-                if (stop) S.done = 1;
-            }
             __syncthreads();
         }
-        stamp(a.ts, it, 3);
-        if (!S.done) ++it;
+        if (NR == 1) stamp(a.ts, it, 3);
+        bool more = false;
+#pragma unroll
+        for (int j = 0; j < NR; ++j) more |= !S[j].done;
+        if (more) ++it;
+        else break;
     }
-    if (tid == 0 && !S.done) S.iters = it;
-    __syncthreads();
-    // ---- x = P U^-1 D^-1 x~ ----
-    for (int g = row0 + ctx.g0; g < row1; g += ctx.gstride) a.tmp[g] = a.x[g];
-    ctx.sync();
+    // ---- x = P U^-1 D^-1 x~ into ev, then x (column-major) ----
     for (int L = a.nl - 1; L >= 0; --L) {
         const int r0 = __ldg(sv.qb + L), nr = __ldg(sv.qe + L) - r0;
         for (int t = wid; t < nr; t += nwarps) {
             const int I = __ldg(a.lvl_rows + r0 + t);
             const int fr = __ldg(a.bs + I), h = __ldg(a.bs + I + 1) - fr;
-            const double y = (lane < h) ? a.tmp[fr + lane] : 0.0;
-            u_item<TF>(a, I, fr, h, y, a.x);
+            double y[NR], d[NR];
+#pragma unroll
+            for (int j = 0; j < NR; ++j) y[j] = (lane < h) ? a.xt[(size_t)(fr + lane) * NR + j] : 0.0;
+            u_item<TF, NR>(a, I, fr, h, y, a.ev, d);
         }
-        if (L > 0) ctx.sync();
+        ctx.sync();
     }
-    if (sv.out && tid == 0) {
-        sv.out[0] = S.gamma / S.norm_pb;
-        sv.out[1] = S.iters;
-        sv.out[2] = S.breakdown;
-        sv.out[3] = (S.snap0 || S.snap1) ? 1 : 0;
-        sv.out[4] = S.norm_pb;
-        sv.out[5] = it;
-    }
+    for (int g = row0 + ctx.g0; g < row1; g += ctx.gstride)
+#pragma unroll
+        for (int j = 0; j < NR; ++j) a.x[(size_t)j * a.n + g] = a.ev[(size_t)g * NR + j];
+    if (sv.out && tid == 0)
+        for (int j = 0; j < NR; ++j) {
+            const Scal& Q = S[j];
+            double* o = sv.out + 8 * j;
+            o[0] = Q.gamma / Q.norm_pb;
+            o[1] = Q.done ? Q.iters : it;
+            o[2] = Q.breakdown;
+            o[3] = (Q.snap0 || Q.snap1) ? 1 : 0;
+            o[4] = Q.norm_pb;
+            o[5] = Q.done ? Q.stop_it : it;
+        }
     __syncthreads();
 }
 
-template <class TF, int CTAS>
+template <class TF, int CTAS, int NR>
 __global__ void __launch_bounds__(kT, CTAS) k_sqmr_persistent(PArgs<TF> a)
 {
-    __shared__ Scal S;
+    __shared__ Scal S[NR];
     __shared__ double sh[kMaxNV][kW];
     const int G = gridDim.x;
     GridCtx ctx{cg::this_grid(), a.partials, 0, (int)(threadIdx.x >> 5) * G + (int)blockIdx.x,  // items interleaved
                 G * kW, (int)(blockIdx.x * kT + threadIdx.x), G * kT};
     const SysView sv{0, a.n, a.lvl_off, a.lvl_off + 1, blockIdx.x == 0 ? a.out : nullptr};
-    sqmr_body<TF>(a, ctx, sv, S, sh);
+    sqmr_body<TF, NR>(a, ctx, sv, S, sh);
 }
 
 // Batched solves of independent systems stored as one block-diagonal union
@@ -830,7 +1034,7 @@ struct BatchArgs {
 template <class TF>
 __global__ void __launch_bounds__(kT, kCtasPerSm) k_sqmr_batched(PArgs<TF> a, BatchArgs bt)
 {
-    __shared__ Scal S;
+    __shared__ Scal S[1];
     __shared__ double sh[kMaxNV][kW];
     __shared__ int sys;
     CtaCtx ctx{(int)(threadIdx.x >> 5), kW, (int)threadIdx.x, kT};
@@ -842,7 +1046,7 @@ __global__ void __launch_bounds__(kT, kCtasPerSm) k_sqmr_batched(PArgs<TF> a, Ba
         if (s >= bt.num) break;
         const SysView sv{__ldg(bt.row_off + s), __ldg(bt.row_off + s + 1), bt.qb + (size_t)s * a.nl,
                          bt.qe + (size_t)s * a.nl, bt.out + (size_t)s * 8};
-        sqmr_body<TF>(a, ctx, sv, S, sh);
+        sqmr_body<TF, 1>(a, ctx, sv, S, sh);
     }
 }
 
@@ -853,7 +1057,7 @@ template <class TF>
 __global__ void __launch_bounds__(kT, kCtasPerSm) k_sqmr_many(const PArgs<TF>* __restrict__ sys_args, int num,
                                                              int* next)
 {
-    __shared__ Scal S;
+    __shared__ Scal S[1];
     __shared__ double sh[kMaxNV][kW];
     __shared__ int sys;
     __shared__ PArgs<TF> pa;
@@ -869,14 +1073,14 @@ __global__ void __launch_bounds__(kT, kCtasPerSm) k_sqmr_many(const PArgs<TF>* _
         for (int i = threadIdx.x; i < (int)(sizeof(PArgs<TF>) / 8); i += kT) dst[i] = src[i];
         __syncthreads();
         const SysView sv{0, pa.n, pa.lvl_off, pa.lvl_off + 1, pa.out};
-        sqmr_body<TF>(pa, ctx, sv, S, sh);
+        sqmr_body<TF, 1>(pa, ctx, sv, S, sh);
     }
 }
 
-// kernel arguments over a work area of kVecs n doubles + 6 (vectors, then out)
+// kernel arguments over a work area of kVecs n nr doubles + 8 nr (vectors, then out)
 template <class TF>
 PArgs<TF> make_args(Csr* A, Factor* M, double* base, double* partials, const double* b, double* x, double tol,
-                    int max_it)
+                    int max_it, int nr = 1)
 {
     Pattern& p = *M->pat;
     const int n = A->m;
@@ -910,14 +1114,15 @@ PArgs<TF> make_args(Csr* A, Factor* M, double* base, double* partials, const dou
     a.scan_c = M->scan_c.as<int>();
     a.simple_rows = M->simple_rows.as<int>();
     a.cplx = M->cplx.as<int>();
+    const size_t vn = (size_t)n * nr;
     for (int i = 0; i < 2; ++i) {
-        a.v[i] = base + (size_t)i * n;
-        a.p[i] = base + (size_t)(2 + i) * n;
+        a.v[i] = base + (size_t)i * vn;
+        a.p[i] = base + (size_t)(2 + i) * vn;
     }
-    a.Av = base + (size_t)4 * n;
-    a.ev = base + (size_t)5 * n;
-    a.tmp = base + (size_t)6 * n;
-    a.out = base + (size_t)kVecs * n;
+    a.Av = base + (size_t)4 * vn;
+    a.ev = base + (size_t)5 * vn;
+    a.xt = base + (size_t)6 * vn;
+    a.out = base + (size_t)kVecs * vn;
     a.partials = partials;
     a.ts = nullptr;
     a.x = x;
@@ -934,72 +1139,138 @@ int ctas_per_sm()
     return c;
 }
 
-template <class TF>
+template <class TF, int NR>
 const void* persistent_kernel()
 {
-    return ctas_per_sm() == 1 ? (const void*)k_sqmr_persistent<TF, 1> : (const void*)k_sqmr_persistent<TF, 2>;
+    return ctas_per_sm() == 1 ? (const void*)k_sqmr_persistent<TF, 1, NR> : (const void*)k_sqmr_persistent<TF, 2, NR>;
 }
 
 // resident CTAs for the cooperative launch
-template <class TF>
+template <class TF, int NR>
 int persistent_grid(int dev, int* G)
 {
     int per_sm = 0, sms = 0;
     CULIPX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    CULIPX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, persistent_kernel<TF>(), kT, 0));
+    CULIPX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, persistent_kernel<TF, NR>(), kT, 0));
     if (per_sm < 1) return fail(CULIPX_NOT_SUPPORTED, "persistent SQMR kernel does not fit on an SM");
     *G = sms * std::min(per_sm, ctas_per_sm());
     return CULIPX_OK;
 }
 
-template <class TF>
-int run_persistent(culipx_handle_t* h, PArgs<TF>& a, int G, double* residual, int* iterations, bool* converged,
-                   bool* breakdown)
+// launch and wait; out_host receives 8 values per right-hand side
+template <class TF, int NR>
+int run_persistent(culipx_handle_t* h, PArgs<TF>& a, int G, double* out_host)
 {
     cudaStream_t s = h->stream;
     // the recurrence vectors start at zero; x is zeroed as in the reference
-    CULIPX_CUDA(cudaMemsetAsync(a.v[0], 0, (size_t)kVecs * a.n * sizeof(double), s));
-    CULIPX_CUDA(cudaMemsetAsync(a.x, 0, (size_t)a.n * sizeof(double), s));
+    CULIPX_CUDA(cudaMemsetAsync(a.v[0], 0, (size_t)kVecs * a.n * NR * sizeof(double), s));
+    CULIPX_CUDA(cudaMemsetAsync(a.x, 0, (size_t)a.n * NR * sizeof(double), s));
     void* args[] = {&a};
-    CULIPX_CUDA(cudaLaunchCooperativeKernel(persistent_kernel<TF>(), dim3(G), dim3(kT), args, 0, s));
+    CULIPX_CUDA(cudaLaunchCooperativeKernel(persistent_kernel<TF, NR>(), dim3(G), dim3(kT), args, 0, s));
     h->launches += 1;
-    double out[6];
-    CULIPX_CUDA(cudaMemcpyAsync(out, a.out, sizeof(out), cudaMemcpyDeviceToHost, s));
+    CULIPX_CUDA(cudaMemcpyAsync(out_host, a.out, (size_t)8 * NR * sizeof(double), cudaMemcpyDeviceToHost, s));
     CULIPX_CUDA(cudaStreamSynchronize(s));
-    if (residual) *residual = out[0];
-    if (iterations) *iterations = (int)out[1];
-    *breakdown = out[2] != 0.0;
-    *converged = out[3] != 0.0;
     return CULIPX_OK;
 }
 
-template <class TF>
+template <class TF, int NR>
 int launch_persistent(culipx_handle_t* h, Csr* A, Factor* M, const double* b, double* x, double tol, int max_it,
-                      double* residual, int* iterations, Sqmr* w, bool* converged, bool* breakdown)
+                      Sqmr* w, double* out_host)
 {
     const int n = A->m;
     cudaStream_t s = h->stream;
-    CULIPX_TRY(sqmr_workspace(w, h, n));
-    static int grid_cache[2] = {0, 0};
-    int& G = grid_cache[sizeof(TF) == 8 ? 0 : 1];
+    const size_t need = ((size_t)kVecs * n * NR + 8 * NR + 64) * sizeof(double);
+    if (w->vecs.bytes() < need) {
+        CULIPX_TRY(w->vecs.alloc(h, need));
+        w->n = -1;  // the single-RHS workspace size is no longer known
+    }
+    if (NR == 1) CULIPX_TRY(sqmr_workspace(w, h, n));
+    static int grid_cache[2][kMaxNR + 1] = {};
+    int& G = grid_cache[sizeof(TF) == 8 ? 0 : 1][NR];
     if (G == 0) {
         int dev = 0;
         CULIPX_CUDA(cudaGetDevice(&dev));
-        CULIPX_TRY(persistent_grid<TF>(dev, &G));
+        CULIPX_TRY((persistent_grid<TF, NR>(dev, &G)));
     }
     if ((size_t)(2 * kMaxNV * G) * sizeof(double) > w->partials.bytes())
         CULIPX_TRY(w->partials.alloc(h, (size_t)2 * kMaxNV * G * sizeof(double)));
-    PArgs<TF> a = make_args<TF>(A, M, w->vecs.as<double>(), w->partials.as<double>(), b, x, tol, max_it);
-    if (w->profile) {
+    PArgs<TF> a = make_args<TF>(A, M, w->vecs.as<double>(), w->partials.as<double>(), b, x, tol, max_it, NR);
+    if (w->profile && NR == 1) {
         if (w->ts.bytes() < (size_t)kTsIters * 8 * sizeof(unsigned long long))
             CULIPX_TRY(w->ts.alloc(h, (size_t)kTsIters * 8 * sizeof(unsigned long long)));
         CULIPX_CUDA(cudaMemsetAsync(w->ts.get(), 0, (size_t)kTsIters * 8 * sizeof(unsigned long long), s));
         a.ts = w->ts.as<unsigned long long>();
     }
-    return run_persistent<TF>(h, a, G, residual, iterations, converged, breakdown);
+    return run_persistent<TF, NR>(h, a, G, out_host);
+}
+
+template <class TF>
+int launch_nr(int nr, culipx_handle_t* h, Csr* A, Factor* M, const double* b, double* x, double tol, int max_it,
+              Sqmr* w, double* out_host)
+{
+    switch (nr) {
+    case 1: return launch_persistent<TF, 1>(h, A, M, b, x, tol, max_it, w, out_host);
+    case 2: return launch_persistent<TF, 2>(h, A, M, b, x, tol, max_it, w, out_host);
+    default: return launch_persistent<TF, 4>(h, A, M, b, x, tol, max_it, w, out_host);
+    }
+}
+
+int status_of(const double* o, int max_it)
+{
+    if (o[2] != 0.0) return CULIPX_BREAKDOWN;
+    if (o[3] == 0.0 && max_it > 0 && (int)o[1] >= max_it) return CULIPX_MAXIT;
+    return CULIPX_OK;
 }
 
 }  // namespace
+
+// nrhs right-hand sides (column-major n x nrhs) in launches of up to
+// kMaxNR at a time; per right-hand side the quasi-residual, iterations and
+// status (OK / MAXIT / BREAKDOWN)
+int sqmr_solve_multi(culipx_handle_t* h, Csr* A, Factor* M, int nrhs, const double* B, double* X, double tol,
+                     int max_it, double* h_res, int* h_its, int* h_status, Sqmr* w)
+{
+    if (!A || !M || !B || !X || !w || nrhs < 1) return fail(CULIPX_INVALID_ARG, "culipx_sqmr_solve_multi: bad argument");
+    if (A->precision != CULIPX_F64 || A->m != A->n || !M->computed || M->pat->n != A->m)
+        return fail(CULIPX_INVALID_ARG, "culipx_sqmr_solve_multi: A must be square FP64 and M its computed factor");
+    if (M->solve_algorithm == CULIPX_SOLVE_JACOBI)
+        return fail(CULIPX_NOT_SUPPORTED, "culipx_sqmr_solve_multi: SOLVE_JACOBI needs culipx_sqmr_solve");
+    if (max_it < 0) return fail(CULIPX_INVALID_ARG, "culipx_sqmr_solve_multi: max_it < 0");
+    const size_t n = A->m;
+    double out[8 * kMaxNR];
+    for (int r0 = 0; r0 < nrhs; r0 += kMaxNR) {
+        const int nr = std::min(kMaxNR, nrhs - r0);
+        // 3 right-hand sides run as 4, the fourth a copy of the third: it stops
+        // when the third does and its x is dropped
+        const int nl = (nr == 1) ? 1 : (nr == 2) ? 2 : 4;
+        const double* b = B + r0 * n;
+        double* x = X + r0 * n;
+        DeviceBuffer pad_b, pad_x;
+        if (nl != nr) {
+            CULIPX_TRY(pad_b.alloc(h, nl * n * sizeof(double)));
+            CULIPX_TRY(pad_x.alloc(h, nl * n * sizeof(double)));
+            CULIPX_CUDA(cudaMemcpyAsync(pad_b.get(), b, nr * n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+            CULIPX_CUDA(cudaMemcpyAsync(pad_b.as<double>() + nr * n, b + (nr - 1) * n, n * sizeof(double),
+                                        cudaMemcpyDeviceToDevice, h->stream));
+            b = pad_b.as<double>();
+            x = pad_x.as<double>();
+        }
+        const int st = (M->precision == CULIPX_F64) ? launch_nr<double>(nl, h, A, M, b, x, tol, max_it, w, out)
+                                                    : launch_nr<float>(nl, h, A, M, b, x, tol, max_it, w, out);
+        if (st != CULIPX_OK) return st;
+        if (nl != nr) {
+            CULIPX_CUDA(cudaMemcpyAsync(X + r0 * n, x, nr * n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+            CULIPX_CUDA(cudaStreamSynchronize(h->stream));
+        }
+        for (int j = 0; j < nr; ++j) {
+            const double* o = out + 8 * j;
+            if (h_res) h_res[r0 + j] = o[0];
+            if (h_its) h_its[r0 + j] = (int)o[1];
+            if (h_status) h_status[r0 + j] = status_of(o, max_it);
+        }
+    }
+    return CULIPX_OK;
+}
 
 // ---------------------------------------------------------------------------
 // Batched solves (no counterpart in the reference, which solves one system
@@ -1220,13 +1491,14 @@ int sqmr_solve_many(culipx_handle_t* h, int num, Csr* const* A, Factor* const* M
 int sqmr_solve_persistent(culipx_handle_t* h, Csr* A, Factor* M, const double* b, double* x, double tol, int max_it,
                           double* residual, int* iterations, Sqmr* w)
 {
-    bool conv = false, bd = false;
-    int st;
-    if (M->precision == CULIPX_F64) st = launch_persistent<double>(h, A, M, b, x, tol, max_it, residual, iterations, w, &conv, &bd);
-    else st = launch_persistent<float>(h, A, M, b, x, tol, max_it, residual, iterations, w, &conv, &bd);
+    double out[8];
+    const int st = (M->precision == CULIPX_F64) ? launch_persistent<double, 1>(h, A, M, b, x, tol, max_it, w, out)
+                                                : launch_persistent<float, 1>(h, A, M, b, x, tol, max_it, w, out);
     if (st != CULIPX_OK) return st;
-    if (bd) return fail(CULIPX_BREAKDOWN, "culipx_sqmr_solve: breakdown (non-finite scalar)");
-    if (!conv && max_it > 0 && iterations && *iterations >= max_it) return CULIPX_MAXIT;
+    if (residual) *residual = out[0];
+    if (iterations) *iterations = (int)out[1];
+    if (out[2] != 0.0) return fail(CULIPX_BREAKDOWN, "culipx_sqmr_solve: breakdown (non-finite scalar)");
+    if (out[3] == 0.0 && max_it > 0 && (int)out[1] >= max_it) return CULIPX_MAXIT;
     return CULIPX_OK;
 }
 
@@ -1282,7 +1554,7 @@ int noalloc_grid(int dev, int* G)
 {
     int& g = g_noalloc_grid[dev][sizeof(TF) == 8 ? 0 : 1];
     if (g == 0) {
-        CULIPX_TRY(persistent_grid<TF>(dev, &g));
+        CULIPX_TRY((persistent_grid<TF, 1>(dev, &g)));
         g = std::min(g, kNoAllocMaxGrid);
     }
     *G = g;
@@ -1301,7 +1573,13 @@ int launch_noalloc(culipx_handle_t* h, Csr* A, Factor* M, const double* b, doubl
     double* base = g_noalloc_ptr[dev];
     // run_persistent clears the recurrence vectors the scratch kept from the last call
     PArgs<TF> a = make_args<TF>(A, M, base, base + kNoAllocVecs, b, x, tol, max_it);
-    return run_persistent<TF>(h, a, G, residual, iterations, converged, breakdown);
+    double out[8];
+    CULIPX_TRY((run_persistent<TF, 1>(h, a, G, out)));
+    if (residual) *residual = out[0];
+    if (iterations) *iterations = (int)out[1];
+    *breakdown = out[2] != 0.0;
+    *converged = out[3] != 0.0;
+    return CULIPX_OK;
 }
 
 }  // namespace

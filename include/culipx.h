@@ -252,6 +252,17 @@ int culipx_batch_destroy(culipx_batch b);
 int culipx_batch_sqmr_solve(culipx_batch b, culipx_csr A, culipx_factor M, const double *d_b, double *d_x,
                             double tol, int max_it, double *h_residual, int *h_iterations, int *h_status);
 
+/* Several right-hand sides of one system (no counterpart in the reference,
+ * whose SQMR takes one): d_B and d_X are n x nrhs column-major.  Up to four
+ * right-hand sides share one launch, in which every work item reads the
+ * factor and K once for all of them; each has its own SQMR scalars and
+ * stopping test (tol, max_it as culipx_sqmr_solve) and its x is final once
+ * it stops.  Per right-hand side: quasi-residual, iterations, status (OK,
+ * MAXIT, BREAKDOWN); any of the three may be NULL. */
+int culipx_sqmr_solve_multi(culipx_handle h, culipx_csr A, culipx_factor M, int nrhs, const double *d_B,
+                            double *d_X, double tol, int max_it, double *h_residual, int *h_iterations,
+                            int *h_status);
+
 /* Many independent systems, each with its own pattern, factor, matrix and
  * vectors (no union), solved in one launch, one CTA per system; all factors
  * of one call share a precision.  Same per-system outputs as

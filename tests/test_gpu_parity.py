@@ -168,6 +168,46 @@ def test_sqmr_reference_fixture_unpreconditioned(handle):
     assert abs(its - ito) <= 4
 
 
+@pytest.mark.parametrize("precision", [cb.F64, cb.F32])
+@pytest.mark.parametrize("nrhs", [1, 2, 3, 4, 6])
+def test_sqmr_multi_rhs(handle, precision, nrhs):
+    """Several right-hand sides in one launch: each follows its own SQMR
+    recurrence and stopping test, so it matches its single-RHS solve up to
+    summation order, and its x stays final once it stops."""
+    rp, ci, v, bs = kkt("small")
+    n = len(rp) - 1
+    P = cb.Pattern(handle, rp, ci, bs, 0, 1.0, precision)
+    F = cb.Factor(P)
+    F.compute(torch.from_numpy(v.astype(np.float32 if precision == cb.F32 else np.float64)).cuda())
+    A = _csr_op(handle, rp, ci, v)
+    rng = np.random.default_rng(77 + nrhs)
+    B = rng.standard_normal((nrhs, n))
+    B[-1] *= 1e-3  # a small right-hand side converges at its own iteration
+    X = torch.full((nrhs, n), 7.0, dtype=torch.float64, device="cuda")
+    res, its, st = cb.sqmr_solve_multi(handle, A, F, torch.from_numpy(B).cuda(), X, 1e-8, 1000)
+    import scipy.sparse as sp
+
+    K = sp.csr_matrix((v, ci, rp))
+    X = X.cpu().numpy()
+    for r in range(nrhs):
+        x1 = torch.zeros(n, dtype=torch.float64, device="cuda")
+        r1, i1, s1 = cb.sqmr_solve(handle, A, F, torch.from_numpy(B[r]).cuda(), x1, 1e-8, 1000)
+        x1 = x1.cpu().numpy()
+        assert st[r] == s1 == capi.OK
+        assert abs(int(its[r]) - i1) <= 4
+        assert np.linalg.norm(X[r] - x1) / np.linalg.norm(x1) < 1e-6
+        rel = np.linalg.norm(B[r] - K @ X[r]) / np.linalg.norm(B[r])
+        rel1 = np.linalg.norm(B[r] - K @ x1) / np.linalg.norm(B[r])
+        assert rel <= 2 * rel1 + 1e-12
+    if precision == cb.F64:
+        xo, _, ito = oracle.sqmr(rp, ci, v, B[0], _oracle_factor(rp, ci, v, bs), 1e-8, 1000)
+        assert abs(int(its[0]) - ito) <= 4
+
+
+def _oracle_factor(rp, ci, v, bs):
+    return oracle.Sym(rp, ci, bs, 0, 1.0).factor(v)
+
+
 def test_sqmr_fp32_factor_mixed(handle):
     """FP32 factor and applies, FP64 recurrence: converges on the small KKT."""
     rp, ci, v, bs = kkt("small")
