@@ -9,7 +9,8 @@ and max_it 1000 (the driver's settings, apps/block_ildlt/block_ildlt_invariants.
 The sparsity pattern's symbolic analysis is done once (as for a stream of
 IPM iterations on one pattern); a step is one numeric factorization plus one
 SQMR solve with the values resident in HBM.  L2 (126 MB) is flushed before
-every step by writing a 512 MB buffer outside the timed events.
+every step outside the timed events (a 512 MB write, then a 512 MB read that
+pushes the written lines back to HBM).
 
 `e2e` times the same step through the public C ABI with host buffers: K's
 values and b copied host -> device from pinned memory, the factor and the
@@ -47,13 +48,16 @@ def _parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="culipx", choices=["culipx", "reference"])
-    ap.add_argument("--config", default="scale", choices=["small", "scale", "batch", "served"])
+    ap.add_argument("--config", default="scale", choices=["small", "scale", "mixed", "batch", "served", "spmv"])
+    ap.add_argument("--spmv-workload", default="mixed", choices=["small", "scale", "mixed"],
+                    help="--config spmv: the KKT matrix whose product is timed")
     ap.add_argument("--rate", type=float, default=2000.0, help="--config served: arrivals per second")
     ap.add_argument("--duration", type=float, default=0.25, help="--config served: seconds of arrivals")
     ap.add_argument("--patterns", type=int, default=64, help="--config served: sparsity patterns")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--max-it", type=int, default=1000, help="SQMR iteration cap (1000 = the driver's setting)")
     ap.add_argument("--batch", type=int, default=512, help="systems in --config batch")
+    ap.add_argument("--max-refine", type=int, default=10, help="--config mixed / batch: refinement corrections")
     return ap.parse_args()
 
 
@@ -67,15 +71,35 @@ def _workload(name):
     return cfg, rp, ci, v, bs, b
 
 
-def _config_dict(name, cfg, nnz, extra=None):
+def _config_dict(name, cfg, nnz, extra=None, solve="SQMR tol 1e-8 max_it 1000, 1 RHS"):
     d = {"workload": f"KKT {name}: n={cfg['n']} m={cfg['m']} N={cfg['n'] + cfg['m']} nnz_K={nnz}, "
                      f"A {cfg['nnz_per_col']}/col (band_half={cfg['band_half']}), H log-U[{cfg['hmin']:g},{cfg['hmax']:g}], "
-                     f"blocks {cfg['block']}, BK, fill 0, SQMR tol 1e-8 max_it 1000, 1 RHS",
+                     f"blocks {cfg['block']}, BK, fill 0, {solve}",
          "pattern_reuse": "symbolic analysis once, numeric factor + solve per step",
-         "l2": "flushed before every step (512 MB write outside the timed events)"}
+         "l2": L2Flush.NOTE}
     if extra:
         d.update(extra)
     return d
+
+
+class L2Flush:
+    """Evicts L2 (126 MB) between timed steps, outside the timed events: a
+    512 MB buffer is written, then a second 512 MB buffer is read, so the
+    written lines are already back in HBM when the next step starts (a write
+    alone leaves up to 126 MB of dirty lines whose write-back would be
+    charged to the timed kernel)."""
+
+    NOTE = "flushed before every step (512 MB write + 512 MB read outside the timed events)"
+
+    def __init__(self):
+        import torch
+
+        self.w = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+        self.r = torch.ones(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def fill_(self, v):
+        self.w.fill_(v)
+        self.r.max()
 
 
 class ClockSampler:
@@ -165,7 +189,7 @@ def run_culipx(args):
     d_b = torch.from_numpy(b).cuda()
     d_x = torch.zeros(N, dtype=torch.float64, device="cuda")
     A = cb.CsrOperator(h, d_rp, d_ci, d_v)
-    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    flush = L2Flush()
 
     iters_seen = []
     sq_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
@@ -266,6 +290,7 @@ def run_culipx(args):
         "e2e": {"value": world * e2e_steps / (e2e_total / 1e3), "unit": UNIT,
                 "h2d_bytes_per_step": int(nnz * 8 + N * 8), "d2h_bytes_per_step": int(N * 8)},
         "roofline": roof,
+        "spmv": spmv_roofline(A, N, nnz, flush, stream),
     }
     if rank == 0 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(args.config, rp, ci, v, bs, b, int(np.median(iters_seen)))
@@ -275,7 +300,8 @@ def run_culipx(args):
         print(json.dumps(out), flush=True)
 
 
-def sqmr_roofline(info, N, nnz, its, launch_ms):
+def sqmr_roofline(info, N, nnz, its, launch_ms, nr=1, kernel="k_sqmr_persistent<double> (one cooperative launch per solve)",
+                  profile="sqmr_persistent_scale.txt"):
     """Algorithmic bytes of one persistent SQMR launch (init, its iterations,
     final solve) over its CUDA-event duration.  Per iteration:
       B_spmv = nnz_K (8 + 4) + 4 (N + 1) + 8 N (x) + 8 N (y)
@@ -284,27 +310,57 @@ def sqmr_roofline(info, N, nnz, its, launch_ms):
       B_D    = 3 N s + 2 * 8 N
       B_iter = B_spmv + 2 B_tri + 2 B_D + 11 * 8 N
     and the launch adds B_spmv + 4 B_tri for the initial sweeps and the final
-    x = P U^-1 D^-1 x~.  traffic: DRAM bytes per iteration from the ncu
-    summary profiles/sqmr_persistent_scale.txt, times the iterations."""
+    x = P U^-1 D^-1 x~.  With nr right-hand sides in one launch the matrix and
+    factor terms are read once and every 8 N vector term counts nr times.
+    traffic: DRAM bytes per iteration from the ncu summary under profiles/,
+    times the iterations."""
     s = info["value_bytes"]
-    b_spmv = nnz * 12 + 4 * (N + 1) + 16 * N
-    b_tri = info["u_nnz"] * (s + 4) + 4 * (N + 1) + s * info["tile_entries"] + 16 * N
-    b_d = 3 * N * s + 16 * N
-    b_iter = b_spmv + 2 * b_tri + 2 * b_d + 11 * 8 * N
+    b_spmv = nnz * 12 + 4 * (N + 1) + 16 * N * nr
+    b_tri = info["u_nnz"] * (s + 4) + 4 * (N + 1) + s * info["tile_entries"] + 16 * N * nr
+    b_d = 3 * N * s + 16 * N * nr
+    b_iter = b_spmv + 2 * b_tri + 2 * b_d + 11 * 8 * N * nr
     b_launch = its * b_iter + b_spmv + 4 * b_tri
     achieved = b_launch / (launch_ms * 1e-3) / 1e9
     peak = _peak_hbm()
     traffic = None
-    prof = os.path.join(ROOT, "profiles", "sqmr_persistent_scale.txt")
+    prof = os.path.join(ROOT, "profiles", profile)
     if os.path.exists(prof):
         for ln in open(prof):
             if ln.startswith("dram_bytes_per_iteration"):
                 traffic = float(ln.split("=")[1]) * its
-    return {"kernel": "k_sqmr_persistent<double> (one cooperative launch per solve)", "bound": "hbm",
+    return {"kernel": kernel, "bound": "hbm",
             "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
             "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
             "algorithmic_bytes": int(b_launch), "bytes_per_iteration": int(b_iter), "iterations": its,
             "avg_launch_ms": launch_ms, "us_per_iteration": launch_ms * 1e3 / max(its, 1)}
+
+
+def spmv_roofline(A, N, nnz, flush, stream, reps=20):
+    """Standalone y = K x (culipx_spmv, FP64, beta = 0) with L2 flushed before
+    every launch (outside the events): algorithmic bytes
+    B_spmv = nnz_K (8 + 4) + 4 (N + 1) + 8 N (x) + 8 N (y) over the mean
+    CUDA-event duration."""
+    import torch
+
+    x = torch.linspace(-1.0, 1.0, N, dtype=torch.float64, device="cuda")
+    y = torch.zeros(N, dtype=torch.float64, device="cuda")
+    for _ in range(3):
+        A.spmv(x, y)
+    ms = []
+    for i in range(reps):
+        flush.fill_(float(i))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        A.spmv(x, y)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    t = float(np.mean(ms))
+    b = nnz * 12 + 4 * (N + 1) + 16 * N
+    peak = _peak_hbm()
+    return {"kernel": "k_csr_spmv_rows<double> (culipx_spmv, L2 flushed before each launch)", "achieved": b / (t * 1e-3) / 1e9,
+            "peak": peak, "unit": "GB/s", "frac": b / (t * 1e-3) / 1e9 / peak, "algorithmic_bytes": int(b),
+            "avg_launch_us": t * 1e3, "launches": reps}
 
 
 def _peak_hbm():
@@ -336,9 +392,42 @@ def cpu_baseline(name, rp, ci, v, bs, b, gpu_iters, max_seconds=25.0):
                       f"{gpu_iters} iterations; symbolic {t1 - t0:.2f}s not counted (cached per pattern)"}
 
 
+def run_reference_spmv(args):
+    """The CPU restatement's y = K x (serial CSR loop, 1 thread) on the same
+    matrix; value = algorithmic GB/s as in --config spmv."""
+    import oracle
+
+    cfg, rp, ci, v, bs, _ = _workload(args.spmv_workload)
+    N, nnz = len(rp) - 1, len(ci)
+    x = np.linspace(-1.0, 1.0, N)
+    ms = []
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        oracle.spmv(rp, ci, v, x)
+        if i >= args.warmup:
+            ms.append((time.perf_counter() - t0) * 1e3)
+    t = float(np.mean(ms))
+    b = nnz * 12 + 4 * (N + 1) + 16 * N
+    gbs = b / (t * 1e-3) / 1e9
+    out = {"metric": "SpMV HBM GB/s (culipx_spmv, FP64 CSR, y = K x)", "value": gbs, "unit": "GB/s", "n_gpus": 1,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": t, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded KKT generator)", "impl": "reference",
+           "config": _config_dict(args.spmv_workload, cfg, nnz, {"parallelism": "one CPU thread"}, solve="y = K x only"),
+           "cpu_baseline": {"value": gbs, "unit": "GB/s", "cores": 1, "kind": "port",
+                            "sample": "oracle serial CSR product, whole matrix per step"},
+           "e2e": {"value": gbs, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
 def run_reference(args):
     world, rank, _ = _dist()
     if rank != 0:
+        return
+    if args.config == "spmv":
+        return run_reference_spmv(args)
+    if args.config in ("batch", "served"):
+        print(json.dumps({"impl": "reference", "unavailable": f"--config {args.config}: the reference arm times the "
+                          "single-system workloads (small, scale, mixed) and spmv only"}), flush=True)
         return
     cfg, rp, ci, v, bs, b = _workload(args.config)
     import oracle
@@ -376,6 +465,215 @@ def _reference_iterations(name):
     if os.path.exists(cache):
         return int(open(cache).read().strip())
     return 300
+
+
+def run_mixed(args):
+    """Mixed precision with several right-hand sides (n = 1e6, m = 5e5, 4
+    N(0,1) right-hand sides): FP32 factor and preconditioner applies, FP64
+    SQMR recurrence, FP64 true residual and refinement to relres 1e-10, the 4
+    right-hand sides solved together in multi-RHS launches.  A step = FP32
+    factor + the refined solve of all 4; value = right-hand sides solved per
+    second.  The error is stated against the FP64 path (FP64 factor, plain
+    SQMR on the same right-hand sides)."""
+    import torch
+
+    import culip_b200 as cb
+
+    world, rank, local = _dist()
+    torch.cuda.set_device(local)
+    nr = 4
+    cfg, rp, ci, v, bs, _ = _workload("mixed")
+    N, nnz = len(rp) - 1, len(ci)
+    Bh = np.stack([cb.normal_vector(cb.SEED + 1 + j, N) for j in range(nr)])
+    stream = torch.cuda.current_stream()
+    h = cb.Handle(local, stream)
+    P = cb.Pattern(h, rp, ci, bs, 0, 1.0, cb.F32)
+    F = cb.Factor(P)
+    d_rp = torch.from_numpy(rp).cuda()
+    d_ci = torch.from_numpy(ci).cuda()
+    d_v = torch.from_numpy(v).cuda()
+    d_v32 = d_v.float()
+    d_B = torch.from_numpy(Bh).cuda()
+    d_X = torch.zeros_like(d_B)
+    A = cb.CsrOperator(h, d_rp, d_ci, d_v)
+    flush = L2Flush()
+    tol, inner_tol, inner_it, max_ref = 1e-10, 1e-6, args.max_it, args.max_refine
+    stats = {}
+
+    def step():
+        F.compute(d_v32, None, cb.PIV_BK, 0.0)
+        rel, its, steps, st = cb.sqmr_refine_multi(h, A, F, d_B, d_X, tol, inner_tol, inner_it, max_ref)
+        stats.update(rel=rel, its=its, steps=steps, st=st)
+
+    for _ in range(args.warmup):
+        flush.fill_(1.0)
+        step()
+    torch.cuda.synchronize()
+    h.launch_count(reset=True)
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms = []
+    for i in range(args.steps):
+        flush.fill_(float(i))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    ck = clocks.stop()
+    launches = h.launch_count(reset=True)
+    total_ms = float(np.sum(ms))
+    fac_ms, _ = F.stats()
+    Xm = d_X.cpu().numpy()
+
+    # the multi-RHS launch alone, for the roofline: a fixed 200 iterations (tol 0)
+    its_roof = 200
+    R = torch.zeros_like(d_B)
+    for _ in range(2):
+        cb.sqmr_solve_multi(h, A, F, d_B, R, 0.0, its_roof)
+    flush.fill_(2.0)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    cb.sqmr_solve_multi(h, A, F, d_B, R, 0.0, its_roof)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    roof = sqmr_roofline(F.info(), N, nnz, its_roof, e0.elapsed_time(e1), nr=nr,
+                         kernel="k_sqmr_persistent<float, NR=4> (4 right-hand sides per cooperative launch)",
+                         profile="sqmr_persistent_mixed.txt")
+
+    # e2e: K's values and the 4 right-hand sides from pinned host memory, X back
+    hv = torch.from_numpy(v).pin_memory()
+    hB = torch.from_numpy(Bh).pin_memory()
+    hX = torch.empty_like(hB).pin_memory()
+    e_ms = []
+    for i in range(max(2, min(args.steps, 3))):
+        flush.fill_(float(i))
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        d_v.copy_(hv, non_blocking=True)
+        d_B.copy_(hB, non_blocking=True)
+        d_v32.copy_(d_v)
+        step()
+        hX.copy_(d_X, non_blocking=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        e_ms.append(e0.elapsed_time(e1))
+
+    # the FP64 path on the same right-hand sides: FP64 factor, plain SQMR
+    P64 = cb.Pattern(h, rp, ci, bs, 0, 1.0, cb.F64)
+    F64 = cb.Factor(P64)
+    F64.compute(d_v, None, cb.PIV_BK, 0.0)
+    X64 = torch.zeros_like(d_B)
+    _, its64, st64 = cb.sqmr_solve_multi(h, A, F64, d_B, X64, tol, args.max_it)
+    X64 = X64.cpu().numpy()
+    import scipy.sparse as sp
+
+    K = sp.csr_matrix((v, ci, rp), shape=(N, N))
+    rel_m = [float(np.linalg.norm(Bh[j] - K @ Xm[j]) / np.linalg.norm(Bh[j])) for j in range(nr)]
+    rel_64 = [float(np.linalg.norm(Bh[j] - K @ X64[j]) / np.linalg.norm(Bh[j])) for j in range(nr)]
+    err = [float(np.linalg.norm(Xm[j] - X64[j]) / max(np.linalg.norm(X64[j]), 1e-300)) for j in range(nr)]
+    out = {
+        "metric": "KKT right-hand sides solved/s (FP32 factor + FP64 refinement to relres 1e-10, 4 RHS per system)",
+        "value": nr * args.steps / (total_ms / 1e3), "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 factor / f64 recurrence and refinement",
+        "data": "synthetic (seeded KKT generator)",
+        "config": _config_dict("mixed", cfg, nnz, {
+            "solver": f"{nr} RHS in one multi-RHS SQMR launch per correction, inner tol {inner_tol:g} max_it "
+                      f"{inner_it}, FP64 refinement to {tol:g}, at most {max_ref} corrections",
+            "parallelism": "one GPU"}, solve=f"FP32 factor, {nr} N(0,1) RHS, relres 1e-10"),
+        "true_relres": rel_m, "status": [int(t) for t in stats["st"]],
+        "sqmr_iterations": [int(t) for t in stats["its"]], "corrections": [int(t) for t in stats["steps"]],
+        "fp64_path": {"true_relres": rel_64, "sqmr_iterations": [int(t) for t in its64],
+                      "status": [int(t) for t in st64]},
+        "rel_error_vs_fp64_path": err,
+        "factor_ms": fac_ms, "gpu_launches": int(launches), "clocks": ck,
+        "e2e": {"value": nr * len(e_ms) / (float(np.sum(e_ms)) / 1e3), "unit": "solves/s",
+                "h2d_bytes_per_step": int(nnz * 8 + nr * N * 8), "d2h_bytes_per_step": int(nr * N * 8)},
+        "roofline": roof,
+        "spmv": spmv_roofline(A, N, nnz, flush, stream),
+    }
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+def run_spmv(args):
+    """y = K x alone (culipx_spmv, FP64, beta = 0) on a KKT matrix: a step is
+    one product with L2 flushed before it; value = algorithmic HBM GB/s
+    (nnz_K (8 + 4) + 4 (N + 1) + 8 N + 8 N bytes per product)."""
+    import torch
+
+    import culip_b200 as cb
+
+    world, rank, local = _dist()
+    torch.cuda.set_device(local)
+    cfg, rp, ci, v, bs, _ = _workload(args.spmv_workload)
+    N, nnz = len(rp) - 1, len(ci)
+    stream = torch.cuda.current_stream()
+    h = cb.Handle(local, stream)
+    A = cb.CsrOperator(h, torch.from_numpy(rp).cuda(), torch.from_numpy(ci).cuda(), torch.from_numpy(v).cuda())
+    flush = L2Flush()
+    x = torch.linspace(-1.0, 1.0, N, dtype=torch.float64, device="cuda")
+    y = torch.zeros(N, dtype=torch.float64, device="cuda")
+    for _ in range(args.warmup):
+        flush.fill_(1.0)
+        A.spmv(x, y)
+    torch.cuda.synchronize()
+    h.launch_count(reset=True)
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms = []
+    for i in range(args.steps):
+        flush.fill_(float(i))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        A.spmv(x, y)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    ck = clocks.stop()
+    launches = h.launch_count(reset=True)
+    t = float(np.mean(ms))
+    b = nnz * 12 + 4 * (N + 1) + 16 * N
+    peak = _peak_hbm()
+    gbs = b / (t * 1e-3) / 1e9
+    # e2e: x from pinned host memory, y back
+    hx = x.cpu().pin_memory()
+    hy = torch.empty_like(hx).pin_memory()
+    e_ms = []
+    for i in range(max(3, min(args.steps, 10))):
+        flush.fill_(float(i))
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        x.copy_(hx, non_blocking=True)
+        A.spmv(x, y)
+        hy.copy_(y, non_blocking=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        e_ms.append(e0.elapsed_time(e1))
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", f"spmv_{args.spmv_workload}.txt")
+    if os.path.exists(prof):
+        for ln in open(prof):
+            if ln.startswith("dram_bytes_per_launch"):
+                traffic = float(ln.split("=")[1])
+    out = {
+        "metric": "SpMV HBM GB/s (culipx_spmv, FP64 CSR, y = K x)", "value": gbs, "unit": "GB/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded KKT generator)",
+        "config": _config_dict(args.spmv_workload, cfg, nnz, {"parallelism": "one GPU"}, solve="y = K x only"),
+        "gpu_launches": int(launches), "clocks": ck,
+        "e2e": {"value": b / (float(np.mean(e_ms)) * 1e-3) / 1e9, "unit": "GB/s", "h2d_bytes_per_step": int(8 * N),
+                "d2h_bytes_per_step": int(8 * N)},
+        "roofline": {"kernel": "k_csr_spmv_rows<double>", "bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s",
+                     "frac": gbs / peak, "traffic": traffic, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
+                     "algorithmic_bytes": int(b), "avg_launch_us": t * 1e3},
+    }
+    if rank == 0:
+        print(json.dumps(out), flush=True)
 
 
 def batch_systems(num=512, seed_base=None):
@@ -425,8 +723,8 @@ def run_batch(args):
     d_b = torch.from_numpy(b).cuda()
     d_x = torch.zeros(N, dtype=torch.float64, device="cuda")
     A = cb.CsrOperator(h, d_rp, d_ci, d_v)
-    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-    tol, inner_tol, inner_it, max_ref = 1e-8, 1e-6, args.max_it, 10
+    flush = L2Flush()
+    tol, inner_tol, inner_it, max_ref = 1e-8, 1e-6, args.max_it, args.max_refine
     stats = {}
 
     def step():
@@ -483,7 +781,7 @@ def run_batch(args):
                                f"H log-U[1e-4,1e4], blocks 32, BK, fill 0; union N={N} nnz={nnz}",
                    "solver": f"batched SQMR (one CTA per system), inner tol {inner_tol:g} max_it {inner_it}, "
                              f"FP64 refinement to {tol:g}, at most {max_ref} corrections",
-                   "l2": "flushed before every step (512 MB write outside the timed events)",
+                   "l2": L2Flush.NOTE,
                    "parallelism": "one GPU, systems as CTAs"},
         "converged_fraction": conv,
         "median_iterations": int(np.median(stats["its"])), "max_iterations": int(np.max(stats["its"])),
@@ -611,6 +909,10 @@ if __name__ == "__main__":
     a = _parse()
     if a.impl == "reference":
         run_reference(a)
+    elif a.config == "mixed":
+        run_mixed(a)
+    elif a.config == "spmv":
+        run_spmv(a)
     elif a.config == "batch":
         run_batch(a)
     elif a.config == "served":

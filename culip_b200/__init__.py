@@ -470,6 +470,21 @@ def sqmr_solve_multi(handle: Handle, A: CsrOperator, M: Factor, B, X, tol=1e-8, 
     return res, its, st
 
 
+def sqmr_refine_multi(handle: Handle, A: CsrOperator, M: Factor, B, X, tol=1e-8, inner_tol=1e-6, inner_max_it=1000,
+                      max_refine=20):
+    """sqmr_refine for several right-hand sides: B, X torch float64 CUDA
+    tensors of shape (nrhs, n).  Returns per-RHS (relres, iterations,
+    corrections, status) numpy arrays."""
+    nrhs = int(B.shape[0])
+    rel = np.zeros(nrhs)
+    its = np.zeros(nrhs, np.int32)
+    steps = np.zeros(nrhs, np.int32)
+    st = np.zeros(nrhs, np.int32)
+    capi.call("culipx_sqmr_refine_multi", handle._h, A._h, M._h, nrhs, _dptr(B), _dptr(X), float(tol),
+              float(inner_tol), int(inner_max_it), int(max_refine), _p(rel), _p(its), _p(steps), _p(st))
+    return rel, its, steps, st
+
+
 def sqmr_solve_many(handle: Handle, As, Ms, bs, xs, tol=1e-8, max_it=1000):
     """Independent systems with their own factors, one launch; per-system
     (residual, iterations, status) numpy arrays."""

@@ -82,6 +82,7 @@ _SIGS = {
     "culipx_batch_destroy": [vp],
     "culipx_batch_sqmr_solve": [vp, vp, vp, vp, vp, f64, i32, vp, vp, vp],
     "culipx_sqmr_solve_multi": [vp, vp, vp, i32, vp, vp, f64, i32, vp, vp, vp],
+    "culipx_sqmr_refine_multi": [vp, vp, vp, i32, vp, vp, f64, f64, i32, i32, vp, vp, vp, vp],
     "culipx_sqmr_solve_many": [vp, i32, vp, vp, vp, vp, f64, i32, vp, vp, vp],
     "culipx_server_create": [i32, i64, i32, i32, f64, i32, ctypes.POINTER(vp)],
     "culipx_server_destroy": [vp],

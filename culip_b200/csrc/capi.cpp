@@ -522,6 +522,18 @@ CULIPX_API int culipx_sqmr_solve_multi(culipx_handle h, culipx_csr A, culipx_fac
     GUARD_END
 }
 
+CULIPX_API int culipx_sqmr_refine_multi(culipx_handle h, culipx_csr A, culipx_factor M, int nrhs, const double* d_B,
+                                        double* d_X, double tol, double inner_tol, int inner_max_it, int max_refine,
+                                        double* h_relres, int* h_iterations, int* h_steps, int* h_status)
+{
+    if (!h) return fail(CULIPX_INVALID_ARG, "null handle");
+    GUARD_BEGIN
+    CULIPX_TRY(use_device(h));
+    return sqmr_refine_multi(h, A, M, nrhs, d_B, d_X, tol, inner_tol, inner_max_it, max_refine, h_relres,
+                             h_iterations, h_steps, h_status, h->sqmr);
+    GUARD_END
+}
+
 CULIPX_API int culipx_sqmr_solve_many(culipx_handle h, int num, const culipx_csr* A, const culipx_factor* M,
                                       const double* const* d_b, double* const* d_x, double tol, int max_it,
                                       double* h_residual, int* h_iterations, int* h_status)

@@ -227,4 +227,82 @@ int sqmr_refine(culipx_handle_t* h, Csr* A, Factor* M, const double* b, double* 
     return converged ? CULIPX_OK : CULIPX_MAXIT;
 }
 
+// The same loop for several right-hand sides (column-major n x nrhs): per
+// column its own residual, step count and stopping test; each step solves the
+// corrections of the columns still above tol together (sqmr_solve_multi, up
+// to four per launch, every launch reading the factor and K once for all).
+int sqmr_refine_multi(culipx_handle_t* h, Csr* A, Factor* M, int nrhs, const double* B, double* X, double tol,
+                      double inner_tol, int inner_max_it, int max_refine, double* h_relres, int* h_its, int* h_steps,
+                      int* h_status, Sqmr* w)
+{
+    if (!A || !M || !B || !X || !w || nrhs < 1) return fail(CULIPX_INVALID_ARG, "culipx_sqmr_refine_multi: bad argument");
+    if (A->precision != CULIPX_F64 || A->m != A->n)
+        return fail(CULIPX_INVALID_ARG, "culipx_sqmr_refine_multi: A must be square FP64");
+    if (!M->computed || M->pat->n != A->m)
+        return fail(CULIPX_INVALID_ARG, "culipx_sqmr_refine_multi: preconditioner not computed or wrong size");
+    if (!(tol >= 0.0) || !(inner_tol >= 0.0) || inner_max_it < 0 || max_refine < 0)
+        return fail(CULIPX_INVALID_ARG, "culipx_sqmr_refine_multi: bad tolerance or limit");
+    const size_t n = A->m;
+    cudaStream_t s = h->stream;
+    const size_t vb = n * sizeof(double);
+    if (w->ref_r.bytes() < vb * nrhs + 16) CULIPX_TRY(w->ref_r.alloc(h, vb * nrhs + 16));
+    if (w->ref_d.bytes() < vb * nrhs + 16) CULIPX_TRY(w->ref_d.alloc(h, vb * nrhs + 16));
+    if (w->ref_part.bytes() < kRGrid * sizeof(double)) CULIPX_TRY(w->ref_part.alloc(h, kRGrid * sizeof(double)));
+    double* R = w->ref_r.as<double>();  // residuals of the active columns, packed in column order
+    double* D = w->ref_d.as<double>();  // their corrections
+    double* part = w->ref_part.as<double>();
+    std::vector<double> part_h(kRGrid), nb(nrhs), rel(nrhs);
+    std::vector<int> its(nrhs, 0), steps(nrhs, 0), st(nrhs, CULIPX_OK), it_k(nrhs), st_k(nrhs);
+    std::vector<int> act, pos(nrhs, -1);  // pos[j]: column of R holding column j's residual
+
+    CULIPX_CUDA(cudaMemsetAsync(X, 0, vb * nrhs, s));
+    for (int j = 0; j < nrhs; ++j) {
+        CULIPX_TRY(norm2(B + j * n, (int)n, part, part_h.data(), s, h, &nb[j]));
+        rel[j] = nb[j] > 0.0 ? 1.0 : 0.0;
+        // x = 0: the first residual is b
+        CULIPX_CUDA(cudaMemcpyAsync(R + j * n, B + j * n, vb, cudaMemcpyDeviceToDevice, s));
+        pos[j] = j;
+    }
+    for (int step = 0; step < max_refine; ++step) {
+        act.clear();
+        for (int j = 0; j < nrhs; ++j)
+            if (rel[j] > tol && st[j] != CULIPX_BREAKDOWN) act.push_back(j);
+        if (act.empty()) break;
+        // pack: positions only move left, so copying in increasing order is safe
+        for (int a = 0; a < (int)act.size(); ++a) {
+            const int j = act[a];
+            if (pos[j] != a)
+                CULIPX_CUDA(cudaMemcpyAsync(R + a * n, R + pos[j] * n, vb, cudaMemcpyDeviceToDevice, s));
+            pos[j] = a;
+        }
+        const int na = (int)act.size();
+        CULIPX_TRY(sqmr_solve_multi(h, A, M, na, R, D, inner_tol, inner_max_it, nullptr, it_k.data(), st_k.data(), w));
+        for (int a = 0; a < na; ++a) {
+            const int j = act[a];
+            double* x = X + j * n;
+            double* r = R + a * n;
+            k_add<<<kRGrid, kRT, 0, s>>>(x, D + a * n, (int)n);
+            h->launches += 1;
+            CULIPX_TRY(launch_check("k_add"));
+            CULIPX_CUDA(cudaMemcpyAsync(r, B + j * n, vb, cudaMemcpyDeviceToDevice, s));
+            CULIPX_TRY(csr_spmv(A, x, r, -1.0, 1.0, 0, s));
+            h->launches += 1;
+            double nr = 0.0;
+            CULIPX_TRY(norm2(r, (int)n, part, part_h.data(), s, h, &nr));
+            its[j] += it_k[a];
+            steps[j] += 1;
+            rel[j] = nr / nb[j];
+            if (st_k[a] == CULIPX_BREAKDOWN || !std::isfinite(rel[j])) st[j] = CULIPX_BREAKDOWN;
+        }
+    }
+    for (int j = 0; j < nrhs; ++j) {
+        if (st[j] != CULIPX_BREAKDOWN) st[j] = rel[j] <= tol ? CULIPX_OK : CULIPX_MAXIT;
+        if (h_relres) h_relres[j] = rel[j];
+        if (h_its) h_its[j] = its[j];
+        if (h_steps) h_steps[j] = steps[j];
+        if (h_status) h_status[j] = st[j];
+    }
+    return CULIPX_OK;
+}
+
 }  // namespace culipx

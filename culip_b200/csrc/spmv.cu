@@ -2,10 +2,17 @@
 //
 // Replaces CSRMatrixSPMV<T>::multiply -> T_csrmv -> legacy cusparse{S,D}csrmv
 // (libs/la/spmv.impl.cuh:78-113, libs/la/sparse_la_instances.cu:129-217).
-// Sub-warp vector kernel: a group of L lanes (L = 4..32, picked from the
-// average row length) owns a row, streams its column indices and values
-// with coalesced read-only loads, gathers x, and reduces with a fixed
-// shfl_xor tree, so results are bit-reproducible run to run.  The transpose
+//
+// Short rows (average up to 16 nonzeros, the KKT case): a thread owns a
+// row and sums it in column order (acc = fma(v, x, acc) from 0, the order of
+// a serial CSR loop, so the result is bit-identical to it), loading its
+// entries in batches of 8 with all 8 x gathers in flight before the fmas.
+// Rows of more than 64 nonzeros are summed by their whole warp instead
+// (lane-strided partial sums, fixed shfl_xor tree).  Measured on B200 this
+// beats shared-memory staging of the rows' range (warp-wide or through TMA
+// bulk copies): the kernel is bound by the L1TEX pipe, not by DRAM.
+// Longer rows: a group of L lanes (L = 16 or 32) owns a row and reduces with a fixed
+// shfl_xor tree (bit-reproducible run to run).  The transpose
 // product uses an explicit transposed copy, as CSRMatrixSPMV does when
 // explicit_At is set (spmv.impl.cuh:34-41).
 #include "spmv.h"
@@ -42,6 +49,57 @@ __global__ void __launch_bounds__(256) k_csr_spmv(int m, const int* __restrict__
     }
 }
 
+// rows up to kLongRow nonzeros: one thread, entries in batches of 8 (all 8
+// x gathers issued before the 8 fmas); longer rows: the whole warp
+constexpr int kLongRow = 64;
+constexpr int kGatherBatch = 8;
+
+template <class T>
+__global__ void __launch_bounds__(256) k_csr_spmv_rows(int m, const int* __restrict__ rowptr,
+                                                       const int* __restrict__ colidx, const T* __restrict__ val,
+                                                       const T* __restrict__ x, T* __restrict__ y, T alpha, T beta)
+{
+    const int row = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = lane_id();
+    int rs = 0, re = 0;
+    if (row < m) {
+        rs = __ldg(rowptr + row);
+        re = __ldg(rowptr + row + 1);
+    }
+    const bool lng = re - rs > kLongRow;
+    T acc = T(0);
+    if (!lng) {
+        for (int kb = rs; kb < re; kb += kGatherBatch) {
+            T v[kGatherBatch], xv[kGatherBatch];
+            int c[kGatherBatch];
+#pragma unroll
+            for (int j = 0; j < kGatherBatch; ++j) {
+                const bool ok = kb + j < re;
+                c[j] = ok ? __ldg(colidx + kb + j) : -1;
+                v[j] = ok ? __ldg(val + kb + j) : T(0);
+            }
+#pragma unroll
+            for (int j = 0; j < kGatherBatch; ++j) xv[j] = (c[j] >= 0) ? __ldg(x + c[j]) : T(0);
+#pragma unroll
+            for (int j = 0; j < kGatherBatch; ++j)
+                if (c[j] >= 0) acc = fma_rn(v[j], xv[j], acc);
+        }
+    }
+    // long rows of this warp, one at a time with all lanes (fixed shfl_xor tree)
+    unsigned todo = __ballot_sync(0xffffffffu, lng);
+    while (todo) {
+        const int src = __ffs(todo) - 1;
+        todo &= todo - 1;
+        const int a = __shfl_sync(0xffffffffu, rs, src), e = __shfl_sync(0xffffffffu, re, src);
+        T part = T(0);
+        for (int k = a + lane; k < e; k += 32) part = fma_rn(__ldg(val + k), __ldg(x + __ldg(colidx + k)), part);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+        if (lane == src) acc = part;
+    }
+    if (row < m) y[row] = (beta == T(0)) ? alpha * acc : fma_rn(alpha, acc, beta * y[row]);
+}
+
 template <class T>
 int launch(const int* rowptr, const int* colidx, const void* val, int m, double avg, const void* x, void* y,
            double alpha, double beta, cudaStream_t s)
@@ -49,15 +107,19 @@ int launch(const int* rowptr, const int* colidx, const void* val, int m, double 
     const T* v = static_cast<const T*>(val);
     const T* xx = static_cast<const T*>(x);
     T* yy = static_cast<T*>(y);
-    auto grid = [&](int L) {
-        const long long warps = ((long long)m * L + 31) / 32;
-        const long long blocks = (warps + 7) / 8;
-        return (int)std::min<long long>(std::max<long long>(blocks, 1), 148LL * 16);
-    };
-    if (avg <= 4.5) k_csr_spmv<T, 4><<<grid(4), 256, 0, s>>>(m, rowptr, colidx, v, xx, yy, (T)alpha, (T)beta);
-    else if (avg <= 12.0) k_csr_spmv<T, 8><<<grid(8), 256, 0, s>>>(m, rowptr, colidx, v, xx, yy, (T)alpha, (T)beta);
-    else if (avg <= 24.0) k_csr_spmv<T, 16><<<grid(16), 256, 0, s>>>(m, rowptr, colidx, v, xx, yy, (T)alpha, (T)beta);
-    else k_csr_spmv<T, 32><<<grid(32), 256, 0, s>>>(m, rowptr, colidx, v, xx, yy, (T)alpha, (T)beta);
+    if (avg <= 16.0) {
+        k_csr_spmv_rows<T><<<(m + 255) / 256, 256, 0, s>>>(m, rowptr, colidx, v, xx, yy, (T)alpha, (T)beta);
+    } else {
+        // 8 warps per block, 32 / L rows per warp
+        auto grid = [&](int L) {
+            const long long blocks = ((long long)m * L + 255) / 256;
+            return (int)std::min<long long>(blocks, 148LL * 16);
+        };
+        if (avg <= 24.0)
+            k_csr_spmv<T, 16><<<grid(16), 256, 0, s>>>(m, rowptr, colidx, v, xx, yy, (T)alpha, (T)beta);
+        else
+            k_csr_spmv<T, 32><<<grid(32), 256, 0, s>>>(m, rowptr, colidx, v, xx, yy, (T)alpha, (T)beta);
+    }
     return launch_check("k_csr_spmv");
 }
 

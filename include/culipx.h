@@ -263,6 +263,16 @@ int culipx_sqmr_solve_multi(culipx_handle h, culipx_csr A, culipx_factor M, int 
                             double *d_X, double tol, int max_it, double *h_residual, int *h_iterations,
                             int *h_status);
 
+/* culipx_sqmr_refine for several right-hand sides (d_B, d_X n x nrhs
+ * column-major): per right-hand side its own true residual, corrections and
+ * stopping test; every step solves the corrections of the right-hand sides
+ * still above tol together (culipx_sqmr_solve_multi).  Per right-hand side:
+ * relres = ||b - K x|| / ||b||, SQMR iterations summed, corrections, status
+ * (OK, MAXIT, BREAKDOWN); any output array may be NULL. */
+int culipx_sqmr_refine_multi(culipx_handle h, culipx_csr A, culipx_factor M, int nrhs, const double *d_B,
+                             double *d_X, double tol, double inner_tol, int inner_max_it, int max_refine,
+                             double *h_relres, int *h_iterations, int *h_steps, int *h_status);
+
 /* Many independent systems, each with its own pattern, factor, matrix and
  * vectors (no union), solved in one launch, one CTA per system; all factors
  * of one call share a precision.  Same per-system outputs as

@@ -99,6 +99,52 @@ def test_spmv(handle, transpose):
     assert np.allclose(yg.cpu().numpy(), ref, rtol=1e-13, atol=1e-13)
 
 
+def _rows_matrix(lengths, n_cols, seed):
+    rng = np.random.default_rng(seed)
+    rp = np.concatenate([[0], np.cumsum(lengths)]).astype(np.int32)
+    ci = np.concatenate([np.sort(rng.choice(n_cols, k, replace=False)) for k in lengths] + [np.zeros(0)]).astype(np.int32)
+    return rp, ci, rng.standard_normal(int(rp[-1]))
+
+
+@pytest.mark.parametrize("case", ["kkt_small", "kkt_scale_rows", "ragged_empty", "rows_to_64", "long_row", "wide_rows"])
+def test_spmv_bit_exact(handle, case):
+    """y = alpha K x + beta y against the serial CSR loop: bit for bit where
+    every row has at most 64 nonzeros and the average is at most 16 (a thread
+    sums its row in column order), within rounding otherwise (warp-parallel
+    sums of the long rows)."""
+    if case == "kkt_small":
+        rp, ci, v, _ = kkt("small")
+    elif case == "kkt_scale_rows":
+        rp, ci, v = cb.kkt_generate(20000, 10000, 6, 32, 1e-6, 1e6, seed=11)
+    elif case == "ragged_empty":  # 1000 rows (not a multiple of the block), a third empty
+        rng = np.random.default_rng(4)
+        rp, ci, v = _rows_matrix(rng.integers(0, 3, 1000) * rng.integers(0, 12, 1000), 1000, 5)
+    elif case == "rows_to_64":  # short rows and rows of exactly 64
+        lengths = np.full(2000, 6)
+        lengths[::97] = 64
+        rp, ci, v = _rows_matrix(lengths, 2000, 3)
+    elif case == "long_row":  # one row summed by its warp
+        lengths = np.full(3000, 5)
+        lengths[1234] = 2900
+        rp, ci, v = _rows_matrix(lengths, 3000, 6)
+    else:
+        rp, ci, v = _rows_matrix(np.full(700, 40), 3000, 7)
+    m = len(rp) - 1
+    n_cols = int(ci.max()) + 1 if len(ci) else 1
+    x = cb.normal_vector(8, max(n_cols, m))
+    y0 = cb.normal_vector(9, m)
+    A = cb.CsrOperator(handle, torch.from_numpy(rp).cuda(), torch.from_numpy(ci).cuda(), torch.from_numpy(v).cuda(),
+                       ncols=len(x))
+    for alpha, beta in ((1.0, 0.0), (-1.0, 1.0), (0.5, -2.0)):
+        yg = torch.from_numpy(y0.copy()).cuda()
+        A.spmv(torch.from_numpy(x).cuda(), yg, alpha, beta)
+        ref = oracle.spmv(rp, ci, v, x, alpha, beta, y0)
+        if case in ("wide_rows", "long_row"):
+            assert np.allclose(yg.cpu().numpy(), ref, rtol=1e-13, atol=1e-13)
+        else:
+            assert np.array_equal(yg.cpu().numpy(), ref)
+
+
 def test_sqmr_small_kkt(handle):
     rp, ci, v, bs = kkt("small")
     S, OF, P, F = _factor_both(handle, rp, ci, v, bs)
@@ -202,6 +248,34 @@ def test_sqmr_multi_rhs(handle, precision, nrhs):
     if precision == cb.F64:
         xo, _, ito = oracle.sqmr(rp, ci, v, B[0], _oracle_factor(rp, ci, v, bs), 1e-8, 1000)
         assert abs(int(its[0]) - ito) <= 4
+
+
+@pytest.mark.parametrize("nrhs", [1, 3, 5])
+def test_sqmr_refine_multi(handle, nrhs):
+    """FP32 factor, FP64 refinement, several right-hand sides: every column
+    reaches the tolerance in about the corrections its single refinement
+    takes, and columns of very different scale stop independently."""
+    rp, ci, v, bs = kkt("small")
+    n = len(rp) - 1
+    P = cb.Pattern(handle, rp, ci, bs, 0, 1.0, cb.F32)
+    F = cb.Factor(P)
+    F.compute(torch.from_numpy(v.astype(np.float32)).cuda())
+    A = _csr_op(handle, rp, ci, v)
+    rng = np.random.default_rng(5 + nrhs)
+    B = rng.standard_normal((nrhs, n)) * (10.0 ** np.arange(nrhs))[:, None]
+    X = torch.zeros((nrhs, n), dtype=torch.float64, device="cuda")
+    rel, its, steps, st = cb.sqmr_refine_multi(handle, A, F, torch.from_numpy(B).cuda(), X, 1e-10, 1e-6, 1000, 20)
+    import scipy.sparse as sp
+
+    K = sp.csr_matrix((v, ci, rp))
+    X = X.cpu().numpy()
+    for r in range(nrhs):
+        assert st[r] == capi.OK and rel[r] <= 1e-10
+        true = np.linalg.norm(B[r] - K @ X[r]) / np.linalg.norm(B[r])
+        assert abs(true - rel[r]) <= 1e-3 * rel[r] + 1e-15
+        x1 = torch.zeros(n, dtype=torch.float64, device="cuda")
+        r1, i1, s1, st1 = cb.sqmr_refine(handle, A, F, torch.from_numpy(B[r]).cuda(), x1, 1e-10, 1e-6, 1000, 20)
+        assert st1 == capi.OK and abs(int(steps[r]) - s1) <= 1
 
 
 def _oracle_factor(rp, ci, v, bs):
