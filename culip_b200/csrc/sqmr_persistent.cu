@@ -445,11 +445,17 @@ __device__ __forceinline__ void u_item(const PArgs<TF>& a, int I, int fr, int h,
     }
 }
 
-// One U'-sweep work item.  The lane's right-hand sides are, with SPMV,
-// sc[r] * (K src)[perm[row]] (src interleaved), else b[r n + perm[row]] of the
-// caller's column-major right-hand sides; dst[row] = U_II'^-1 (rhs - U'_I*
-// dst) (interleaved).  t receives the lane's results (0 for lanes >= h).
-template <class TF, int NR, bool SPMV>
+// Where a U'-sweep item's right-hand side comes from
+enum RhsFrom {
+    kRhsCaller = 0,  // b[r n + perm[row]] of the caller's column-major right-hand sides
+    kRhsSpmv = 1,    // sc[r] * (K src)[perm[row]], src interleaved
+    kRhsPre = 2,     // dst[perm[row]]: sc (K src) stored there by an earlier phase
+};
+
+// One U'-sweep work item: dst[row] = U_II'^-1 (rhs - U'_I* dst) (interleaved)
+// with the lane's right-hand sides taken as FROM says.  t receives the
+// lane's results (0 for lanes >= h).
+template <class TF, int NR, int FROM>
 __device__ __forceinline__ void ut_item(const PArgs<TF>& a, int I, int fr, int h, int flags, const double* src,
                                         const double (&sc)[NR], double* dst, double (&t)[NR])
 {
@@ -459,10 +465,13 @@ __device__ __forceinline__ void ut_item(const PArgs<TF>& a, int I, int fr, int h
     if (lane < h) {
         const int q = (flags & kRowPermIdentity) ? fr + lane : __ldg(a.perm + fr + lane);
         double y[NR];
-        if (SPMV) {
+        if (FROM == kRhsSpmv) {
             spmv_row<TF, NR>(a, q, src, y);
 #pragma unroll
             for (int r = 0; r < NR; ++r) y[r] *= sc[r];
+        } else if (FROM == kRhsPre) {
+#pragma unroll
+            for (int r = 0; r < NR; ++r) y[r] = dst[(size_t)q * NR + r];
         } else {
 #pragma unroll
             for (int r = 0; r < NR; ++r) y[r] = src[(size_t)r * a.n + q];
@@ -474,6 +483,8 @@ __device__ __forceinline__ void ut_item(const PArgs<TF>& a, int I, int fr, int h
 #pragma unroll
         for (int r = 0; r < NR; ++r) t[r] = (double)acc[r];
     }
+    // with kRhsPre the lanes read dst inside this block row: all reads before any write
+    if (FROM == kRhsPre) __syncwarp();
     if (!(flags & kRowIdentity)) tile_lower<TF, NR>(t, a.pk_row + __ldg(a.pk_off + I), h, __ldg(a.ndmask + I));
     if (lane < h)
 #pragma unroll
@@ -627,7 +638,7 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal 
                 const int I = __ldg(a.lvl_rows + r0 + t);
                 const int fr = __ldg(a.bs + I), h = __ldg(a.bs + I + 1) - fr;
                 double tt[NR];
-                ut_item<TF, NR, false>(a, I, fr, h, __ldg(a.rowflags + I), a.b, one, a.v[0], tt);
+                ut_item<TF, NR, kRhsCaller>(a, I, fr, h, __ldg(a.rowflags + I), a.b, one, a.v[0], tt);
             }
             ctx.sync();
         }
@@ -696,7 +707,7 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal 
                 const int fr = __ldg(a.bs + I), h = __ldg(a.bs + I + 1) - fr;
                 const int flags = __ldg(a.rowflags + I);
                 double av[NR];
-                ut_item<TF, NR, true>(a, I, fr, h, flags, a.ev, one, a.Av, av);
+                ut_item<TF, NR, kRhsSpmv>(a, I, fr, h, flags, a.ev, one, a.Av, av);
                 DBlock<TF> D;
                 D.load(a, fr, h, flags);
 #pragma unroll
@@ -855,7 +866,8 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal 
                     const int fr = __ldg(a.bs + I), h = __ldg(a.bs + I + 1) - fr;
                     const int flags = __ldg(a.rowflags + I);
                     double av[NR];
-                    ut_item<TF, NR, true>(a, I, fr, h, flags, a.ev, cf.sc, a.Av, av);
+                    if (L == 0) ut_item<TF, NR, kRhsSpmv>(a, I, fr, h, flags, a.ev, cf.sc, a.Av, av);
+                    else ut_item<TF, NR, kRhsPre>(a, I, fr, h, flags, a.ev, cf.sc, a.Av, av);
                     DBlock<TF> D;
                     D.load(a, fr, h, flags);
 #pragma unroll
@@ -890,9 +902,39 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal 
                 // update wait for the next level's phase, whose threads are
                 // mostly free (the last level does them at once)
                 const bool last = (L == a.nl - 1);
-                const int s1 = __ldg(a.scan_s + q1);
-                for (int i = __ldg(a.scan_s + q0) + ctx.g0; i < s1; i += ctx.gstride) {
-                    const int g = __ldg(a.simple_rows + i);
+                const int s0 = __ldg(a.scan_s + q0), s1 = __ldg(a.scan_s + q1);
+                // Level 0 also computes (K ev) / delta for the rows of the later
+                // levels' pivot-tile block rows and leaves it in Av at those rows:
+                // their items read it there instead of running the product on
+                // the critical path of a level of few, long items.  Units
+                // [0, npre) are those rows (lane ln of item t), the rest this
+                // level's simple rows, both spread over all threads.
+                long long npre = 0;
+                if (L == 0)
+                    for (int L2 = 1; L2 < a.nl; ++L2)
+                        npre += 32LL * (__ldg(a.scan_c + __ldg(sv.qe + L2)) - __ldg(a.scan_c + __ldg(sv.qb + L2)));
+                const long long nunits = npre + (s1 - s0);
+                for (long long k = ctx.g0; k < nunits; k += ctx.gstride) {
+                    if (k < npre) {
+                        long long u = k;
+                        int L2 = 1;
+                        for (;; ++L2) {
+                            const long long len =
+                                32LL * (__ldg(a.scan_c + __ldg(sv.qe + L2)) - __ldg(a.scan_c + __ldg(sv.qb + L2)));
+                            if (u < len) break;
+                            u -= len;
+                        }
+                        const int I = __ldg(a.cplx + __ldg(a.scan_c + __ldg(sv.qb + L2)) + (int)(u >> 5));
+                        const int ln = (int)(u & 31), fr = __ldg(a.bs + I);
+                        if (ln < __ldg(a.bs + I + 1) - fr) {
+                            double y[NR];
+                            spmv_row<TF, NR>(a, fr + ln, a.ev, y);
+#pragma unroll
+                            for (int j = 0; j < NR; ++j) a.Av[(size_t)(fr + ln) * NR + j] = y[j] * cf.sc[j];
+                        }
+                        continue;
+                    }
+                    const int g = __ldg(a.simple_rows + s0 + (int)(k - npre));
                     double y[NR];
                     spmv_row<TF, NR>(a, g, a.ev, y);
                     TF acc[NR];
