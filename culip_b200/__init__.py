@@ -447,8 +447,12 @@ class Server:
     def stats(self) -> dict:
         v = np.zeros(8, np.int64)
         capi.call("culipx_server_stats", self._h, _p(v))
-        keys = ["queued", "running", "done", "batches", "running_bytes", "held_bytes", "patterns"]
+        keys = ["queued", "running", "done", "batches", "running_bytes", "held_bytes", "patterns", "large_batches"]
         return {k: int(x) for k, x in zip(keys, v)}
+
+    def set_large_rows(self, rows: int):
+        """Patterns with n >= rows are solved by the whole-GPU solver."""
+        capi.call("culipx_server_set_large_rows", self._h, int(rows))
 
     def __del__(self):
         try:

@@ -11,11 +11,18 @@
 //     admission and release never synchronize the device);
 //   * runs admitted requests as a batch on one of several slots, each with
 //     its own stream and workspace: per request the values' upload and the
-//     numeric factor, then ONE launch solving every (request, right-hand
-//     side) pair, one CTA each (k_sqmr_many); results come back through
-//     pinned buffers;
-//   * keeps up to `slots` batches in flight, so requests that arrive while
-//     others run are admitted into the next slot and overlap on the device.
+//     numeric factor, then the solves; results come back through pinned
+//     buffers.  A batch holds requests of one class, in arrival order:
+//       - small patterns (n < large_rows): ONE launch solving every
+//         (request, right-hand side) pair, one CTA each (k_sqmr_many);
+//       - large patterns: per request the whole-GPU cooperative solver,
+//         its right-hand sides in groups of up to 4 per launch (one CTA per
+//         system would leave a large system to a single SM for its whole
+//         solve).  A large batch runs alone on the device: it starts when no
+//         other batch runs, and none starts beside it;
+//   * keeps up to `slots` small batches in flight, so requests that arrive
+//     while others run are admitted into the next slot and overlap on the
+//     device.
 // Latency is measured from submit to the progress() call that sees the
 // batch's completion event.
 #include "server.h"
@@ -185,7 +192,18 @@ long long Server::fixed_bytes() const
     return t;
 }
 
+int server_set_large_rows(Server* s, int rows)
+{
+    if (!s || rows < 1) return fail(CULIPX_INVALID_ARG, "culipx_server_set_large_rows: bad argument");
+    s->large_rows = rows;
+    return CULIPX_OK;
+}
+
 namespace {
+
+// requests per large batch: large batches are exclusive, so small requests
+// queued behind them get the device back after a few
+constexpr int kLargeBatch = 4;
 
 int finish_slot(Server* s, ServerSlot& sl)
 {
@@ -214,16 +232,25 @@ int finish_slot(Server* s, ServerSlot& sl)
     }
     sl.reqs.clear();
     sl.busy = false;
+    sl.large = false;
     return CULIPX_OK;
 }
 
 int launch_slot(Server* s, ServerSlot& sl)
 {
     cudaStream_t st = sl.h->stream;
-    // admit in arrival order while the budget allows
+    if (s->queue.empty()) return CULIPX_OK;
+    for (const auto& o : s->slots)
+        if (o.busy && o.large) return CULIPX_OK;  // a large batch has the device
+    auto is_large = [&](int id) { return s->patterns[s->requests.at(id).pid].n >= s->large_rows; };
+    const bool large = is_large(s->queue.front());
+    if (large && s->running_slots() > 0) return CULIPX_OK;  // wait until the device is idle
+    const int cap = large ? std::min(s->max_batch, kLargeBatch) : s->max_batch;
+    // admit in arrival order, one class per batch, while the budget allows
     std::vector<int> admit;
     int systems = 0;
-    while (!s->queue.empty() && (int)admit.size() < s->max_batch) {
+    while (!s->queue.empty() && (int)admit.size() < cap) {
+        if (is_large(s->queue.front()) != large) break;
         ServerRequest& r = s->requests.at(s->queue.front());
         const ServerPattern& sp = s->patterns[r.pid];
         const long long need = request_bytes(sp, r.nrhs);
@@ -300,7 +327,22 @@ int launch_slot(Server* s, ServerSlot& sl)
         A.precision = CULIPX_F64;
         r.state = 1;
     }
-    for (size_t q = 0; q < admit.size(); ++q) {
+    if (large) {
+        // whole-GPU solves, request after request on this stream; results in
+        // request order
+        int k = 0;
+        for (size_t q = 0; q < admit.size(); ++q) {
+            ServerRequest& r = s->requests.at(admit[q]);
+            CULIPX_TRY(sqmr_solve_multi_async(sl.h, &sl.csrs[q], r.F, r.nrhs, static_cast<const double*>(r.d_b),
+                                              static_cast<double*>(r.d_x), s->tol, s->max_it, sl.h->sqmr,
+                                              sl.out_host + (size_t)k * 8));
+            k += r.nrhs;
+        }
+        sl.order.resize(k);
+        for (int i = 0; i < k; ++i) sl.order[i] = i;
+        ++s->large_batches;
+    }
+    for (size_t q = 0; q < admit.size() && !large; ++q) {
         ServerRequest& r = s->requests.at(admit[q]);
         const int n = s->patterns[r.pid].n;
         for (int k = 0; k < r.nrhs; ++k) {
@@ -315,7 +357,7 @@ int launch_slot(Server* s, ServerSlot& sl)
     for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return Ms[a]->precision < Ms[b]->precision; });
     size_t g0 = 0;
-    while (g0 < order.size()) {
+    while (!large && g0 < order.size()) {
         size_t g1 = g0;
         while (g1 < order.size() && Ms[order[g1]]->precision == Ms[order[g0]]->precision) ++g1;
         std::vector<Csr*> a;
@@ -333,7 +375,7 @@ int launch_slot(Server* s, ServerSlot& sl)
         g0 = g1;
     }
     // the groups' results were written in sorted order; keep the permutation to undo it
-    sl.order = order;
+    if (!large) sl.order = order;
     size_t xo = 0;
     for (int id : admit) {
         ServerRequest& r = s->requests.at(id);
@@ -349,6 +391,7 @@ int launch_slot(Server* s, ServerSlot& sl)
     CULIPX_CUDA(cudaEventRecord(sl.done, st));
     sl.reqs = admit;
     sl.busy = true;
+    sl.large = large;
     ++s->batches;
     return CULIPX_OK;
 }
@@ -443,7 +486,7 @@ int server_stats(Server* s, long long* st8)
     st8[4] = s->in_use;
     st8[5] = s->fixed_bytes();
     st8[6] = (long long)s->patterns.size();
-    st8[7] = 0;
+    st8[7] = s->large_batches;
     return CULIPX_OK;
 }
 

@@ -41,6 +41,7 @@ struct ServerSlot {
     culipx_handle_t* h = nullptr;          // own stream and SQMR workspace
     cudaEvent_t done = nullptr;
     bool busy = false;
+    bool large = false;                    // the running batch is of whole-GPU solves
     std::vector<int> reqs;
     std::vector<Csr> csrs;
     std::vector<int> order;                // precision-group order of the systems
@@ -54,6 +55,8 @@ struct Server {
     int device = 0;
     long long budget = 0, in_use = 0;
     int max_batch = 0, max_it = 0;
+    int large_rows = 32768;                // patterns with n >= this get the whole-GPU solver
+    long long large_batches = 0;
     double tol = 0.0;
     culipx_handle_t* base = nullptr;       // owns the patterns' device mirrors
     std::vector<ServerPattern> patterns;
@@ -75,6 +78,7 @@ int server_progress(Server* s, int wait, int* completed);
 int server_result(Server* s, int id, double* x, int* its, int* status, double* latency_ms);
 int server_release(Server* s, int id);
 int server_stats(Server* s, long long* st8);
+int server_set_large_rows(Server* s, int rows);
 int factor_compute(Factor* f, const void* d_vals, const int* h_is_piv, int pivot, double threshold);
 int factor_create(Pattern* p, Factor** out);
 

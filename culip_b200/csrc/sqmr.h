@@ -55,6 +55,8 @@ void many_results(int num, int max_it, const double* out, double* h_res, int* h_
 
 int sqmr_solve_multi(culipx_handle_t* h, Csr* A, Factor* M, int nrhs, const double* B, double* X, double tol,
                      int max_it, double* h_res, int* h_its, int* h_status, Sqmr* w);
+int sqmr_solve_multi_async(culipx_handle_t* h, Csr* A, Factor* M, int nrhs, const double* B, double* X, double tol,
+                           int max_it, Sqmr* w, double* out_host);
 
 int sqmr_refine_multi(culipx_handle_t* h, Csr* A, Factor* M, int nrhs, const double* B, double* X, double tol,
                       double inner_tol, int inner_max_it, int max_refine, double* h_relres, int* h_its, int* h_steps,

@@ -1201,7 +1201,7 @@ int persistent_grid(int dev, int* G)
 
 // launch and wait; out_host receives 8 values per right-hand side
 template <class TF, int NR>
-int run_persistent(culipx_handle_t* h, PArgs<TF>& a, int G, double* out_host)
+int run_persistent(culipx_handle_t* h, PArgs<TF>& a, int G, double* out_host, bool wait = true)
 {
     cudaStream_t s = h->stream;
     // the recurrence vectors start at zero; x is zeroed as in the reference
@@ -1211,13 +1211,13 @@ int run_persistent(culipx_handle_t* h, PArgs<TF>& a, int G, double* out_host)
     CULIPX_CUDA(cudaLaunchCooperativeKernel(persistent_kernel<TF, NR>(), dim3(G), dim3(kT), args, 0, s));
     h->launches += 1;
     CULIPX_CUDA(cudaMemcpyAsync(out_host, a.out, (size_t)8 * NR * sizeof(double), cudaMemcpyDeviceToHost, s));
-    CULIPX_CUDA(cudaStreamSynchronize(s));
+    if (wait) CULIPX_CUDA(cudaStreamSynchronize(s));
     return CULIPX_OK;
 }
 
 template <class TF, int NR>
 int launch_persistent(culipx_handle_t* h, Csr* A, Factor* M, const double* b, double* x, double tol, int max_it,
-                      Sqmr* w, double* out_host)
+                      Sqmr* w, double* out_host, bool wait = true)
 {
     const int n = A->m;
     cudaStream_t s = h->stream;
@@ -1226,7 +1226,6 @@ int launch_persistent(culipx_handle_t* h, Csr* A, Factor* M, const double* b, do
         CULIPX_TRY(w->vecs.alloc(h, need));
         w->n = -1;  // the single-RHS workspace size is no longer known
     }
-    if (NR == 1) CULIPX_TRY(sqmr_workspace(w, h, n));
     static int grid_cache[2][kMaxNR + 1] = {};
     int& G = grid_cache[sizeof(TF) == 8 ? 0 : 1][NR];
     if (G == 0) {
@@ -1243,7 +1242,7 @@ int launch_persistent(culipx_handle_t* h, Csr* A, Factor* M, const double* b, do
         CULIPX_CUDA(cudaMemsetAsync(w->ts.get(), 0, (size_t)kTsIters * 8 * sizeof(unsigned long long), s));
         a.ts = w->ts.as<unsigned long long>();
     }
-    return run_persistent<TF, NR>(h, a, G, out_host);
+    return run_persistent<TF, NR>(h, a, G, out_host, wait);
 }
 
 template <class TF>
@@ -1310,6 +1309,42 @@ int sqmr_solve_multi(culipx_handle_t* h, Csr* A, Factor* M, int nrhs, const doub
             if (h_its) h_its[r0 + j] = (int)o[1];
             if (h_status) h_status[r0 + j] = status_of(o, max_it);
         }
+    }
+    return CULIPX_OK;
+}
+
+// The right-hand sides of one system in groups of 4 (then 2 and 1: no
+// padding, so nothing is allocated per call) enqueued on h's stream without
+// waiting; right-hand side r's 8 result values go to out_host + 8 r (pinned
+// memory for a truly asynchronous call).  Groups run one after another on
+// the stream and share the workspace.
+int sqmr_solve_multi_async(culipx_handle_t* h, Csr* A, Factor* M, int nrhs, const double* B, double* X, double tol,
+                           int max_it, Sqmr* w, double* out_host)
+{
+    if (!A || !M || !B || !X || !w || !out_host || nrhs < 1)
+        return fail(CULIPX_INVALID_ARG, "sqmr_solve_multi_async: bad argument");
+    if (A->precision != CULIPX_F64 || A->m != A->n || !M->computed || M->pat->n != A->m)
+        return fail(CULIPX_INVALID_ARG, "sqmr_solve_multi_async: A must be square FP64 and M its computed factor");
+    const size_t n = A->m;
+    const bool f64 = M->precision == CULIPX_F64;
+    for (int r0 = 0; r0 < nrhs;) {
+        const int rem = nrhs - r0;
+        const int nr = rem >= 4 ? 4 : (rem >= 2 ? 2 : 1);
+        const double* b = B + r0 * n;
+        double* x = X + r0 * n;
+        double* o = out_host + (size_t)8 * r0;
+        int st;
+        if (nr == 4)
+            st = f64 ? launch_persistent<double, 4>(h, A, M, b, x, tol, max_it, w, o, false)
+                     : launch_persistent<float, 4>(h, A, M, b, x, tol, max_it, w, o, false);
+        else if (nr == 2)
+            st = f64 ? launch_persistent<double, 2>(h, A, M, b, x, tol, max_it, w, o, false)
+                     : launch_persistent<float, 2>(h, A, M, b, x, tol, max_it, w, o, false);
+        else
+            st = f64 ? launch_persistent<double, 1>(h, A, M, b, x, tol, max_it, w, o, false)
+                     : launch_persistent<float, 1>(h, A, M, b, x, tol, max_it, w, o, false);
+        if (st != CULIPX_OK) return st;
+        r0 += nr;
     }
     return CULIPX_OK;
 }

@@ -288,10 +288,15 @@ int culipx_sqmr_solve_many(culipx_handle h, int num, const culipx_csr *A, const 
  * copied at submit.  progress() completes finished batches and admits queued
  * requests, in arrival order and within memory_budget device bytes (<= 0:
  * unlimited), into free slots: per request the values' upload and the numeric
- * factor (BK, level-0 fill), then one launch solving every (request,
- * right-hand side) with SQMR(tol, max_it), one CTA each.  Up to `slots`
- * batches run concurrently on their own streams; at most max_batch requests
- * per batch.  A request's results do not depend on the other requests.
+ * factor (BK, level-0 fill), then the SQMR(tol, max_it) solves.  A batch
+ * holds requests of one class, in arrival order.  Patterns with n below the
+ * large-row threshold (culipx_server_set_large_rows, default 32768): one
+ * launch solving every (request, right-hand side), one CTA each; up to
+ * `slots` such batches run concurrently on their own streams, at most
+ * max_batch requests each.  Larger patterns: per request the whole-GPU
+ * solver of culipx_sqmr_solve_multi (right-hand sides in groups of up to 4),
+ * at most 4 requests per batch, and such a batch runs alone on the device.
+ * A request's results do not depend on the other requests.
  * result() returns CULIPX_PENDING until the request is done; latency_ms runs
  * from submit to the progress() call that saw it finish. */
 typedef struct culipx_server_t *culipx_server;
@@ -309,8 +314,12 @@ int culipx_server_result(culipx_server s, int request_id, double *h_x, int *h_it
 /* forget a finished request */
 int culipx_server_release(culipx_server s, int request_id);
 /* stats[0..7]: queued, running, done, batches launched, device bytes of
- * running requests, device bytes held by patterns and factor pools, patterns, 0 */
+ * running requests, device bytes held by patterns and factor pools, patterns,
+ * large (whole-GPU) batches launched */
 int culipx_server_stats(culipx_server s, long long *stats8);
+/* requests on patterns with n >= rows use the whole-GPU solver (rows >= 1;
+ * default 32768); applies to batches admitted afterwards */
+int culipx_server_set_large_rows(culipx_server s, int rows);
 
 /* culipx_sqmr_refine per system of a batch: every step solves all systems
  * still above tol in one batched launch (the others get a zero right-hand

@@ -46,8 +46,10 @@ def _requests(pats, count, seed):
     return reqs
 
 
-def _serve(pats, reqs, slots=2, max_batch=4, budget=0):
+def _serve(pats, reqs, slots=2, max_batch=4, budget=0, large_rows=None):
     s = cb.Server(0, budget, slots, max_batch, 1e-8, 1000)
+    if large_rows is not None:
+        s.set_large_rows(large_rows)
     pids = [s.add_pattern(rp, ci, bs) for rp, ci, v, bs in pats]
     ids = [s.submit(pids[p], vals, b) for p, vals, b in reqs]
     done = 0
@@ -78,6 +80,33 @@ def test_server_same_alone_and_in_the_mix():
     for r in range(b.shape[1]):
         xo, _, ito = oracle.sqmr(rp, ci, vals, b[:, r], F, 1e-8, 1000)
         # hundreds of iterations: the summation orders' rounding shifts the count a little
+        assert abs(int(its[r]) - ito) <= max(4, 0.05 * ito)
+        assert np.linalg.norm(x[:, r] - xo) / np.linalg.norm(xo) < 1e-4
+
+
+def test_server_large_requests_whole_gpu_path():
+    """Patterns at or above the large-row threshold are solved by the
+    whole-GPU solver in batches of their own that run alone; results are the
+    same alone and in the mix, and agree with the oracle."""
+    pats = []
+    for k, n in enumerate((400, 900, 1100)):  # N = 600 (small), 1350, 1650 (large)
+        rp, ci, v = cb.kkt_generate(n, n // 2, 6, 16, 1e-3, 1e3, seed=cb.SEED + 5100 + k)
+        pats.append((rp, ci, v, cb.kkt_blocking(n, n // 2, 16)))
+    reqs = _requests(pats, 9, seed=4)
+    mixed, s = _serve(pats, reqs, slots=2, max_batch=4, large_rows=1000)
+    st = s.stats()
+    assert st["done"] == 9 and st["large_batches"] >= 1 and st["batches"] > st["large_batches"]
+    for k in range(9):
+        alone, _ = _serve(pats, [reqs[k]], slots=1, max_batch=1, large_rows=1000)
+        assert np.array_equal(mixed[k][0], alone[0][0]) and np.array_equal(mixed[k][1], alone[0][1])
+    # a large request against the oracle
+    k = next(i for i, (p, _, _) in enumerate(reqs) if len(pats[p][0]) - 1 >= 1000)
+    p, vals, b = reqs[k]
+    rp, ci, v, bs = pats[p]
+    F = oracle.Sym(rp, ci, bs, 0, 1.0).factor(vals)
+    x, its, status, lat = mixed[k]
+    for r in range(b.shape[1]):
+        xo, _, ito = oracle.sqmr(rp, ci, vals, b[:, r], F, 1e-8, 1000)
         assert abs(int(its[r]) - ito) <= max(4, 0.05 * ito)
         assert np.linalg.norm(x[:, r] - xo) / np.linalg.norm(xo) < 1e-4
 
