@@ -419,16 +419,120 @@ def run_reference_spmv(args):
     print(json.dumps(out), flush=True)
 
 
+def run_reference_batch(args):
+    """The CPU restatement on the batched workload: each step solves one
+    system of the 512 (a fixed spread sample, system 37 k mod 512 at step k)
+    with the whole algorithm: FP64 factor (the restatement's SQMR takes an
+    FP64 factor) and the same refinement loop (inner SQMR tol 1e-6, max_it,
+    at most --max-refine corrections, true FP64 residual, target 1e-8);
+    value = systems solved per second by one core."""
+    import oracle
+
+    syst = batch_systems(args.batch)
+    ms, its_all = [], []
+    for i in range(args.warmup + args.steps):
+        rp, ci, v, bs = syst[(37 * i) % len(syst)]
+        N = len(rp) - 1
+        b = __import__("culip_b200").normal_vector(__import__("culip_b200").SEED + 4000 + 100000 + (37 * i) % len(syst), N)
+        t0 = time.perf_counter()
+        F = oracle.Sym(rp, ci, bs, 0, 1.0).factor(v)
+        x = np.zeros(N)
+        r = b.copy()
+        nb = float(np.linalg.norm(b))
+        its = 0
+        for _ in range(args.max_refine):
+            if np.linalg.norm(r) <= 1e-8 * nb:
+                break
+            d, _, it = oracle.sqmr(rp, ci, v, r, F, 1e-6, args.max_it)
+            its += it
+            x += d
+            r = b - oracle.spmv(rp, ci, v, x)
+        if i >= args.warmup:
+            ms.append((time.perf_counter() - t0) * 1e3)
+            its_all.append(its)
+    t = float(np.mean(ms))
+    value = 1e3 / t
+    out = {"metric": "KKT solves/s (batched uneven instances, FP32 factor + FP64 refinement to relres 1e-8)",
+           "value": value, "unit": "solves/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": t, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic (seeded KKT generator)", "impl": "reference",
+           "config": {"workload": f"{len(syst)} KKT systems, n U[500,20000], m=n/2, A 4-8/col (band_half=32), "
+                                  f"H log-U[1e-4,1e4], blocks 32, BK, fill 0",
+                      "solver": f"oracle FP64 factor + SQMR (inner tol 1e-6, max_it {args.max_it}) in the same "
+                                f"refinement loop, at most {args.max_refine} corrections", "parallelism": "one CPU thread"},
+           "cpu_baseline": {"value": value, "unit": "solves/s", "cores": 1, "kind": "port",
+                            "sample": f"{args.steps} systems (37 k mod 512), each solved whole; median SQMR "
+                                      f"iterations {int(np.median(its_all))}"},
+           "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def run_reference_served(args):
+    """The CPU restatement on the served stream's requests, one after another
+    on one core: each step takes the next request of the same arrival trace
+    (pattern, 1-8 right-hand sides; the trace's first --warmup + --steps
+    requests) and runs the oracle's factor plus, per right-hand side, a
+    20-iteration SQMR sample scaled to max_it iterations (every right-hand
+    side of this stream runs to max_it: none reaches 1e-8); value = requests
+    per second."""
+    import oracle
+
+    import culip_b200 as cb
+
+    seed_base = cb.SEED + 5000
+    pats = served_workload(args.patterns, seed_base)
+    rng = np.random.default_rng(seed_base + 999)
+    reqs = []
+    while len(reqs) < args.warmup + args.steps:
+        rng.exponential(1.0 / args.rate)
+        reqs.append((int(rng.integers(0, len(pats))), int(rng.integers(1, 9))))
+    syms = {}
+    ms = []
+    sample_it = 20
+    for i, (j, nrhs) in enumerate(reqs):
+        rp, ci, v, bs, n = pats[j]
+        N = len(rp) - 1
+        if j not in syms:
+            syms[j] = oracle.Sym(rp, ci, bs, 0, 1.0)  # the server analyses each pattern once
+        t0 = time.perf_counter()
+        F = syms[j].factor(v)
+        t1 = time.perf_counter()
+        solve = 0.0
+        for k in range(nrhs):
+            b = cb.normal_vector(seed_base + 7 * i + k, N)
+            t2 = time.perf_counter()
+            oracle.sqmr(rp, ci, v, b, F, 1e-8, sample_it)
+            solve += (time.perf_counter() - t2) / sample_it * args.max_it
+        if i >= args.warmup:
+            ms.append(((t1 - t0) + solve) * 1e3)
+    t = float(np.mean(ms))
+    value = 1e3 / t
+    out = {"metric": "KKT solves/s and p50/p99 latency (served IPM stream, FP64 plain method per request)",
+           "value": value, "unit": "requests/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": t, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic (seeded KKT generator, Poisson arrivals)", "impl": "reference",
+           "config": {"workload": f"{len(pats)} patterns, n log-U[1e3,5e5], m=n/2, A 6/col (band_half=32), "
+                                  f"the served trace's requests, 1-8 RHS",
+                      "solver": f"oracle factor + SQMR tol 1e-8, max_it {args.max_it}, requests one after another",
+                      "parallelism": "one CPU thread"},
+           "latency_ms": {"p50": float(np.percentile(ms, 50)), "p99": float(np.percentile(ms, 99))},
+           "cpu_baseline": {"value": value, "unit": "requests/s", "cores": 1, "kind": "port",
+                            "sample": f"{args.steps} requests of the trace: factor whole, SQMR {sample_it} "
+                                      f"iterations per right-hand side scaled to {args.max_it}"},
+           "e2e": {"value": value, "unit": "requests/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
 def run_reference(args):
     world, rank, _ = _dist()
     if rank != 0:
         return
     if args.config == "spmv":
         return run_reference_spmv(args)
-    if args.config in ("batch", "served"):
-        print(json.dumps({"impl": "reference", "unavailable": f"--config {args.config}: the reference arm times the "
-                          "single-system workloads (small, scale, mixed) and spmv only"}), flush=True)
-        return
+    if args.config == "batch":
+        return run_reference_batch(args)
+    if args.config == "served":
+        return run_reference_served(args)
     cfg, rp, ci, v, bs, b = _workload(args.config)
     import oracle
 
@@ -861,6 +965,7 @@ def run_served(args):
         srv.progress(wait=True)
     clocks = ClockSampler(local)
     clocks.start()
+    launches0 = srv.launch_count()
     ids = []
     start = time.perf_counter()
     k = 0
@@ -877,6 +982,7 @@ def run_served(args):
             srv.progress(wait=True)
     elapsed = time.perf_counter() - start
     ck = clocks.stop()
+    launches = srv.launch_count() - launches0
     lat, its, conv, nrhs_tot = [], [], 0, 0
     for i in ids:
         x, it, st, l = srv.result(i)
@@ -893,13 +999,14 @@ def run_served(args):
         "config": {"workload": f"{len(pats)} patterns, n log-U[1e3,5e5], m=n/2, A 6/col (band_half=32), "
                                f"Poisson {args.rate:g} req/s for {args.duration:g} s ({len(ids)} requests), "
                                f"1-8 RHS, H *= 10^U(-1,1) clipped [1e-8,1e8] per request",
-                   "solver": f"server: 3 slots, batched SQMR (one CTA per right-hand side), tol 1e-8, "
-                             f"max_it {args.max_it}", "parallelism": "one GPU"},
+                   "solver": f"server: 3 slots; patterns with N < 32768: batched SQMR, one CTA per right-hand "
+                             f"side; larger: the whole-GPU solver, right-hand sides in groups of up to 4, in "
+                             f"exclusive batches; tol 1e-8, max_it {args.max_it}", "parallelism": "one GPU"},
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                        "mean": float(lat.mean()), "max": float(lat.max())},
         "right_hand_sides": nrhs_tot, "converged_fraction": conv / max(nrhs_tot, 1),
         "median_iterations": int(np.median(its)) if its else None, "pattern_analysis_s_once": analysis_s,
-        "clocks": ck, "gpu_launches": None,
+        "clocks": ck, "gpu_launches": int(launches),
     }
     if rank == 0:
         print(json.dumps(out), flush=True)

@@ -450,6 +450,11 @@ class Server:
         keys = ["queued", "running", "done", "batches", "running_bytes", "held_bytes", "patterns", "large_batches"]
         return {k: int(x) for k, x in zip(keys, v)}
 
+    def launch_count(self) -> int:
+        v = ctypes.c_longlong()
+        capi.call("culipx_server_launch_count", self._h, ctypes.byref(v))
+        return v.value
+
     def set_large_rows(self, rows: int):
         """Patterns with n >= rows are solved by the whole-GPU solver."""
         capi.call("culipx_server_set_large_rows", self._h, int(rows))

@@ -617,6 +617,11 @@ CULIPX_API int culipx_server_set_large_rows(culipx_server s, int rows)
     return server_set_large_rows(s, rows);
 }
 
+CULIPX_API int culipx_server_launch_count(culipx_server s, long long* count)
+{
+    return server_launch_count(s, count);
+}
+
 CULIPX_API int culipx_batch_sqmr_refine(culipx_batch b, culipx_csr A, culipx_factor M, const double* d_b,
                                         double* d_x, double tol, double inner_tol, int inner_max_it, int max_refine,
                                         double* h_relres, int* h_iterations, int* h_steps, int* h_status)

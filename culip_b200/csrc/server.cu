@@ -192,6 +192,15 @@ long long Server::fixed_bytes() const
     return t;
 }
 
+int server_launch_count(Server* s, long long* out)
+{
+    if (!s || !out) return fail(CULIPX_INVALID_ARG, "null argument");
+    long long t = s->base->launches;
+    for (const auto& sl : s->slots) t += sl.h->launches;
+    *out = t;
+    return CULIPX_OK;
+}
+
 int server_set_large_rows(Server* s, int rows)
 {
     if (!s || rows < 1) return fail(CULIPX_INVALID_ARG, "culipx_server_set_large_rows: bad argument");

@@ -79,6 +79,7 @@ int server_result(Server* s, int id, double* x, int* its, int* status, double* l
 int server_release(Server* s, int id);
 int server_stats(Server* s, long long* st8);
 int server_set_large_rows(Server* s, int rows);
+int server_launch_count(Server* s, long long* out);
 int factor_compute(Factor* f, const void* d_vals, const int* h_is_piv, int pivot, double threshold);
 int factor_create(Pattern* p, Factor** out);
 

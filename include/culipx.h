@@ -320,6 +320,8 @@ int culipx_server_stats(culipx_server s, long long *stats8);
 /* requests on patterns with n >= rows use the whole-GPU solver (rows >= 1;
  * default 32768); applies to batches admitted afterwards */
 int culipx_server_set_large_rows(culipx_server s, int rows);
+/* kernels the server has launched so far (all slots) */
+int culipx_server_launch_count(culipx_server s, long long *count);
 
 /* culipx_sqmr_refine per system of a batch: every step solves all systems
  * still above tol in one batched launch (the others get a zero right-hand
