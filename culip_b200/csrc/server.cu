@@ -12,7 +12,9 @@
 //   * runs admitted requests as a batch on one of several slots, each with
 //     its own stream and workspace: per request the values' upload and the
 //     numeric factor, then the solves; results come back through pinned
-//     buffers.  A batch holds requests of one class, in arrival order:
+//     buffers.  A batch holds requests of one class, the class of the
+//     oldest queued request, in arrival order (requests of the other class
+//     keep their places in the queue):
 //       - small patterns (n < large_rows): ONE launch solving every
 //         (request, right-hand side) pair, one CTA each (k_sqmr_many);
 //       - large patterns: per request the whole-GPU cooperative solver,
@@ -255,25 +257,39 @@ int launch_slot(Server* s, ServerSlot& sl)
     const bool large = is_large(s->queue.front());
     if (large && s->running_slots() > 0) return CULIPX_OK;  // wait until the device is idle
     const int cap = large ? std::min(s->max_batch, kLargeBatch) : s->max_batch;
-    // admit in arrival order, one class per batch, while the budget allows
+    // admit requests of the oldest request's class, in arrival order (those of
+    // the other class keep their places), while the budget allows
     std::vector<int> admit;
     int systems = 0;
-    while (!s->queue.empty() && (int)admit.size() < cap) {
-        if (is_large(s->queue.front()) != large) break;
-        ServerRequest& r = s->requests.at(s->queue.front());
+    std::deque<int> rest;
+    while (!s->queue.empty()) {
+        const int id = s->queue.front();
+        s->queue.pop_front();
+        if ((int)admit.size() >= cap || is_large(id) != large) {
+            rest.push_back(id);
+            continue;
+        }
+        ServerRequest& r = s->requests.at(id);
         const ServerPattern& sp = s->patterns[r.pid];
         const long long need = request_bytes(sp, r.nrhs);
         const long long fbytes = sp.free_factors.empty() ? sp.factor_bytes_estimate() : 0;
         const bool fits = s->budget <= 0 || s->fixed_bytes() + s->in_use + need + fbytes <= s->budget;
         // over the budget: wait for running batches to free memory (a request
         // that fits alone always runs once the device is idle)
-        if (!fits && (!admit.empty() || s->running_slots() > 0)) break;
+        if (!fits && (!admit.empty() || s->running_slots() > 0)) {
+            rest.push_back(id);
+            while (!s->queue.empty()) {
+                rest.push_back(s->queue.front());
+                s->queue.pop_front();
+            }
+            break;
+        }
         r.bytes = need;
         s->in_use += need;
         admit.push_back(r.id);
         systems += r.nrhs;
-        s->queue.pop_front();
     }
+    s->queue.swap(rest);
     if (admit.empty()) return CULIPX_OK;
     // pinned result buffers
     size_t xtot = 0;
