@@ -54,6 +54,8 @@ def _parse():
     ap.add_argument("--rate", type=float, default=2000.0, help="--config served: arrivals per second")
     ap.add_argument("--duration", type=float, default=0.25, help="--config served: seconds of arrivals")
     ap.add_argument("--patterns", type=int, default=64, help="--config served: sparsity patterns")
+    ap.add_argument("--large-rows", type=int, default=131072,
+                    help="--config served: patterns with N >= this use the whole-GPU solver")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--max-it", type=int, default=1000, help="SQMR iteration cap (1000 = the driver's setting)")
     ap.add_argument("--batch", type=int, default=512, help="systems in --config batch")
@@ -955,6 +957,7 @@ def run_served(args):
         return v, rng.standard_normal((len(pats[j][0]) - 1, nrhs))
 
     srv = cb.Server(local, 0, 3, 512, 1e-8, args.max_it)
+    srv.set_large_rows(args.large_rows)
     t0 = time.perf_counter()
     pids = [srv.add_pattern(rp, ci, bs) for rp, ci, v, bs, n in pats]
     analysis_s = time.perf_counter() - t0
@@ -999,7 +1002,7 @@ def run_served(args):
         "config": {"workload": f"{len(pats)} patterns, n log-U[1e3,5e5], m=n/2, A 6/col (band_half=32), "
                                f"Poisson {args.rate:g} req/s for {args.duration:g} s ({len(ids)} requests), "
                                f"1-8 RHS, H *= 10^U(-1,1) clipped [1e-8,1e8] per request",
-                   "solver": f"server: 3 slots; patterns with N < 32768: batched SQMR, one CTA per right-hand "
+                   "solver": f"server: 3 slots; patterns with N < {args.large_rows}: batched SQMR, one CTA per right-hand "
                              f"side; larger: the whole-GPU solver, right-hand sides in groups of up to 4, in "
                              f"exclusive batches; tol 1e-8, max_it {args.max_it}", "parallelism": "one GPU"},
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),

@@ -55,7 +55,7 @@ struct Server {
     int device = 0;
     long long budget = 0, in_use = 0;
     int max_batch = 0, max_it = 0;
-    int large_rows = 32768;                // patterns with n >= this get the whole-GPU solver
+    int large_rows = 131072;               // patterns with n >= this get the whole-GPU solver
     long long large_batches = 0;
     double tol = 0.0;
     culipx_handle_t* base = nullptr;       // owns the patterns' device mirrors

@@ -290,7 +290,7 @@ int culipx_sqmr_solve_many(culipx_handle h, int num, const culipx_csr *A, const 
  * unlimited), into free slots: per request the values' upload and the numeric
  * factor (BK, level-0 fill), then the SQMR(tol, max_it) solves.  A batch
  * holds requests of one class, in arrival order.  Patterns with n below the
- * large-row threshold (culipx_server_set_large_rows, default 32768): one
+ * large-row threshold (culipx_server_set_large_rows, default 131072): one
  * launch solving every (request, right-hand side), one CTA each; up to
  * `slots` such batches run concurrently on their own streams, at most
  * max_batch requests each.  Larger patterns: per request the whole-GPU
@@ -318,7 +318,7 @@ int culipx_server_release(culipx_server s, int request_id);
  * large (whole-GPU) batches launched */
 int culipx_server_stats(culipx_server s, long long *stats8);
 /* requests on patterns with n >= rows use the whole-GPU solver (rows >= 1;
- * default 32768); applies to batches admitted afterwards */
+ * default 131072); applies to batches admitted afterwards */
 int culipx_server_set_large_rows(culipx_server s, int rows);
 /* kernels the server has launched so far (all slots) */
 int culipx_server_launch_count(culipx_server s, long long *count);
