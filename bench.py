@@ -54,6 +54,8 @@ def _parse():
     ap.add_argument("--rate", type=float, default=2000.0, help="--config served: arrivals per second")
     ap.add_argument("--duration", type=float, default=0.25, help="--config served: seconds of arrivals")
     ap.add_argument("--patterns", type=int, default=64, help="--config served: sparsity patterns")
+    ap.add_argument("--precision", default="f32", choices=["f32", "f64"],
+                    help="--config served: factor precision (f32: FP32 factor and applies, FP64 SQMR)")
     ap.add_argument("--large-rows", type=int, default=131072,
                     help="--config served: patterns with N >= this use the whole-GPU solver")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -959,7 +961,8 @@ def run_served(args):
     srv = cb.Server(local, 0, 3, 512, 1e-8, args.max_it)
     srv.set_large_rows(args.large_rows)
     t0 = time.perf_counter()
-    pids = [srv.add_pattern(rp, ci, bs) for rp, ci, v, bs, n in pats]
+    prec = cb.F32 if args.precision == "f32" else cb.F64
+    pids = [srv.add_pattern(rp, ci, bs, prec) for rp, ci, v, bs, n in pats]
     analysis_s = time.perf_counter() - t0
     # warm-up: one request per pattern (factor pools, workspaces)
     for j in range(len(pats)):
@@ -995,10 +998,12 @@ def run_served(args):
         nrhs_tot += len(st)
     lat = np.array(lat)
     out = {
-        "metric": "KKT solves/s and p50/p99 latency (served IPM stream, FP64 plain method per request)",
+        "metric": "KKT solves/s and p50/p99 latency (served IPM stream, "
+                  + ("FP32 factor + FP64 SQMR" if args.precision == "f32" else "FP64 plain method") + " per request)",
         "value": len(ids) / elapsed, "unit": "requests/s", "n_gpus": world, "steps": len(ids), "warmup": len(pats),
         "ms_per_step": 1e3 * elapsed / max(len(ids), 1), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded KKT generator, Poisson arrivals)",
+        "vs_baseline": None, "dtype": "f32 factor / f64 recurrence" if args.precision == "f32" else "f64",
+        "data": "synthetic (seeded KKT generator, Poisson arrivals)",
         "config": {"workload": f"{len(pats)} patterns, n log-U[1e3,5e5], m=n/2, A 6/col (band_half=32), "
                                f"Poisson {args.rate:g} req/s for {args.duration:g} s ({len(ids)} requests), "
                                f"1-8 RHS, H *= 10^U(-1,1) clipped [1e-8,1e8] per request",

@@ -46,11 +46,11 @@ def _requests(pats, count, seed):
     return reqs
 
 
-def _serve(pats, reqs, slots=2, max_batch=4, budget=0, large_rows=None):
+def _serve(pats, reqs, slots=2, max_batch=4, budget=0, large_rows=None, precision=cb.F64):
     s = cb.Server(0, budget, slots, max_batch, 1e-8, 1000)
     if large_rows is not None:
         s.set_large_rows(large_rows)
-    pids = [s.add_pattern(rp, ci, bs) for rp, ci, v, bs in pats]
+    pids = [s.add_pattern(rp, ci, bs, precision) for rp, ci, v, bs in pats]
     ids = [s.submit(pids[p], vals, b) for p, vals, b in reqs]
     done = 0
     while done < len(ids):
@@ -109,6 +109,31 @@ def test_server_large_requests_whole_gpu_path():
         xo, _, ito = oracle.sqmr(rp, ci, vals, b[:, r], F, 1e-8, 1000)
         assert abs(int(its[r]) - ito) <= max(4, 0.05 * ito)
         assert np.linalg.norm(x[:, r] - xo) / np.linalg.norm(xo) < 1e-4
+
+
+@pytest.mark.parametrize("large_rows", [None, 1000])
+def test_server_fp32_factors(large_rows):
+    """FP32 factors (FP64 SQMR): both solver classes, the same alone and in
+    the mix; the SQMR stopping test (tol 1e-8 on the quasi-residual, which an
+    FP32 preconditioner bounds) leaves a true residual of about 1e-4."""
+    import scipy.sparse as sp
+
+    pats = []
+    for k, n in enumerate((400, 900)):  # N = 600, 1350
+        rp, ci, v = cb.kkt_generate(n, n // 2, 6, 16, 1e-3, 1e3, seed=cb.SEED + 5200 + k)
+        pats.append((rp, ci, v, cb.kkt_blocking(n, n // 2, 16)))
+    reqs = _requests(pats, 6, seed=5)
+    mixed, s = _serve(pats, reqs, large_rows=large_rows, precision=cb.F32)
+    assert s.stats()["done"] == 6
+    for k in (0, 5):
+        alone, _ = _serve(pats, [reqs[k]], slots=1, max_batch=1, large_rows=large_rows, precision=cb.F32)
+        assert np.array_equal(mixed[k][0], alone[0][0])
+    for (p, vals, b), (x, its, status, lat) in zip(reqs, mixed):
+        rp, ci, v, bs = pats[p]
+        K = sp.csr_matrix((vals, ci, rp))
+        for r in range(b.shape[1]):
+            assert status[r] == capi.OK
+            assert np.linalg.norm(b[:, r] - K @ x[:, r]) / np.linalg.norm(b[:, r]) < 5e-3
 
 
 def test_server_memory_budget_serializes_but_completes():
