@@ -15,8 +15,9 @@
 //     buffers.  A batch holds requests of one class, the class of the
 //     oldest queued request, in arrival order (requests of the other class
 //     keep their places in the queue):
-//       - small patterns (n < large_rows): ONE launch solving every
-//         (request, right-hand side) pair, one CTA each (k_sqmr_many);
+//       - small patterns (n < large_rows): one CTA per request and group
+//         of up to 4 of its right-hand sides (k_sqmr_many, one launch per
+//         factor precision and group size);
 //       - large patterns: per request the whole-GPU cooperative solver,
 //         its right-hand sides in groups of up to 4 per launch (one CTA per
 //         system would leave a large system to a single SM for its whole
@@ -216,6 +217,9 @@ namespace {
 // queued behind them get the device back after a few
 constexpr int kLargeBatch = 4;
 
+// work units that keep every CTA of a batched launch busy (2 per SM)
+constexpr int kManyUnits = 296;
+
 int finish_slot(Server* s, ServerSlot& sl)
 {
     const double t = now_ms();
@@ -367,40 +371,34 @@ int launch_slot(Server* s, ServerSlot& sl)
         for (int i = 0; i < k; ++i) sl.order[i] = i;
         ++s->large_batches;
     }
-    for (size_t q = 0; q < admit.size() && !large; ++q) {
-        ServerRequest& r = s->requests.at(admit[q]);
-        const int n = s->patterns[r.pid].n;
-        for (int k = 0; k < r.nrhs; ++k) {
-            As.push_back(&sl.csrs[q]);
-            Ms.push_back(r.F);
-            bs.push_back(static_cast<const double*>(r.d_b) + (size_t)k * n);
-            xs.push_back(static_cast<double*>(r.d_x) + (size_t)k * n);
+    if (!large) {
+        // one CTA per (request, group of 4 / 2 / 1 right-hand sides): the
+        // group's right-hand sides share every factor and K load; results
+        // land in request order
+        std::vector<int> nrs;
+        // group right-hand sides only when the groups still outnumber the
+        // CTAs several times over: otherwise fewer, longer work units leave
+        // the device idle at the end of the batch
+        const bool group_rhs = systems >= 4 * kManyUnits;
+        for (size_t q = 0; q < admit.size(); ++q) {
+            ServerRequest& r = s->requests.at(admit[q]);
+            const int n = s->patterns[r.pid].n;
+            for (int c0 = 0; c0 < r.nrhs;) {
+                const int rem = r.nrhs - c0;
+                const int g = (group_rhs && rem >= 4) ? 4 : ((group_rhs && rem >= 2) ? 2 : 1);
+                As.push_back(&sl.csrs[q]);
+                Ms.push_back(r.F);
+                bs.push_back(static_cast<const double*>(r.d_b) + (size_t)c0 * n);
+                xs.push_back(static_cast<double*>(r.d_x) + (size_t)c0 * n);
+                nrs.push_back(g);
+                c0 += g;
+            }
         }
+        CULIPX_TRY(sqmr_solve_many_nr_async(sl.h, (int)As.size(), As.data(), Ms.data(), bs.data(), xs.data(),
+                                            nrs.data(), s->tol, s->max_it, sl.h->sqmr, sl.out_host));
+        sl.order.resize(systems);
+        for (int i = 0; i < systems; ++i) sl.order[i] = i;
     }
-    // one launch for every (request, right-hand side); FP32 and FP64 factors go in separate launches
-    std::vector<int> order(As.size());
-    for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return Ms[a]->precision < Ms[b]->precision; });
-    size_t g0 = 0;
-    while (!large && g0 < order.size()) {
-        size_t g1 = g0;
-        while (g1 < order.size() && Ms[order[g1]]->precision == Ms[order[g0]]->precision) ++g1;
-        std::vector<Csr*> a;
-        std::vector<Factor*> m;
-        std::vector<const double*> bb;
-        std::vector<double*> xx;
-        for (size_t i = g0; i < g1; ++i) {
-            a.push_back(As[order[i]]);
-            m.push_back(Ms[order[i]]);
-            bb.push_back(bs[order[i]]);
-            xx.push_back(xs[order[i]]);
-        }
-        CULIPX_TRY(sqmr_solve_many_async(sl.h, (int)(g1 - g0), a.data(), m.data(), bb.data(), xx.data(), s->tol,
-                                         s->max_it, sl.h->sqmr, sl.out_host + g0 * 8));
-        g0 = g1;
-    }
-    // the groups' results were written in sorted order; keep the permutation to undo it
-    if (!large) sl.order = order;
     size_t xo = 0;
     for (int id : admit) {
         ServerRequest& r = s->requests.at(id);

@@ -51,6 +51,8 @@ int sqmr_solve_many(culipx_handle_t* h, int num, Csr* const* A, Factor* const* M
 
 int sqmr_solve_many_async(culipx_handle_t* h, int num, Csr* const* A, Factor* const* M, const double* const* b,
                           double* const* x, double tol, int max_it, Sqmr* w, double* out_host);
+int sqmr_solve_many_nr_async(culipx_handle_t* h, int num, Csr* const* A, Factor* const* M, const double* const* b,
+                             double* const* x, const int* nr, double tol, int max_it, Sqmr* w, double* out_host);
 void many_results(int num, int max_it, const double* out, double* h_res, int* h_its, int* h_status);
 
 int sqmr_solve_multi(culipx_handle_t* h, Csr* A, Factor* M, int nrhs, const double* B, double* X, double tol,

@@ -1094,12 +1094,14 @@ __global__ void __launch_bounds__(kT, kCtasPerSm) k_sqmr_batched(PArgs<TF> a, Ba
 
 // Batched solves of independent systems that each have their own pattern,
 // factor, matrix and vectors (the serving path): the CTA copies system s's
-// argument block into shared memory and runs the same body over its rows.
+// argument block into shared memory and runs the same body over its rows,
+// for nr[s] (1, 2 or 4) right-hand sides of that system at once.  Systems are
+// handed out in index order, so the host lists the longest first.
 template <class TF>
-__global__ void __launch_bounds__(kT, kCtasPerSm) k_sqmr_many(const PArgs<TF>* __restrict__ sys_args, int num,
-                                                             int* next)
+__global__ void __launch_bounds__(kT, kCtasPerSm) k_sqmr_many(const PArgs<TF>* __restrict__ sys_args,
+                                                             const int* __restrict__ nr, int num, int* next)
 {
-    __shared__ Scal S[1];
+    __shared__ Scal S[kMaxNR];
     __shared__ double sh[kMaxNV][kW];
     __shared__ int sys;
     __shared__ PArgs<TF> pa;
@@ -1115,7 +1117,10 @@ __global__ void __launch_bounds__(kT, kCtasPerSm) k_sqmr_many(const PArgs<TF>* _
         for (int i = threadIdx.x; i < (int)(sizeof(PArgs<TF>) / 8); i += kT) dst[i] = src[i];
         __syncthreads();
         const SysView sv{0, pa.n, pa.lvl_off, pa.lvl_off + 1, pa.out};
-        sqmr_body<TF, 1>(pa, ctx, sv, S, sh);
+        const int r = __ldg(nr + s);
+        if (r == 4) sqmr_body<TF, 4>(pa, ctx, sv, reinterpret_cast<Scal(&)[4]>(S), sh);
+        else if (r == 2) sqmr_body<TF, 2>(pa, ctx, sv, reinterpret_cast<Scal(&)[2]>(S), sh);
+        else sqmr_body<TF, 1>(pa, ctx, sv, reinterpret_cast<Scal(&)[1]>(S), sh);
     }
 }
 
@@ -1474,33 +1479,49 @@ int batch_sqmr_solve(Batch* bt, Csr* A, Factor* M, const double* b, double* x, d
 
 namespace {
 
-// Enqueues the launch on h's stream; each system's 6 result values are
-// copied to out_host + 8 k (pinned memory for a truly asynchronous call)
+// Enqueues one launch per (factor precision, right-hand sides per system)
+// group on h's stream.  System k solves nr[k] (1, 2 or 4) right-hand sides,
+// b[k] / x[k] each n x nr[k] column-major; its results (8 values per
+// right-hand side) go to out_host + 8 (nr[0] + ... + nr[k-1]) (pinned
+// memory for a truly asynchronous call).  One workspace allocation serves
+// every group.
+// every system's work area starts on a 256-byte boundary: with NR even the
+// kernel reads the interleaved vectors with 16-byte loads
+double* align256(double* p)
+{
+    return reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(p) + 255) & ~static_cast<uintptr_t>(255));
+}
+
 template <class TF>
-int launch_many(culipx_handle_t* h, int num, Csr* const* A, Factor* const* M, const double* const* b,
-                double* const* x, double tol, int max_it, Sqmr* w, double* out_host)
+int launch_many_prec(culipx_handle_t* h, const std::vector<int>& ks, const int* nr, Csr* const* A, Factor* const* M,
+                     const double* const* b, double* const* x, const std::vector<size_t>& slot, double tol,
+                     int max_it, double*& base, double* out_host)
 {
     cudaStream_t s = h->stream;
-    size_t total = 0;
-    for (int k = 0; k < num; ++k) total += (size_t)kVecs * A[k]->m + 8;
-    const size_t need = total * sizeof(double) + (size_t)num * sizeof(PArgs<TF>) + 64;
-    if (w->many.bytes() < need) CULIPX_TRY(w->many.alloc(h, need));
-    double* base = w->many.as<double>();
+    const int num = (int)ks.size();
     std::vector<PArgs<TF>> args(num);
-    size_t o = 0;
-    for (int k = 0; k < num; ++k) {
-        args[k] = make_args<TF>(A[k], M[k], base + o, nullptr, b[k], x[k], tol, max_it);
-        o += (size_t)kVecs * A[k]->m + 8;
-        CULIPX_CUDA(cudaMemsetAsync(args[k].v[0], 0, (size_t)kVecs * A[k]->m * sizeof(double), s));
-        CULIPX_CUDA(cudaMemsetAsync(x[k], 0, (size_t)A[k]->m * sizeof(double), s));
+    std::vector<int> nrs(num);
+    for (int i = 0; i < num; ++i) {
+        const int k = ks[i];
+        const int r = nr ? nr[k] : 1;
+        const size_t m = A[k]->m;
+        base = align256(base);
+        args[i] = make_args<TF>(A[k], M[k], base, nullptr, b[k], x[k], tol, max_it, r);
+        base += (size_t)kVecs * m * r + 8 * r;
+        nrs[i] = r;
+        CULIPX_CUDA(cudaMemsetAsync(args[i].v[0], 0, (size_t)kVecs * m * r * sizeof(double), s));
+        CULIPX_CUDA(cudaMemsetAsync(x[k], 0, m * r * sizeof(double), s));
     }
-    // argument blocks after the vectors (8-byte aligned), then the counter
-    PArgs<TF>* d_args = reinterpret_cast<PArgs<TF>*>(base + o);
-    int* d_next = reinterpret_cast<int*>(d_args + num);
+    // argument blocks after the vectors, then the right-hand-side counts and the counter
+    base = align256(base);
+    PArgs<TF>* d_args = reinterpret_cast<PArgs<TF>*>(base);
+    int* d_nr = reinterpret_cast<int*>(d_args + num);
+    int* d_next = d_nr + num;
+    base = reinterpret_cast<double*>(d_args + num) + (num + 2) / 2 + 1;
     CULIPX_CUDA(cudaMemcpyAsync(d_args, args.data(), (size_t)num * sizeof(PArgs<TF>), cudaMemcpyHostToDevice, s));
+    CULIPX_CUDA(cudaMemcpyAsync(d_nr, nrs.data(), (size_t)num * sizeof(int), cudaMemcpyHostToDevice, s));
     CULIPX_CUDA(cudaMemsetAsync(d_next, 0, sizeof(int), s));
-    static int grid_cache[2] = {0, 0};
-    int& G = grid_cache[sizeof(TF) == 8 ? 0 : 1];
+    static int G = 0;
     if (G == 0) {
         int dev = 0, per_sm = 0, sms = 0;
         CULIPX_CUDA(cudaGetDevice(&dev));
@@ -1509,23 +1530,58 @@ int launch_many(culipx_handle_t* h, int num, Csr* const* A, Factor* const* M, co
         if (per_sm < 1) return fail(CULIPX_NOT_SUPPORTED, "batched SQMR kernel does not fit on an SM");
         G = sms * std::min(per_sm, kCtasPerSm);
     }
-    k_sqmr_many<TF><<<std::min(G, num), kT, 0, s>>>(d_args, num, d_next);
+    k_sqmr_many<TF><<<std::min(G, num), kT, 0, s>>>(d_args, d_nr, num, d_next);
     h->launches += 1;
     CULIPX_TRY(launch_check("k_sqmr_many"));
-    for (int k = 0; k < num; ++k)
-        CULIPX_CUDA(cudaMemcpyAsync(out_host + (size_t)k * 8, args[k].out, 6 * sizeof(double),
+    for (int i = 0; i < num; ++i)
+        CULIPX_CUDA(cudaMemcpyAsync(out_host + 8 * slot[ks[i]], args[i].out, (size_t)8 * nrs[i] * sizeof(double),
                                     cudaMemcpyDeviceToHost, s));
     return CULIPX_OK;
 }
 
 }  // namespace
 
+int sqmr_solve_many_nr_async(culipx_handle_t* h, int num, Csr* const* A, Factor* const* M, const double* const* b,
+                             double* const* x, const int* nr, double tol, int max_it, Sqmr* w, double* out_host)
+{
+    if (num == 0) return CULIPX_OK;
+    // result slots in the caller's order; per factor precision one launch with
+    // the systems longest first (rows x right-hand sides), so the CTAs that
+    // take the last systems finish close together
+    std::vector<size_t> slot(num);
+    size_t total = 0, acc = 0;
+    std::vector<int> groups[2];
+    for (int k = 0; k < num; ++k) {
+        const int r = nr ? nr[k] : 1;
+        if (r != 1 && r != 2 && r != 4) return fail(CULIPX_INVALID_ARG, "sqmr_solve_many: nr must be 1, 2 or 4");
+        slot[k] = acc;
+        acc += r;
+        total += (size_t)kVecs * A[k]->m * r + 8 * r + 32;  // + alignment
+        groups[M[k]->precision == CULIPX_F64 ? 0 : 1].push_back(k);
+    }
+    size_t argbytes = 0;
+    for (int p = 0; p < 2; ++p) {
+        std::vector<int>& ks = groups[p];
+        std::stable_sort(ks.begin(), ks.end(), [&](int a, int c) {
+            return (long long)A[a]->m * (nr ? nr[a] : 1) > (long long)A[c]->m * (nr ? nr[c] : 1);
+        });
+        if (!ks.empty())
+            argbytes += ks.size() * ((p == 0 ? sizeof(PArgs<double>) : sizeof(PArgs<float>)) + sizeof(int)) + 512;
+    }
+    const size_t need = total * sizeof(double) + argbytes + 256;
+    if (w->many.bytes() < need) CULIPX_TRY(w->many.alloc(h, need));
+    double* base = w->many.as<double>();
+    if (!groups[0].empty())
+        CULIPX_TRY(launch_many_prec<double>(h, groups[0], nr, A, M, b, x, slot, tol, max_it, base, out_host));
+    if (!groups[1].empty())
+        CULIPX_TRY(launch_many_prec<float>(h, groups[1], nr, A, M, b, x, slot, tol, max_it, base, out_host));
+    return CULIPX_OK;
+}
+
 int sqmr_solve_many_async(culipx_handle_t* h, int num, Csr* const* A, Factor* const* M, const double* const* b,
                           double* const* x, double tol, int max_it, Sqmr* w, double* out_host)
 {
-    if (num == 0) return CULIPX_OK;
-    return (M[0]->precision == CULIPX_F64) ? launch_many<double>(h, num, A, M, b, x, tol, max_it, w, out_host)
-                                           : launch_many<float>(h, num, A, M, b, x, tol, max_it, w, out_host);
+    return sqmr_solve_many_nr_async(h, num, A, M, b, x, nullptr, tol, max_it, w, out_host);
 }
 
 void many_results(int num, int max_it, const double* out, double* h_res, int* h_its, int* h_status)

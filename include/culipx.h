@@ -290,10 +290,10 @@ int culipx_sqmr_solve_many(culipx_handle h, int num, const culipx_csr *A, const 
  * unlimited), into free slots: per request the values' upload and the numeric
  * factor (BK, level-0 fill), then the SQMR(tol, max_it) solves.  A batch
  * holds requests of one class, in arrival order.  Patterns with n below the
- * large-row threshold (culipx_server_set_large_rows, default 131072): one
- * launch solving every (request, right-hand side), one CTA each; up to
- * `slots` such batches run concurrently on their own streams, at most
- * max_batch requests each.  Larger patterns: per request the whole-GPU
+ * large-row threshold (culipx_server_set_large_rows, default 131072): one CTA
+ * per request and group of up to 4 of its right-hand sides (the group shares
+ * every factor and K load); up to `slots` such batches run concurrently on
+ * their own streams, at most max_batch requests each.  Larger patterns: per request the whole-GPU
  * solver of culipx_sqmr_solve_multi (right-hand sides in groups of up to 4),
  * at most 4 requests per batch, and such a batch runs alone on the device.
  * A request's results do not depend on the other requests.
