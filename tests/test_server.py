@@ -136,6 +136,26 @@ def test_server_fp32_factors(large_rows):
             assert np.linalg.norm(b[:, r] - K @ x[:, r]) / np.linalg.norm(b[:, r]) < 5e-3
 
 
+def test_server_grouped_right_hand_sides():
+    """A batch of more than 4 x 296 right-hand sides is solved four (then two,
+    one) right-hand sides per CTA: every request's result agrees with the
+    same request served alone (one right-hand side per CTA)."""
+    n = 300
+    rp, ci, v = cb.kkt_generate(n, n // 2, 6, 16, 1e-3, 1e3, seed=cb.SEED + 5300)
+    pats = [(rp, ci, v, cb.kkt_blocking(n, n // 2, 16))]
+    rng = np.random.default_rng(6)
+    reqs = []
+    for i in range(160):
+        vals = _ipm_values(rp, ci, v, n, rng)
+        reqs.append((0, vals, rng.standard_normal((len(rp) - 1, 8 if i % 10 else 7))))
+    mixed, s = _serve(pats, reqs, slots=1, max_batch=512)
+    assert s.stats()["batches"] == 1  # one batch of 1264 right-hand sides
+    for k in (0, 9, 10, 159):
+        alone, _ = _serve(pats, [reqs[k]], slots=1, max_batch=1)
+        assert np.array_equal(mixed[k][1], alone[0][1])
+        assert np.allclose(mixed[k][0], alone[0][0], rtol=1e-9, atol=1e-12)
+
+
 def test_server_memory_budget_serializes_but_completes():
     pats = _patterns(2, seed=41)
     reqs = _requests(pats, 6, seed=2)
