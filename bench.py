@@ -56,6 +56,8 @@ def _parse():
     ap.add_argument("--patterns", type=int, default=64, help="--config served: sparsity patterns")
     ap.add_argument("--precision", default="f32", choices=["f32", "f64"],
                     help="--config served: factor precision (f32: FP32 factor and applies, FP64 SQMR)")
+    ap.add_argument("--refine", type=int, default=0,
+                    help="--config served: FP64 refinement corrections per right-hand side (0: none)")
     ap.add_argument("--large-rows", type=int, default=131072,
                     help="--config served: patterns with N >= this use the whole-GPU solver")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -960,6 +962,7 @@ def run_served(args):
 
     srv = cb.Server(local, 0, 3, 512, 1e-8, args.max_it)
     srv.set_large_rows(args.large_rows)
+    srv.set_refine(args.refine, 1e-6)
     t0 = time.perf_counter()
     prec = cb.F32 if args.precision == "f32" else cb.F64
     pids = [srv.add_pattern(rp, ci, bs, prec) for rp, ci, v, bs, n in pats]
@@ -1009,7 +1012,8 @@ def run_served(args):
                                f"1-8 RHS, H *= 10^U(-1,1) clipped [1e-8,1e8] per request",
                    "solver": f"server: 3 slots; patterns with N < {args.large_rows}: batched SQMR, one CTA per right-hand "
                              f"side; larger: the whole-GPU solver, right-hand sides in groups of up to 4, in "
-                             f"exclusive batches; tol 1e-8, max_it {args.max_it}", "parallelism": "one GPU"},
+                             f"exclusive batches; tol 1e-8, max_it {args.max_it}; FP64 refinement: "
+                             f"{args.refine} corrections at most (inner tol 1e-6)", "parallelism": "one GPU"},
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                        "mean": float(lat.mean()), "max": float(lat.max())},
         "right_hand_sides": nrhs_tot, "converged_fraction": conv / max(nrhs_tot, 1),

@@ -455,6 +455,10 @@ class Server:
         capi.call("culipx_server_launch_count", self._h, ctypes.byref(v))
         return v.value
 
+    def set_refine(self, max_refine: int, inner_tol: float = 1e-6):
+        """FP64 refinement of every request to the server's tol (0: off)."""
+        capi.call("culipx_server_set_refine", self._h, int(max_refine), float(inner_tol))
+
     def set_large_rows(self, rows: int):
         """Patterns with n >= rows are solved by the whole-GPU solver."""
         capi.call("culipx_server_set_large_rows", self._h, int(rows))

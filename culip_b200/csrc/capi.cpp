@@ -617,6 +617,11 @@ CULIPX_API int culipx_server_set_large_rows(culipx_server s, int rows)
     return server_set_large_rows(s, rows);
 }
 
+CULIPX_API int culipx_server_set_refine(culipx_server s, int max_refine, double inner_tol)
+{
+    return server_set_refine(s, max_refine, inner_tol);
+}
+
 CULIPX_API int culipx_server_launch_count(culipx_server s, long long* count)
 {
     return server_launch_count(s, count);

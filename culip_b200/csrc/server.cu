@@ -35,6 +35,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cmath>
 #include <cstring>
 
 namespace culipx {
@@ -47,16 +48,67 @@ __global__ void k_to_f32(const double* __restrict__ in, float* __restrict__ out,
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += stride) out[i] = (float)in[i];
 }
 
+// one right-hand side of a refinement round: x += d (if d), r = b - K x, ||r||^2
+struct ResJob {
+    const int* rowptr;
+    const int* colidx;
+    const double* val;
+    const double* b;
+    const double* d;
+    double* x;
+    double* r;
+    long long n;
+};
+
+constexpr int kResT = 256;
+
+__global__ void k_add_corrections(const ResJob* __restrict__ jobs, int num)
+{
+    for (int j = blockIdx.x; j < num; j += gridDim.x) {
+        const ResJob J = jobs[j];
+        if (J.d)
+            for (long long i = threadIdx.x; i < J.n; i += kResT) J.x[i] += J.d[i];
+    }
+}
+
+// one CTA per right-hand side; the sum of squares in a fixed order
+__global__ void k_residuals(const ResJob* __restrict__ jobs, int num, double* __restrict__ sumsq)
+{
+    __shared__ double sh[kResT / 32];
+    for (int j = blockIdx.x; j < num; j += gridDim.x) {
+        const ResJob J = jobs[j];
+        double t = 0.0;
+        for (long long i = threadIdx.x; i < J.n; i += kResT) {
+            double acc = 0.0;
+            for (int k = __ldg(J.rowptr + i); k < __ldg(J.rowptr + i + 1); ++k)
+                acc = fma_rn(__ldg(J.val + k), J.x[__ldg(J.colidx + k)], acc);
+            const double ri = J.b[i] - acc;
+            J.r[i] = ri;
+            t = fma_rn(ri, ri, t);
+        }
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+        if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = t;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double u = 0.0;
+            for (int w = 0; w < kResT / 32; ++w) u += sh[w];
+            sumsq[j] = u;
+        }
+        __syncthreads();
+    }
+}
+
 double now_ms()
 {
     using namespace std::chrono;
     return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
 }
 
-long long request_bytes(const ServerPattern& sp, int nrhs)
+long long request_bytes(const ServerPattern& sp, int nrhs, bool refine)
 {
     const long long n = sp.n;
     long long b = sp.nnz * 8 + 2 * n * nrhs * 8 + (long long)(7 * n + 8) * nrhs * 8 + 4096;
+    if (refine) b += 2 * n * nrhs * 8;
     if (sp.precision == CULIPX_F32) b += sp.nnz * 4;
     return b;
 }
@@ -118,7 +170,7 @@ Server::~Server()
         if (sl.h && sl.h->stream) cudaStreamSynchronize(sl.h->stream);
     }
     for (auto& r : requests)
-        for (void* p : {r.second.d_vals, r.second.d_vals32, r.second.d_b, r.second.d_x})
+        for (void* p : {r.second.d_vals, r.second.d_vals32, r.second.d_b, r.second.d_x, r.second.d_r, r.second.d_d})
             if (p) cudaFree(p);
     for (auto& sp : patterns) {
         for (Factor* f : sp.free_factors) delete static_cast<culipx_factor_t*>(f);
@@ -127,7 +179,9 @@ Server::~Server()
     for (auto& sl : slots) {
         if (sl.out_host) cudaFreeHost(sl.out_host);
         if (sl.x_host) cudaFreeHost(sl.x_host);
+        if (sl.res_host) cudaFreeHost(sl.res_host);
         if (sl.done) cudaEventDestroy(sl.done);
+        sl.jobs.release();  // charged to sl.h, released before it
         if (sl.h) {
             delete sl.h->sqmr;
             if (sl.h->stream) cudaStreamDestroy(sl.h->stream);
@@ -172,7 +226,7 @@ int server_submit(Server* s, int pid, const double* vals, int nrhs, const double
     if (!s || !vals || !b || !request_id || nrhs < 1) return fail(CULIPX_INVALID_ARG, "culipx_server_submit: bad argument");
     if (pid < 0 || pid >= (int)s->patterns.size()) return fail(CULIPX_INVALID_ARG, "culipx_server_submit: unknown pattern %d", pid);
     const ServerPattern& sp = s->patterns[pid];
-    if (s->budget > 0 && request_bytes(sp, nrhs) > s->budget)
+    if (s->budget > 0 && request_bytes(sp, nrhs, s->max_refine > 0) > s->budget)
         return fail(CULIPX_OOM, "culipx_server_submit: the request alone exceeds the memory budget");
     ServerRequest r;
     r.id = s->next_id++;
@@ -204,6 +258,15 @@ int server_launch_count(Server* s, long long* out)
     return CULIPX_OK;
 }
 
+int server_set_refine(Server* s, int max_refine, double inner_tol)
+{
+    if (!s || max_refine < 0 || !(inner_tol >= 0.0))
+        return fail(CULIPX_INVALID_ARG, "culipx_server_set_refine: bad argument");
+    s->max_refine = max_refine;
+    s->inner_tol = inner_tol;
+    return CULIPX_OK;
+}
+
 int server_set_large_rows(Server* s, int rows)
 {
     if (!s || rows < 1) return fail(CULIPX_INVALID_ARG, "culipx_server_set_large_rows: bad argument");
@@ -230,7 +293,14 @@ int finish_slot(Server* s, ServerSlot& sl)
         const ServerPattern& sp = s->patterns[r.pid];
         r.its.resize(r.nrhs);
         r.status.resize(r.nrhs);
-        many_results(r.nrhs, s->max_it, sl.out_host + (size_t)k * 8, nullptr, r.its.data(), r.status.data());
+        if (s->max_refine > 0 && (int)r.its_acc.size() == r.nrhs) {
+            for (int c = 0; c < r.nrhs; ++c) {
+                r.its[c] = r.its_acc[c];
+                r.status[c] = r.broke[c] ? CULIPX_BREAKDOWN : (r.rel[c] <= s->tol ? CULIPX_OK : CULIPX_MAXIT);
+            }
+        } else {
+            many_results(r.nrhs, s->max_it, sl.out_host + (size_t)k * 8, nullptr, r.its.data(), r.status.data());
+        }
         k += r.nrhs;
         r.x.assign(sl.x_host + xo, sl.x_host + xo + (size_t)sp.n * r.nrhs);
         xo += (size_t)sp.n * r.nrhs;
@@ -249,6 +319,113 @@ int finish_slot(Server* s, ServerSlot& sl)
     sl.busy = false;
     sl.large = false;
     return CULIPX_OK;
+}
+
+// the batch's end on its stream: solutions to the pinned buffer, request
+// buffers back to the pool, the completion event
+int enqueue_end(Server* s, ServerSlot& sl)
+{
+    cudaStream_t st = sl.h->stream;
+    size_t xo = 0;
+    for (int id : sl.reqs) {
+        ServerRequest& r = s->requests.at(id);
+        const size_t nb = (size_t)s->patterns[r.pid].n * r.nrhs;
+        CULIPX_CUDA(cudaMemcpyAsync(sl.x_host + xo, r.d_x, nb * sizeof(double), cudaMemcpyDeviceToHost, st));
+        xo += nb;
+        for (void** p : {&r.d_vals, &r.d_vals32, &r.d_b, &r.d_x, &r.d_r, &r.d_d})
+            if (*p) {
+                CULIPX_CUDA(cudaFreeAsync(*p, st));
+                *p = nullptr;
+            }
+    }
+    CULIPX_CUDA(cudaEventRecord(sl.done, st));
+    return CULIPX_OK;
+}
+
+// r = b - K x for the right-hand sides in sl.cols (after x += d when add),
+// their sums of squares to the pinned buffer, then the completion event
+int enqueue_residuals(Server* s, ServerSlot& sl, bool add)
+{
+    cudaStream_t st = sl.h->stream;
+    const int num = (int)sl.cols.size();
+    std::vector<ResJob> jobs(num);
+    for (int i = 0; i < num; ++i) {
+        ServerRequest& r = s->requests.at(sl.cols[i].first);
+        const size_t c = sl.cols[i].second, n = s->patterns[r.pid].n;
+        const Csr& A = sl.csrs[r.q];
+        jobs[i] = ResJob{A.rowptr, A.colidx, static_cast<const double*>(A.val), static_cast<const double*>(r.d_b) + c * n,
+                         add ? static_cast<const double*>(r.d_d) + c * n : nullptr, static_cast<double*>(r.d_x) + c * n,
+                         static_cast<double*>(r.d_r) + c * n, (long long)n};
+    }
+    const size_t need = (size_t)num * (sizeof(ResJob) + sizeof(double)) + 64;
+    if (sl.jobs.bytes() < need) CULIPX_TRY(sl.jobs.alloc(sl.h, 2 * need));
+    ResJob* d_jobs = sl.jobs.as<ResJob>();
+    double* d_sum = reinterpret_cast<double*>(d_jobs + num);
+    CULIPX_CUDA(cudaMemcpyAsync(d_jobs, jobs.data(), (size_t)num * sizeof(ResJob), cudaMemcpyHostToDevice, st));
+    if (add) {
+        k_add_corrections<<<std::min(num, 148 * 8), kResT, 0, st>>>(d_jobs, num);
+        sl.h->launches += 1;
+        CULIPX_TRY(launch_check("k_add_corrections"));
+    }
+    k_residuals<<<std::min(num, 148 * 8), kResT, 0, st>>>(d_jobs, num, d_sum);
+    sl.h->launches += 1;
+    CULIPX_TRY(launch_check("k_residuals"));
+    if (sl.res_cap < (size_t)num) {
+        if (sl.res_host) cudaFreeHost(sl.res_host);
+        sl.res_host = nullptr;
+        CULIPX_CUDA(cudaMallocHost(&sl.res_host, (size_t)num * sizeof(double)));
+        sl.res_cap = num;
+    }
+    CULIPX_CUDA(cudaMemcpyAsync(sl.res_host, d_sum, (size_t)num * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CULIPX_CUDA(cudaEventRecord(sl.done, st));
+    return CULIPX_OK;
+}
+
+// A refinement round finished: take the last solves' iterations and the new
+// residuals; right-hand sides still above tol (and below max_refine
+// corrections, without breakdown) get a correction d = SQMR(K, M, r,
+// inner_tol), then x += d and new residuals; otherwise the batch ends.
+int refine_step(Server* s, ServerSlot& sl)
+{
+    std::vector<std::pair<int, int>> next;
+    for (size_t i = 0; i < sl.cols.size(); ++i) {
+        ServerRequest& r = s->requests.at(sl.cols[i].first);
+        const int c = sl.cols[i].second;
+        const double* o = sl.out_host + 8 * i;
+        r.its_acc[c] += (int)o[1];
+        if (o[2] != 0.0) r.broke[c] = 1;
+        r.rel[c] = r.bnorm[c] > 0.0 ? std::sqrt(sl.res_host[i]) / r.bnorm[c] : 0.0;
+        if (!std::isfinite(r.rel[c])) r.broke[c] = 1;
+        if (!r.broke[c] && r.rel[c] > s->tol && r.steps[c] < s->max_refine) next.push_back(sl.cols[i]);
+    }
+    if (next.empty()) {
+        sl.phase = 0;
+        return enqueue_end(s, sl);
+    }
+    const int num = (int)next.size();
+    std::vector<Csr*> As(num);
+    std::vector<Factor*> Ms(num);
+    std::vector<const double*> bs(num);
+    std::vector<double*> xs(num);
+    for (int i = 0; i < num; ++i) {
+        ServerRequest& r = s->requests.at(next[i].first);
+        const size_t c = next[i].second, n = s->patterns[r.pid].n;
+        r.steps[c] += 1;
+        As[i] = &sl.csrs[r.q];
+        Ms[i] = r.F;
+        bs[i] = static_cast<const double*>(r.d_r) + c * n;
+        xs[i] = static_cast<double*>(r.d_d) + c * n;
+    }
+    if (sl.large) {
+        for (int i = 0; i < num; ++i)
+            CULIPX_TRY(sqmr_solve_multi_async(sl.h, As[i], Ms[i], 1, bs[i], xs[i], s->inner_tol, s->max_it, sl.h->sqmr,
+                                              sl.out_host + (size_t)8 * i));
+    } else {
+        CULIPX_TRY(sqmr_solve_many_nr_async(sl.h, num, As.data(), Ms.data(), bs.data(), xs.data(), nullptr,
+                                            s->inner_tol, s->max_it, sl.h->sqmr, sl.out_host));
+    }
+    sl.cols = next;
+    return enqueue_residuals(s, sl, true);
 }
 
 int launch_slot(Server* s, ServerSlot& sl)
@@ -275,7 +452,7 @@ int launch_slot(Server* s, ServerSlot& sl)
         }
         ServerRequest& r = s->requests.at(id);
         const ServerPattern& sp = s->patterns[r.pid];
-        const long long need = request_bytes(sp, r.nrhs);
+        const long long need = request_bytes(sp, r.nrhs, s->max_refine > 0);
         const long long fbytes = sp.free_factors.empty() ? sp.factor_bytes_estimate() : 0;
         const bool fits = s->budget <= 0 || s->fixed_bytes() + s->in_use + need + fbytes <= s->budget;
         // over the budget: wait for running batches to free memory (a request
@@ -330,6 +507,21 @@ int launch_slot(Server* s, ServerSlot& sl)
         CULIPX_CUDA(cudaMallocAsync(&r.d_vals, std::max<size_t>(nv, 1) * sizeof(double), st));
         CULIPX_CUDA(cudaMallocAsync(&r.d_b, nb * sizeof(double), st));
         CULIPX_CUDA(cudaMallocAsync(&r.d_x, nb * sizeof(double), st));
+        if (s->max_refine > 0) {
+            CULIPX_CUDA(cudaMallocAsync(&r.d_r, nb * sizeof(double), st));
+            CULIPX_CUDA(cudaMallocAsync(&r.d_d, nb * sizeof(double), st));
+            r.bnorm.assign(r.nrhs, 0.0);
+            for (int c = 0; c < r.nrhs; ++c) {
+                double t = 0.0;
+                for (size_t i = 0; i < (size_t)sp.n; ++i) t += r.b[c * (size_t)sp.n + i] * r.b[c * (size_t)sp.n + i];
+                r.bnorm[c] = std::sqrt(t);
+            }
+            r.rel.assign(r.nrhs, 1.0);
+            r.steps.assign(r.nrhs, 0);
+            r.its_acc.assign(r.nrhs, 0);
+            r.broke.assign(r.nrhs, 0);
+        }
+        r.q = (int)(sl.csrs.size());
         CULIPX_CUDA(cudaMemcpyAsync(r.d_vals, r.vals.data(), nv * sizeof(double), cudaMemcpyHostToDevice, st));
         CULIPX_CUDA(cudaMemcpyAsync(r.d_b, r.b.data(), nb * sizeof(double), cudaMemcpyHostToDevice, st));
         const void* fv = r.d_vals;
@@ -367,8 +559,6 @@ int launch_slot(Server* s, ServerSlot& sl)
                                               sl.out_host + (size_t)k * 8));
             k += r.nrhs;
         }
-        sl.order.resize(k);
-        for (int i = 0; i < k; ++i) sl.order[i] = i;
         ++s->large_batches;
     }
     if (!large) {
@@ -396,27 +586,21 @@ int launch_slot(Server* s, ServerSlot& sl)
         }
         CULIPX_TRY(sqmr_solve_many_nr_async(sl.h, (int)As.size(), As.data(), Ms.data(), bs.data(), xs.data(),
                                             nrs.data(), s->tol, s->max_it, sl.h->sqmr, sl.out_host));
-        sl.order.resize(systems);
-        for (int i = 0; i < systems; ++i) sl.order[i] = i;
     }
-    size_t xo = 0;
-    for (int id : admit) {
-        ServerRequest& r = s->requests.at(id);
-        const size_t nb = (size_t)s->patterns[r.pid].n * r.nrhs;
-        CULIPX_CUDA(cudaMemcpyAsync(sl.x_host + xo, r.d_x, nb * sizeof(double), cudaMemcpyDeviceToHost, st));
-        xo += nb;
-        for (void** p : {&r.d_vals, &r.d_vals32, &r.d_b, &r.d_x})
-            if (*p) {
-                CULIPX_CUDA(cudaFreeAsync(*p, st));
-                *p = nullptr;
-            }
-    }
-    CULIPX_CUDA(cudaEventRecord(sl.done, st));
     sl.reqs = admit;
     sl.busy = true;
     sl.large = large;
     ++s->batches;
-    return CULIPX_OK;
+    if (s->max_refine > 0) {
+        // FP64 refinement: the true residuals of every right-hand side next
+        sl.cols.clear();
+        for (int id : admit)
+            for (int c = 0; c < s->requests.at(id).nrhs; ++c) sl.cols.emplace_back(id, c);
+        sl.phase = 1;
+        return enqueue_residuals(s, sl, false);
+    }
+    sl.phase = 0;
+    return enqueue_end(s, sl);
 }
 
 }  // namespace
@@ -448,11 +632,10 @@ int server_progress(Server* s, int wait, int* completed)
                 const cudaError_t e = cudaEventQuery(sl.done);
                 if (e == cudaSuccess) {
                     CULIPX_TRY(launch_check("server batch"));
-                    // undo the precision-group order of the results
-                    std::vector<double> tmp(sl.order.size() * 8);
-                    for (size_t i = 0; i < sl.order.size(); ++i)
-                        std::memcpy(tmp.data() + (size_t)sl.order[i] * 8, sl.out_host + i * 8, 8 * sizeof(double));
-                    std::memcpy(sl.out_host, tmp.data(), tmp.size() * sizeof(double));
+                    if (sl.phase == 1) {
+                        CULIPX_TRY(refine_step(s, sl));  // a refinement round: corrections or the end
+                        continue;
+                    }
                     CULIPX_TRY(finish_slot(s, sl));
                 } else if (e != cudaErrorNotReady) {
                     return fail(CULIPX_CUDA_ERROR, "server batch failed: %s", cudaGetErrorString(e));

@@ -35,6 +35,14 @@ struct ServerRequest {
     long long bytes = 0;                   // device bytes while running
     Factor* F = nullptr;
     void *d_vals = nullptr, *d_vals32 = nullptr, *d_b = nullptr, *d_x = nullptr;
+    // FP64 refinement (Server::max_refine > 0): residuals, corrections, and
+    // per right-hand side ||b||, the last relative residual, corrections taken,
+    // SQMR iterations summed, breakdown seen
+    void *d_r = nullptr, *d_d = nullptr;
+    int q = -1;                            // position in the running batch
+    std::vector<double> bnorm, rel;
+    std::vector<int> steps, its_acc;
+    std::vector<char> broke;
 };
 
 struct ServerSlot {
@@ -44,11 +52,15 @@ struct ServerSlot {
     bool large = false;                    // the running batch is of whole-GPU solves
     std::vector<int> reqs;
     std::vector<Csr> csrs;
-    std::vector<int> order;                // precision-group order of the systems
     double* out_host = nullptr;            // pinned: 8 values per system
     int out_cap = 0;
     double* x_host = nullptr;              // pinned: the batch's solutions
     size_t x_cap = 0;
+    int phase = 0;                         // 0: solving or ending; 1: residuals in flight (refinement)
+    std::vector<std::pair<int, int>> cols; // (request, column) of the last solves, in result-slot order
+    double* res_host = nullptr;            // pinned: their residuals' sums of squares
+    size_t res_cap = 0;
+    DeviceBuffer jobs;                     // device descriptors of the refinement kernels
 };
 
 struct Server {
@@ -56,6 +68,8 @@ struct Server {
     long long budget = 0, in_use = 0;
     int max_batch = 0, max_it = 0;
     int large_rows = 131072;               // patterns with n >= this get the whole-GPU solver
+    int max_refine = 0;                    // FP64 refinement corrections per right-hand side (0: none)
+    double inner_tol = 1e-6;               // SQMR tolerance of the corrections
     long long large_batches = 0;
     double tol = 0.0;
     culipx_handle_t* base = nullptr;       // owns the patterns' device mirrors
@@ -80,6 +94,7 @@ int server_release(Server* s, int id);
 int server_stats(Server* s, long long* st8);
 int server_set_large_rows(Server* s, int rows);
 int server_launch_count(Server* s, long long* out);
+int server_set_refine(Server* s, int max_refine, double inner_tol);
 int factor_compute(Factor* f, const void* d_vals, const int* h_is_piv, int pivot, double threshold);
 int factor_create(Pattern* p, Factor** out);
 

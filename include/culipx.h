@@ -320,6 +320,16 @@ int culipx_server_stats(culipx_server s, long long *stats8);
 /* requests on patterns with n >= rows use the whole-GPU solver (rows >= 1;
  * default 131072); applies to batches admitted afterwards */
 int culipx_server_set_large_rows(culipx_server s, int rows);
+/* FP64 iterative refinement of every request (the mixed-precision serving
+ * path, meant for FP32 patterns; no counterpart in the reference): after the
+ * solve, r = b - K x in FP64 per right-hand side; while ||r|| > tol ||b|| and
+ * fewer than max_refine corrections: d = SQMR(K, M, r, inner_tol), x += d, new
+ * r.  Corrections of a batch's right-hand sides run together.  Then the
+ * request's iterations are the SQMR iterations summed and its status OK when
+ * ||b - K x|| <= tol ||b||, else MAXIT (BREAKDOWN if a solve broke down).
+ * max_refine 0 (the default) turns it off; applies to batches admitted
+ * afterwards. */
+int culipx_server_set_refine(culipx_server s, int max_refine, double inner_tol);
 /* kernels the server has launched so far (all slots) */
 int culipx_server_launch_count(culipx_server s, long long *count);
 

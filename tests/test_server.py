@@ -156,6 +156,42 @@ def test_server_grouped_right_hand_sides():
         assert np.allclose(mixed[k][0], alone[0][0], rtol=1e-9, atol=1e-12)
 
 
+@pytest.mark.parametrize("large_rows", [None, 1000])
+def test_server_fp32_refined(large_rows):
+    """FP32 factors with FP64 refinement: every right-hand side ends with a
+    true relative residual at most tol (1e-8), computed here in FP64; the
+    same alone and in the mix."""
+    import scipy.sparse as sp
+
+    pats = []
+    for k, n in enumerate((400, 900)):  # N = 600, 1350
+        rp, ci, v = cb.kkt_generate(n, n // 2, 6, 16, 1e-3, 1e3, seed=cb.SEED + 5400 + k)
+        pats.append((rp, ci, v, cb.kkt_blocking(n, n // 2, 16)))
+    reqs = _requests(pats, 6, seed=7)
+
+    def serve(rq, slots, mb):
+        s = cb.Server(0, 0, slots, mb, 1e-8, 1000)
+        if large_rows is not None:
+            s.set_large_rows(large_rows)
+        s.set_refine(10, 1e-6)
+        pids = [s.add_pattern(rp, ci, bs, cb.F32) for rp, ci, v, bs in pats]
+        ids = [s.submit(pids[p], vals, b) for p, vals, b in rq]
+        done = 0
+        while done < len(ids):
+            done += s.progress(wait=True)
+        return [s.result(i) for i in ids]
+
+    mixed = serve(reqs, 2, 4)
+    for (p, vals, b), (x, its, status, lat) in zip(reqs, mixed):
+        rp, ci, v, bs = pats[p]
+        K = sp.csr_matrix((vals, ci, rp))
+        for r in range(b.shape[1]):
+            assert status[r] == capi.OK
+            assert np.linalg.norm(b[:, r] - K @ x[:, r]) / np.linalg.norm(b[:, r]) <= 1.0001e-8
+    alone = serve([reqs[2]], 1, 1)
+    assert np.array_equal(alone[0][0], mixed[2][0]) and np.array_equal(alone[0][1], mixed[2][1])
+
+
 def test_server_memory_budget_serializes_but_completes():
     pats = _patterns(2, seed=41)
     reqs = _requests(pats, 6, seed=2)
