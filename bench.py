@@ -64,6 +64,7 @@ def _parse():
     ap.add_argument("--max-it", type=int, default=1000, help="SQMR iteration cap (1000 = the driver's setting)")
     ap.add_argument("--batch", type=int, default=512, help="systems in --config batch")
     ap.add_argument("--max-refine", type=int, default=10, help="--config mixed / batch: refinement corrections")
+    ap.add_argument("--tune", type=int, default=1, help="--config batch: 1 = block size from culipx_tune_kkt_block")
     return ap.parse_args()
 
 
@@ -786,7 +787,7 @@ def run_spmv(args):
         print(json.dumps(out), flush=True)
 
 
-def batch_systems(num=512, seed_base=None):
+def batch_systems(num=512, seed_base=None, block=32):
     """The batched workload: num KKT systems, system i from sub-seed
     SEED + 4000 + i, n uniform in [500, 20000], m = n // 2, A with 4-8
     nonzeros per column (half in a band of half-width 32, half uniform),
@@ -800,8 +801,40 @@ def batch_systems(num=512, seed_base=None):
         m = n // 2
         k = int(rng.integers(4, 9))
         rp, ci, v = cb.kkt_generate(n, m, k, 32, 1e-4, 1e4, seed=cb.SEED + 4000 + i)
-        out.append((rp, ci, v, cb.kkt_blocking(n, m, 32)))
+        out.append((rp, ci, v, cb.kkt_blocking(n, m, block)))
     return out
+
+
+def tune_batch_block(args, local, candidates=(8, 16, 24, 32), samples=(0, 128, 256, 384)):
+    """Block size for the batched workload from culipx_tune_kkt_block on a
+    sample of its systems (FP32 factor, tol 1e-8, max_it): the candidate
+    whose solves met tol most often, then the least summed time (when none
+    met it: the smallest residual estimates, the better start for refinement)."""
+    import torch
+
+    import culip_b200 as cb
+
+    h = cb.Handle(local)
+    rng = np.random.default_rng(cb.SEED + 4000)
+    dims = [(int(rng.integers(500, 20001)), int(rng.integers(4, 9))) for _ in range(args.batch)]
+    score = {c: [0, 0.0, 0.0] for c in candidates}
+    for i in samples:
+        if i >= args.batch:
+            continue
+        n, k = dims[i]
+        rp, ci, v = cb.kkt_generate(n, n // 2, k, 32, 1e-4, 1e4, seed=cb.SEED + 4000 + i)
+        b = cb.normal_vector(cb.SEED + 4000 + 100000 + i, len(rp) - 1)
+        _, res = cb.tune_kkt_block(h, n, n // 2, rp, ci, torch.from_numpy(v).cuda(), torch.from_numpy(b).cuda(),
+                                   cb.F32, candidates, 1e-8, args.max_it)
+        for c, (ms, its, st, rr) in res.items():
+            score[c][0] += int(st == 0)
+            score[c][1] += ms
+            score[c][2] += np.log10(max(rr, 1e-300))
+    # most converged; then, if some converged, the least time, else the smallest residuals
+    any_converged = max(score[c][0] for c in candidates) > 0
+    best = min(candidates, key=lambda c: (-score[c][0], score[c][1] if any_converged else score[c][2]))
+    return best, {str(c): {"converged": score[c][0], "ms": round(score[c][1], 3),
+                           "mean_log10_residual": round(score[c][2] / len(samples), 3)} for c in candidates}
 
 
 def run_batch(args):
@@ -815,7 +848,10 @@ def run_batch(args):
 
     world, rank, local = _dist()
     torch.cuda.set_device(local)
-    syst = batch_systems(args.batch)
+    block, tuning = 32, None
+    if args.tune:
+        block, tuning = tune_batch_block(args, local)
+    syst = batch_systems(args.batch, block=block)
     rp, ci, v, bs, off = cb.union_systems(syst)
     N, nnz = len(rp) - 1, len(ci)
     b = np.concatenate([cb.normal_vector(cb.SEED + 4000 + 100000 + i, len(sy[0]) - 1) for i, sy in enumerate(syst)])
@@ -888,7 +924,10 @@ def run_batch(args):
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 factor / f64 refinement", "data": "synthetic (seeded KKT generator)",
         "config": {"workload": f"{num} KKT systems, n U[500,20000], m=n/2, A 4-8/col (band_half=32), "
-                               f"H log-U[1e-4,1e4], blocks 32, BK, fill 0; union N={N} nnz={nnz}",
+                               f"H log-U[1e-4,1e4], blocks {block} "
+                               f"({'culipx_tune_kkt_block on 4 sample systems' if tuning else 'fixed'}), BK, fill 0; "
+                               f"union N={N} nnz={nnz}",
+                   "block_tuning": tuning,
                    "solver": f"batched SQMR (one CTA per system), inner tol {inner_tol:g} max_it {inner_it}, "
                              f"FP64 refinement to {tol:g}, at most {max_ref} corrections",
                    "l2": L2Flush.NOTE,

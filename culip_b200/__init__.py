@@ -470,6 +470,23 @@ class Server:
             pass
 
 
+def tune_kkt_block(handle: Handle, n, m, rowptr, colidx, vals, b, precision=F32, candidates=(8, 16, 24, 32),
+                   tol=1e-8, max_it=1000):
+    """Block size for culipx_kkt_blocking of this KKT pattern (n H rows, m
+    constraint rows): vals, b torch float64 CUDA tensors, rowptr / colidx host
+    arrays.  Returns (best_block, {block: (ms, iterations, status, residual)})."""
+    rp = np.ascontiguousarray(rowptr, np.int32)
+    ci = np.ascontiguousarray(colidx, np.int32)
+    cand = np.ascontiguousarray(candidates, np.int32)
+    k = len(cand)
+    ms, its, st, res = np.zeros(k), np.zeros(k, np.int32), np.zeros(k, np.int32), np.zeros(k)
+    best = ctypes.c_int()
+    capi.call("culipx_tune_kkt_block", handle._h, int(n), int(m), _p(rp), _p(ci), _dptr(vals), _dptr(b),
+              int(precision), _p(cand), k, float(tol), int(max_it), ctypes.byref(best), _p(ms), _p(its), _p(st),
+              _p(res))
+    return best.value, {int(c): (float(ms[i]), int(its[i]), int(st[i]), float(res[i])) for i, c in enumerate(cand)}
+
+
 def sqmr_solve_multi(handle: Handle, A: CsrOperator, M: Factor, B, X, tol=1e-8, max_it=1000):
     """Several right-hand sides of one system: B, X torch float64 CUDA tensors
     of shape (nrhs, n) (row k = right-hand side k, i.e. n x nrhs column-major).

@@ -95,6 +95,7 @@ _SIGS = {
     "culipx_server_set_large_rows": [vp, i32],
     "culipx_server_launch_count": [vp, vp],
     "culipx_server_set_refine": [vp, i32, f64],
+    "culipx_tune_kkt_block": [vp, i32, i32, vp, vp, vp, vp, i32, vp, i32, f64, i32, vp, vp, vp, vp, vp],
     "culipx_batch_sqmr_refine": [vp, vp, vp, vp, vp, f64, f64, i32, i32, vp, vp, vp, vp],
     "culipx_sqmr_refine": [vp, vp, vp, vp, vp, f64, f64, i32, i32, ctypes.POINTER(f64), ctypes.POINTER(i32),
                            ctypes.POINTER(i32)],

@@ -617,6 +617,19 @@ CULIPX_API int culipx_server_set_large_rows(culipx_server s, int rows)
     return server_set_large_rows(s, rows);
 }
 
+CULIPX_API int culipx_tune_kkt_block(culipx_handle h, int n, int m, const int* h_rowptr, const int* h_colidx,
+                                     const double* d_vals, const double* d_b, int precision, const int* candidates,
+                                     int num_candidates, double tol, int max_it, int* best_block, double* h_ms,
+                                     int* h_iterations, int* h_status, double* h_residual)
+{
+    if (!h) return fail(CULIPX_INVALID_ARG, "null handle");
+    GUARD_BEGIN
+    CULIPX_TRY(use_device(h));
+    return tune_kkt_block(h, n, m, h_rowptr, h_colidx, d_vals, d_b, precision, candidates, num_candidates, tol,
+                          max_it, best_block, h_ms, h_iterations, h_status, h_residual);
+    GUARD_END
+}
+
 CULIPX_API int culipx_server_set_refine(culipx_server s, int max_refine, double inner_tol)
 {
     return server_set_refine(s, max_refine, inner_tol);

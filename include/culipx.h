@@ -320,6 +320,22 @@ int culipx_server_stats(culipx_server s, long long *stats8);
 /* requests on patterns with n >= rows use the whole-GPU solver (rows >= 1;
  * default 131072); applies to batches admitted afterwards */
 int culipx_server_set_large_rows(culipx_server s, int rows);
+/* Block-size tuner for a KKT pattern (n H rows, m constraint rows; no
+ * counterpart in the reference, whose driver reads a fixed blocking from a
+ * file, apps/block_ildlt/block_ildlt.cc:29-35): for each candidate size the
+ * contiguous KKT blocking (culipx_kkt_blocking), symbolic analysis, numeric
+ * factor (precision F64 or F32, BK, level-0 fill) and one SQMR solve of d_b
+ * (tol, max_it), timed with CUDA events on the handle's stream after one
+ * warm-up run.  best_block = the fastest candidate whose solve met tol, else
+ * the one with the smallest final SQMR residual estimate.  Per candidate: the
+ * factor + solve time in ms, iterations, status (OK, MAXIT, BREAKDOWN) and
+ * the residual estimate; each output array may be NULL.  Synchronizes the
+ * stream. */
+int culipx_tune_kkt_block(culipx_handle h, int n, int m, const int *h_rowptr, const int *h_colidx,
+                          const double *d_vals, const double *d_b, int precision, const int *candidates,
+                          int num_candidates, double tol, int max_it, int *best_block, double *h_ms,
+                          int *h_iterations, int *h_status, double *h_residual);
+
 /* FP64 iterative refinement of every request (the mixed-precision serving
  * path, meant for FP32 patterns; no counterpart in the reference): after the
  * solve, r = b - K x in FP64 per right-hand side; while ||r|| > tol ||b|| and
