@@ -470,6 +470,34 @@ class Server:
             pass
 
 
+class KktOperator:
+    """AugmentedMatrixSPMV / NormalMatrixSPMV (FP64): A is the m x n
+    constraint matrix (torch CUDA CSR arrays), d the diagonal D (n), ix the
+    constraint rows that get delta (torch int32 CUDA tensor or None)."""
+
+    AUGMENTED, NORMAL = 0, 1
+
+    def __init__(self, handle: Handle, kind, m, n, rowptr, colidx, val, d, delta=0.0, ix=None):
+        self.handle = handle
+        self._keep = (rowptr, colidx, val, d, ix)
+        self.kind, self.m, self.n = kind, m, n
+        op = ctypes.c_void_p()
+        capi.call("culipx_kkt_operator_create", handle._h, int(kind), int(m), int(n), int(colidx.numel()),
+                  _dptr(rowptr), _dptr(colidx), _dptr(val), _dptr(d), float(delta),
+                  0 if ix is None else int(ix.numel()), None if ix is None else _dptr(ix), ctypes.byref(op))
+        self._h = op
+
+    def multiply(self, x, y, alpha=1.0, beta=0.0):
+        capi.call("culipx_kkt_operator_multiply", self._h, _dptr(x), _dptr(y), float(alpha), float(beta))
+        return y
+
+    def __del__(self):
+        try:
+            _release(self, "culipx_kkt_operator_destroy")
+        except Exception:  # interpreter shutdown
+            pass
+
+
 def tune_kkt_block(handle: Handle, n, m, rowptr, colidx, vals, b, precision=F32, candidates=(8, 16, 24, 32),
                    tol=1e-8, max_it=1000):
     """Block size for culipx_kkt_blocking of this KKT pattern (n H rows, m

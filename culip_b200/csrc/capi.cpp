@@ -1,5 +1,6 @@
 // extern "C" entry points of libculipx (declared in include/culipx.h).
 #include "factor.h"
+#include "operators.h"
 #include "pattern.h"
 #include "permute.h"
 #include "server.h"
@@ -615,6 +616,40 @@ CULIPX_API int culipx_server_stats(culipx_server s, long long* stats8)
 CULIPX_API int culipx_server_set_large_rows(culipx_server s, int rows)
 {
     return server_set_large_rows(s, rows);
+}
+
+CULIPX_API int culipx_kkt_operator_create(culipx_handle h, int kind, int m, int n, long long nnz, const int* d_rowptr,
+                                         const int* d_colidx, const double* d_val, const double* d_d, double delta,
+                                         int num_ix, const int* d_ix, culipx_kkt_operator* out)
+{
+    if (!h || !out) return fail(CULIPX_INVALID_ARG, "culipx_kkt_operator_create: null argument");
+    if (h->device < 0) return fail(CULIPX_INVALID_ARG, "culipx_kkt_operator_create: host-only handle");
+    GUARD_BEGIN
+    CULIPX_TRY(use_device(h));
+    KktOperator* op = nullptr;
+    CULIPX_TRY(kkt_operator_create(h, kind, m, n, nnz, d_rowptr, d_colidx, d_val, d_d, delta, num_ix, d_ix, &op));
+    *out = static_cast<culipx_kkt_operator>(op);
+    return CULIPX_OK;
+    GUARD_END
+}
+
+CULIPX_API int culipx_kkt_operator_multiply(culipx_kkt_operator op, const double* d_x, double* d_y, double alpha,
+                                           double beta)
+{
+    if (!op) return fail(CULIPX_INVALID_ARG, "null operator");
+    GUARD_BEGIN
+    CULIPX_TRY(use_device(op->h));
+    return kkt_operator_multiply(op, d_x, d_y, alpha, beta);
+    GUARD_END
+}
+
+CULIPX_API int culipx_kkt_operator_destroy(culipx_kkt_operator op)
+{
+    if (op) {
+        if (op->h->device >= 0) cudaSetDevice(op->h->device);
+        delete op;
+    }
+    return CULIPX_OK;
 }
 
 CULIPX_API int culipx_tune_kkt_block(culipx_handle h, int n, int m, const int* h_rowptr, const int* h_colidx,

@@ -320,6 +320,30 @@ int culipx_server_stats(culipx_server s, long long *stats8);
 /* requests on patterns with n >= rows use the whole-GPU solver (rows >= 1;
  * default 131072); applies to batches admitted afterwards */
 int culipx_server_set_large_rows(culipx_server s, int rows);
+/* Matrix-free KKT operators over a constraint matrix A (m x n, FP64 CSR on
+ * the device, borrowed) and a diagonal D (n, borrowed); they replace
+ * AugmentedMatrixSPMV<T> and NormalMatrixSPMV<T> (libs/la/spmv.cuh:75-149,
+ * spmv.impl.cuh:122-430), FP64:
+ *   CULIPX_OP_AUGMENTED  y = alpha [D x1 + A' x2 ; A x1 + (delta I)(ix) x2] + beta y,
+ *                        x = [x1; x2], n + m rows
+ *   CULIPX_OP_NORMAL     y = alpha (A D^-1 A' x + (delta I)(ix) x) + beta y, m rows
+ * (delta I)(ix) adds delta * x[ix[i]] at row ix[i] (ix: num_ix row indices of
+ * the constraint block, device, may be NULL with num_ix = 0).  Two
+ * differences from the reference on purpose: its augmented product adds
+ * A' x1 where A' x2 belongs (spmv.impl.cuh:416-420), and its shift multiplies
+ * x[i] instead of x[ix[i]] (k_add_app, helper_kernels.impl.cuh:361-374).
+ * create copies A to the host once to build A' (the reference's
+ * explicit_At) and synchronizes; multiply is asynchronous on the handle's
+ * stream. */
+#define CULIPX_OP_AUGMENTED 0
+#define CULIPX_OP_NORMAL 1
+typedef struct culipx_kkt_operator_t *culipx_kkt_operator;
+int culipx_kkt_operator_create(culipx_handle h, int kind, int m, int n, long long nnz, const int *d_rowptr,
+                               const int *d_colidx, const double *d_val, const double *d_d, double delta,
+                               int num_ix, const int *d_ix, culipx_kkt_operator *out);
+int culipx_kkt_operator_multiply(culipx_kkt_operator op, const double *d_x, double *d_y, double alpha, double beta);
+int culipx_kkt_operator_destroy(culipx_kkt_operator op);
+
 /* Block-size tuner for a KKT pattern (n H rows, m constraint rows; no
  * counterpart in the reference, whose driver reads a fixed blocking from a
  * file, apps/block_ildlt/block_ildlt.cc:29-35): for each candidate size the

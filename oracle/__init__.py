@@ -250,3 +250,33 @@ def permute_scale(rowptr, colidx, val, row_perm, col_perm=None, row_scale=None, 
     b_rowptr = np.zeros(n + 1, np.int32)
     np.add.at(b_rowptr, new_r + 1, 1)
     return np.cumsum(b_rowptr).astype(np.int32), new_c[order].astype(np.int32), v[order]
+
+
+def kkt_operator(kind, rowptr, colidx, val, n, d, x, delta=0.0, ix=None, alpha=1.0, beta=0.0, y=None):
+    """AugmentedMatrixSPMV<T>::multiply (kind 0) / NormalMatrixSPMV<T>::multiply
+    (kind 1), libs/la/spmv.impl.cuh:214-269 and 364-427, in FP64 with numpy,
+    for the operators those classes document (spmv.cuh:70-74, 103-107):
+      kind 0: y = alpha [D x1 + A' x2 ; A x1 + (delta I)(ix) x2] + beta y
+      kind 1: y = alpha (A D^-1 A' x + (delta I)(ix) x) + beta y
+    Where the reference's code departs from them, this follows the documented
+    operator: A' x2, not A' x1, in the augmented product (spmv.impl.cuh:416-420),
+    and the shift at row ix[i] multiplies x[ix[i]] (k_add_app,
+    helper_kernels.impl.cuh:361-374, multiplies x[i])."""
+    import scipy.sparse as sp
+
+    rowptr = np.asarray(rowptr)
+    m = len(rowptr) - 1
+    A = sp.csr_matrix((np.asarray(val, np.float64), np.asarray(colidx), rowptr), shape=(m, n))
+    d = np.asarray(d, np.float64)
+    x = np.asarray(x, np.float64)
+    shift = np.zeros(m)
+    if ix is not None:
+        shift[np.asarray(ix)] = delta
+    if kind == 0:
+        x1, x2 = x[:n], x[n:]
+        v = np.concatenate([d * x1 + A.T @ x2, A @ x1 + shift * x2])
+    else:
+        v = A @ ((A.T @ x) / d) + shift * x
+    if beta == 0.0 or y is None:
+        return alpha * v
+    return alpha * v + beta * np.asarray(y, np.float64)

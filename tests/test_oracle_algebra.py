@@ -63,3 +63,24 @@ def test_natural_kkt_two_levels_and_identity_h_blocks():
     assert np.array_equal(tri[:nH, 1], v[np.asarray([np.searchsorted(ci[rp[i]:rp[i + 1]], i) + rp[i]
                                                      for i in range(nH)])])
     assert np.all(tri[:nH, 0] == 0) and np.all(tri[:nH, 2] == 0)
+
+
+def test_kkt_operator_restatement_algebra():
+    """The augmented operator is K = [[D, A'], [A, shift]] times x, and the
+    normal operator equals its Schur complement form A D^-1 A' x + shift x."""
+    import scipy.sparse as sp
+
+    rng = np.random.default_rng(9)
+    n, m = 60, 25
+    A = sp.random(m, n, density=0.1, random_state=3, format="csr")
+    d = 10.0 ** rng.uniform(-2, 2, n)
+    ix = np.array([0, 4, 7, 24])
+    x = rng.standard_normal(n + m)
+    shift = np.zeros(m)
+    shift[ix] = 0.3
+    K = sp.bmat([[sp.diags(d), A.T], [A, sp.diags(shift)]]).tocsr()
+    got = oracle.kkt_operator(0, A.indptr, A.indices, A.data, n, d, x, 0.3, ix)
+    assert np.allclose(got, K @ x, rtol=1e-14, atol=1e-14)
+    xm = x[:m]
+    want = A @ (A.T @ xm / d) + shift * xm
+    assert np.allclose(oracle.kkt_operator(1, A.indptr, A.indices, A.data, n, d, xm, 0.3, ix), want, rtol=1e-14)
