@@ -160,6 +160,25 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def reduce_max(value, dist=None):
+    """The maximum of a float over all ranks (replicas: the job's time is its
+    slowest rank's); NCCL reduces a CUDA tensor, gloo a CPU one."""
+    if dist is None or not dist.is_initialized():
+        return float(value)
+    import torch
+
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(value)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(world, units_per_rank, max_seconds):
+    """Whole-job throughput of replicas: every rank processed units_per_rank
+    units; the job took as long as its slowest rank."""
+    return world * units_per_rank / max_seconds
+
+
 def _dist():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -231,11 +250,8 @@ def run_culipx(args):
     ck = clocks.stop()
     launches = h.launch_count(reset=True)
     step_ms = [a.elapsed_time(b2) for a, b2 in evs]
-    total_ms = float(np.sum(step_ms))
+    total_ms = reduce_max(float(np.sum(step_ms)), dist)
     if dist:
-        t = torch.tensor([total_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
         dist.barrier()
 
     # accuracy of the last step
@@ -275,14 +291,10 @@ def run_culipx(args):
         e1.record(stream)
         torch.cuda.synchronize()
         e_ms.append(e0.elapsed_time(e1))
-    e2e_total = float(np.sum(e_ms))
-    if dist:
-        t = torch.tensor([e2e_total], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_total = float(t.item())
+    e2e_total = reduce_max(float(np.sum(e_ms)), dist)
 
     fac_ms, fac_launches = F.stats()
-    value = world * args.steps / (total_ms / 1e3)
+    value = job_rate(world, args.steps, total_ms / 1e3)
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
@@ -294,7 +306,7 @@ def run_culipx(args):
         "factor_ms": fac_ms,
         "gpu_launches": int(launches),
         "clocks": ck,
-        "e2e": {"value": world * e2e_steps / (e2e_total / 1e3), "unit": UNIT,
+        "e2e": {"value": job_rate(world, e2e_steps, e2e_total / 1e3), "unit": UNIT,
                 "h2d_bytes_per_step": int(nnz * 8 + N * 8), "d2h_bytes_per_step": int(N * 8)},
         "roofline": roof,
         "spmv": spmv_roofline(A, N, nnz, flush, stream),
