@@ -160,6 +160,14 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def _host_threads():
+    """Host threads this process may use (its CPU affinity)."""
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
 def reduce_max(value, dist=None):
     """The maximum of a float over all ranks (replicas: the job's time is its
     slowest rank's); NCCL reduces a CUDA tensor, gloo a CPU one."""
@@ -391,9 +399,12 @@ def _peak_hbm():
 
 
 def cpu_baseline(name, rp, ci, v, bs, b, gpu_iters, max_seconds=25.0):
-    """Oracle (CPU restatement, 1 thread): symbolic + factor timed fully, SQMR on
+    """Oracle (CPU restatement, all host threads on its row-independent loops;
+    the factor and the dot products stay serial): symbolic + factor timed fully, SQMR on
     a bounded number of iterations, scaled to the GPU run's iteration count."""
     import oracle
+
+    cores = oracle.set_threads(_host_threads())
 
     t0 = time.perf_counter()
     S = oracle.Sym(rp, ci, bs, 0, 1.0)
@@ -406,15 +417,17 @@ def cpu_baseline(name, rp, ci, v, bs, b, gpu_iters, max_seconds=25.0):
     t4 = time.perf_counter()
     per_it = (t4 - t3) / sample_it
     solve_s = (t2 - t1) + per_it * max(gpu_iters, 1)
-    return {"value": 1.0 / solve_s, "unit": UNIT, "cores": 1, "kind": "port",
+    return {"value": 1.0 / solve_s, "unit": UNIT, "cores": cores, "kind": "port",
             "sample": f"oracle factor (full, {t2 - t1:.2f}s) + {sample_it} SQMR iterations ({t4 - t3:.2f}s) scaled to "
                       f"{gpu_iters} iterations; symbolic {t1 - t0:.2f}s not counted (cached per pattern)"}
 
 
 def run_reference_spmv(args):
-    """The CPU restatement's y = K x (serial CSR loop, 1 thread) on the same
+    """The CPU restatement's y = K x (CSR rows spread over the host threads) on the same
     matrix; value = algorithmic GB/s as in --config spmv."""
     import oracle
+
+    cores = oracle.set_threads(_host_threads())
 
     cfg, rp, ci, v, bs, _ = _workload(args.spmv_workload)
     N, nnz = len(rp) - 1, len(ci)
@@ -431,9 +444,9 @@ def run_reference_spmv(args):
     out = {"metric": "SpMV HBM GB/s (culipx_spmv, FP64 CSR, y = K x)", "value": gbs, "unit": "GB/s", "n_gpus": 1,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded KKT generator)", "impl": "reference",
-           "config": _config_dict(args.spmv_workload, cfg, nnz, {"parallelism": "one CPU thread"}, solve="y = K x only"),
-           "cpu_baseline": {"value": gbs, "unit": "GB/s", "cores": 1, "kind": "port",
-                            "sample": "oracle serial CSR product, whole matrix per step"},
+           "config": _config_dict(args.spmv_workload, cfg, nnz, {"parallelism": f"{cores} CPU threads"}, solve="y = K x only"),
+           "cpu_baseline": {"value": gbs, "unit": "GB/s", "cores": cores, "kind": "port",
+                            "sample": "oracle CSR product (rows over the host threads), whole matrix per step"},
            "e2e": {"value": gbs, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
 
@@ -444,8 +457,11 @@ def run_reference_batch(args):
     with the whole algorithm: FP64 factor (the restatement's SQMR takes an
     FP64 factor) and the same refinement loop (inner SQMR tol 1e-6, max_it,
     at most --max-refine corrections, true FP64 residual, target 1e-8);
-    value = systems solved per second by one core."""
+    value = systems solved per second (the restatement's row-independent loops
+    on all host threads)."""
     import oracle
+
+    cores = oracle.set_threads(_host_threads())
 
     syst = batch_systems(args.batch)
     ms, its_all = [], []
@@ -478,8 +494,8 @@ def run_reference_batch(args):
            "config": {"workload": f"{len(syst)} KKT systems, n U[500,20000], m=n/2, A 4-8/col (band_half=32), "
                                   f"H log-U[1e-4,1e4], blocks 32, BK, fill 0",
                       "solver": f"oracle FP64 factor + SQMR (inner tol 1e-6, max_it {args.max_it}) in the same "
-                                f"refinement loop, at most {args.max_refine} corrections", "parallelism": "one CPU thread"},
-           "cpu_baseline": {"value": value, "unit": "solves/s", "cores": 1, "kind": "port",
+                                f"refinement loop, at most {args.max_refine} corrections", "parallelism": f"{cores} CPU threads"},
+           "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": "port",
                             "sample": f"{args.steps} systems (37 k mod 512), each solved whole; median SQMR "
                                       f"iterations {int(np.median(its_all))}"},
            "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -488,13 +504,15 @@ def run_reference_batch(args):
 
 def run_reference_served(args):
     """The CPU restatement on the served stream's requests, one after another
-    on one core: each step takes the next request of the same arrival trace
+    on the host (row-independent loops on all threads): each step takes the next request of the same arrival trace
     (pattern, 1-8 right-hand sides; the trace's first --warmup + --steps
     requests) and runs the oracle's factor plus, per right-hand side, a
     20-iteration SQMR sample scaled to max_it iterations (every right-hand
     side of this stream runs to max_it: none reaches 1e-8); value = requests
     per second."""
     import oracle
+
+    cores = oracle.set_threads(_host_threads())
 
     import culip_b200 as cb
 
@@ -533,9 +551,9 @@ def run_reference_served(args):
            "config": {"workload": f"{len(pats)} patterns, n log-U[1e3,5e5], m=n/2, A 6/col (band_half=32), "
                                   f"the served trace's requests, 1-8 RHS",
                       "solver": f"oracle factor + SQMR tol 1e-8, max_it {args.max_it}, requests one after another",
-                      "parallelism": "one CPU thread"},
+                      "parallelism": f"{cores} CPU threads"},
            "latency_ms": {"p50": float(np.percentile(ms, 50)), "p99": float(np.percentile(ms, 99))},
-           "cpu_baseline": {"value": value, "unit": "requests/s", "cores": 1, "kind": "port",
+           "cpu_baseline": {"value": value, "unit": "requests/s", "cores": cores, "kind": "port",
                             "sample": f"{args.steps} requests of the trace: factor whole, SQMR {sample_it} "
                                       f"iterations per right-hand side scaled to {args.max_it}"},
            "e2e": {"value": value, "unit": "requests/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -554,6 +572,8 @@ def run_reference(args):
         return run_reference_served(args)
     cfg, rp, ci, v, bs, b = _workload(args.config)
     import oracle
+
+    cores = oracle.set_threads(_host_threads())
 
     S = oracle.Sym(rp, ci, bs, 0, 1.0)
     # one step = factor + SQMR; bounded: SQMR capped at 20 iterations per step, scaled to the GPU iteration count
@@ -576,7 +596,7 @@ def run_reference(args):
            "dtype": "f64", "data": "synthetic (seeded KKT generator)", "impl": "reference",
            "config": _config_dict(args.config, cfg, len(ci), {"parallelism": f"replicas x{world} (independent KKT systems)",
                                                              "max_it": args.max_it}),
-           "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
+           "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
                             "sample": f"per step: oracle factor (full) + 20 SQMR iterations scaled to {iters_full}"},
            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)

@@ -64,8 +64,17 @@ def lib():
                                         ctypes.c_int, vp]
         L.orc_sqmr_ldu_d.restype = ctypes.c_int
         L.orc_sqmr_ldu_d.argtypes = [ctypes.c_int] + [vp] * 12 + [ctypes.c_double, ctypes.c_int, vp]
+        L.orc_set_threads.argtypes = [ctypes.c_int]
+        L.orc_get_threads.restype = ctypes.c_int
         _lib = L
     return _lib
+
+
+def set_threads(n: int) -> int:
+    """Threads for the loops that are independent per row / block row (SpMV,
+    vector updates, level sweeps, D); results do not depend on it."""
+    lib().orc_set_threads(int(n))
+    return lib().orc_get_threads()
 
 
 def _p(a: np.ndarray):

@@ -11,6 +11,7 @@
 #include "oracle.h"
 
 #include <math.h>
+#include <omp.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -45,6 +46,7 @@
 void orc_spmv_d(int m, const int *rowptr, const int *colidx, const double *val,
                 const double *x, double *y, double alpha, double beta)
 {
+#pragma omp parallel for schedule(static) if (m > 16384)
     for (int i = 0; i < m; ++i) {
         double acc = 0;
         for (int p = rowptr[i]; p < rowptr[i + 1]; ++p) acc = fma(val[p], x[colidx[p]], acc);
@@ -128,6 +130,13 @@ static void prec_apply(const prec_t *P, int stage, const double *b, double *x)
     else memcpy(x, b, sizeof(double) * P->n);
 }
 
+/* Threads of the loops that are independent per element, per row or per
+ * block row of a level (SpMV, vector updates, the level sweeps, D): the
+ * results do not depend on the count.  Dot products stay serial (their
+ * summation order is part of the restatement). */
+void orc_set_threads(int n) { omp_set_num_threads(n > 0 ? n : 1); }
+int orc_get_threads(void) { return omp_get_max_threads(); }
+
 static double dot(int n, const double *a, const double *b)
 {
     double s = 0;
@@ -185,11 +194,13 @@ static int sqmr_core(int m, const int *rowptr, const int *colidx, const double *
     norm_pb = sqrt(dot(m, v[0], v[0]));
     {
         const double t = 1.0 / norm_pb;
+        #pragma omp parallel for schedule(static) if (m > 16384)
         for (int i = 0; i < m; ++i) v[0][i] *= t;
     }
     prec_apply(P, 1, v[0], w[0]);
     eta = sqrt(dot(m, w[0], w[0]));
     eta = 1.0 / eta;
+    #pragma omp parallel for schedule(static) if (m > 16384)
     for (int i = 0; i < m; ++i) w[0][i] *= eta;
     gamma = norm_pb;
     prec_apply(P, 1, v[0], tmp);
@@ -205,6 +216,7 @@ static int sqmr_core(int m, const int *rowptr, const int *colidx, const double *
         prec_apply(P, 1, v[k0], tmp);
         double t = dot(m, v[k0], tmp);
         alpha = alpha / t;
+#pragma omp parallel for schedule(static) if (m > 16384)
         for (int i = 0; i < m; ++i) {
             double vi = Av[i];
             vi = fma(-alpha, v[k0][i], vi);
@@ -213,9 +225,11 @@ static int sqmr_core(int m, const int *rowptr, const int *colidx, const double *
         }
         delta[k1] = sqrt(dot(m, v[k1], v[k1]));
         t = 1.0 / delta[k1];
+        #pragma omp parallel for schedule(static) if (m > 16384)
         for (int i = 0; i < m; ++i) v[k1][i] *= t;
         prec_apply(P, 1, v[k1], w[k1]);
         t = eta * delta[k1];
+#pragma omp parallel for schedule(static) if (m > 16384)
         for (int i = 0; i < m; ++i) w[k1][i] *= t;
         prec_apply(P, 1, v[k1], tmp);
         prec_apply(P, 2, tmp, ev);
@@ -225,6 +239,7 @@ static int sqmr_core(int m, const int *rowptr, const int *colidx, const double *
         t = dot(m, w[k0], v[k0]);
         beta[k1] = beta[k1] / t;
         t = 1.0 / beta[k1];
+#pragma omp parallel for schedule(static) if (m > 16384)
         for (int i = 0; i < m; ++i) w[k1][i] *= t;
         t = delta[k1] / beta[k1];
         eta = t * eta;
@@ -236,12 +251,14 @@ static int sqmr_core(int m, const int *rowptr, const int *colidx, const double *
         alpha_rot = fma(s[k0], beta_rot, (-c[k0]) * alpha);
         sym_ortho(alpha_rot, delta[k1], &c[k1], &s[k1], &rho);
         tau = c[k1] * gamma;
+#pragma omp parallel for schedule(static) if (m > 16384)
         for (int i = 0; i < m; ++i) {
             double pi = v[k0][i];
             pi = fma(-beta_rot_rot, p[km1][i], pi);
             pi = fma(-epsilon, p[km2][i], pi);
             p[k0][i] = pi * (1.0 / rho);
         }
+        #pragma omp parallel for schedule(static) if (m > 16384)
         for (int i = 0; i < m; ++i) x[i] = fma(tau, p[k0][i], x[i]);
         norm_x = sqrt(dot(m, x, x));
         gamma = s[k1] * gamma;

@@ -68,6 +68,10 @@ int orc_sqmr_jacobi_d(int m, const int *rowptr, const int *colidx, const double 
                       int sweeps, const double *b, double *x, double tol, int max_it, double *residual);
 
 /* y = alpha * A x + beta * y (beta == 0: y is not read) */
+/* threads of the row-independent loops (results do not depend on it) */
+void orc_set_threads(int n);
+int orc_get_threads(void);
+
 void orc_spmv_d(int m, const int *rowptr, const int *colidx, const double *val,
                 const double *x, double *y, double alpha, double beta);
 

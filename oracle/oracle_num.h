@@ -702,6 +702,8 @@ static void F(solve_U)(const F(fac_t) *f, const F(rowlist_t) *U, REAL *x)
 {
     const orc_sym *s = f->s;
     for (int L = s->num_levels - 1; L >= 0; --L) {
+        /* block rows of a level are independent (each reads earlier levels only) */
+#pragma omp parallel for schedule(dynamic, 16) if (s->lvl_off[L + 1] - s->lvl_off[L] > 256)
         for (int q = s->lvl_off[L]; q < s->lvl_off[L + 1]; ++q) {
             const int I = s->lvl_rows[q];
             const int from = s->bs[I], h = F(bsize)(s, I);
@@ -727,6 +729,7 @@ static void F(solve_Ut)(const F(fac_t) *f, const F(rowlist_t) *Ut, REAL *x)
 {
     const orc_sym *s = f->s;
     for (int L = 0; L < s->num_levels; ++L) {
+#pragma omp parallel for schedule(dynamic, 16) if (s->lvl_off[L + 1] - s->lvl_off[L] > 256)
         for (int q = s->lvl_off[L]; q < s->lvl_off[L + 1]; ++q) {
             const int I = s->lvl_rows[q];
             const int from = s->bs[I], h = F(bsize)(s, I);
@@ -751,6 +754,8 @@ static void F(solve_Ut)(const F(fac_t) *f, const F(rowlist_t) *Ut, REAL *x)
 /* k_solve_D (Givens-based 1x1 / 2x2 block-diagonal solve), from a copy */
 static void F(solve_D)(int n, const REAL *tri, const int *is_piv, const REAL *in, REAL *out)
 {
+    /* every out entry is written by one g only, from the copy in */
+#pragma omp parallel for schedule(static) if (n > 16384)
     for (int g = 0; g < n; ++g) {
         const int this_piv = is_piv[g];
         const int next_piv = (g < n - 1) ? is_piv[g + 1] : 1;
