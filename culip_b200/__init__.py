@@ -84,6 +84,20 @@ def kkt_blocking(n, m, block) -> np.ndarray:
     return bs
 
 
+def blocking_generate(rowptr, colidx, min_size=8, max_size=32) -> np.ndarray:
+    """block_starts (num_blocks + 1 entries, last = n) for any symmetric
+    pattern, from culipx_blocking_generate."""
+    rp = np.ascontiguousarray(rowptr, np.int32)
+    ci = np.ascontiguousarray(colidx, np.int32)
+    n = len(rp) - 1
+    nb = ctypes.c_int()
+    capi.call("culipx_blocking_generate", n, _p(rp), _p(ci), int(min_size), int(max_size), None, 0, ctypes.byref(nb))
+    bs = np.zeros(nb.value + 1, np.int32)
+    capi.call("culipx_blocking_generate", n, _p(rp), _p(ci), int(min_size), int(max_size), _p(bs), nb.value + 1,
+              ctypes.byref(nb))
+    return bs
+
+
 def normal_vector(seed, n) -> np.ndarray:
     out = np.zeros(n, np.float64)
     capi.call("culipx_normal_vector", seed, n, _p(out))

@@ -45,6 +45,7 @@ _SIGS = {
     "culipx_kkt_nnz": [ctypes.POINTER(KktSpec), ctypes.POINTER(i64)],
     "culipx_kkt_generate": [ctypes.POINTER(KktSpec), vp, vp, vp],
     "culipx_kkt_blocking": [i32, i32, i32, vp, i32, ctypes.POINTER(i32)],
+    "culipx_blocking_generate": [i32, vp, vp, i32, i32, vp, i32, ctypes.POINTER(i32)],
     "culipx_normal_vector": [ctypes.c_ulonglong, i64, vp],
     "culipx_handle_create": [ctypes.POINTER(vp), i32, vp],
     "culipx_handle_destroy": [vp],

@@ -89,6 +89,17 @@ int culipx_kkt_generate(const culipx_kkt_spec *spec, int *h_rowptr, int *h_colid
 /* contiguous blocking that never straddles row n; block_starts gets
  * num_blocks + 1 entries (NULL: only count) */
 int culipx_kkt_blocking(int n, int m, int block, int *h_block_starts, int capacity, int *num_blocks);
+
+/* Blocking generator for any symmetric pattern (host CSR, sorted columns; no
+ * counterpart in the reference, whose driver reads the blocking from a file
+ * it does not create, apps/block_ildlt/block_ildlt.cc:29-35; same output
+ * contract: first rows of the blocks, then n).  Contiguous blocks of at most
+ * max_size (<= 32) rows: runs of consecutive rows with equal column sets stay
+ * together, a block closes once it holds min_size rows at the first run not
+ * coupled to it, and a short last block is merged or split evenly with its
+ * predecessor.  With h_block_starts NULL only num_blocks is returned. */
+int culipx_blocking_generate(int n, const int *h_rowptr, const int *h_colidx, int min_size, int max_size,
+                             int *h_block_starts, int capacity, int *num_blocks);
 int culipx_normal_vector(unsigned long long seed, long long len, double *h_out);
 
 /* ------------------------------------------------------------------------ */
