@@ -484,6 +484,37 @@ class Server:
             pass
 
 
+class ImportLDU:
+    """ImportLDUPreconditioner: L (lower CSR), D (tri, is_piv), perm, scale as
+    torch CUDA tensors (copied at creation)."""
+
+    def __init__(self, handle: Handle, L_rowptr, L_colidx, L_val, tri, is_piv, perm, scale):
+        self.handle = handle
+        self.n = L_rowptr.numel() - 1
+        P = ctypes.c_void_p()
+        capi.call("culipx_ldu_create", handle._h, self.n, _dptr(L_rowptr), _dptr(L_colidx), _dptr(L_val), _dptr(tri),
+                  _dptr(is_piv), _dptr(perm), _dptr(scale), ctypes.byref(P))
+        self._h = P
+
+    def apply(self, stage, b, x):
+        capi.call("culipx_ldu_apply", self._h, int(stage), _dptr(b), _dptr(x))
+        return x
+
+    def sqmr_solve(self, A: "CsrOperator", b, x, tol=1e-8, max_it=1000):
+        """Returns (residual, iterations, status)."""
+        res = ctypes.c_double()
+        its = ctypes.c_int()
+        st = capi.call("culipx_sqmr_solve_ldu", self.handle._h, A._h, self._h, _dptr(b), _dptr(x), float(tol),
+                       int(max_it), ctypes.byref(res), ctypes.byref(its), allow=(capi.OK, capi.MAXIT))
+        return res.value, its.value, st
+
+    def __del__(self):
+        try:
+            _release(self, "culipx_ldu_destroy")
+        except Exception:  # interpreter shutdown
+            pass
+
+
 class KktOperator:
     """AugmentedMatrixSPMV / NormalMatrixSPMV (FP64): A is the m x n
     constraint matrix (torch CUDA CSR arrays), d the diagonal D (n), ix the

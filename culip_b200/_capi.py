@@ -96,6 +96,10 @@ _SIGS = {
     "culipx_server_set_large_rows": [vp, i32],
     "culipx_server_launch_count": [vp, vp],
     "culipx_server_set_refine": [vp, i32, f64],
+    "culipx_ldu_create": [vp, i32, vp, vp, vp, vp, vp, vp, vp, vp],
+    "culipx_ldu_apply": [vp, i32, vp, vp],
+    "culipx_sqmr_solve_ldu": [vp, vp, vp, vp, vp, f64, i32, vp, vp],
+    "culipx_ldu_destroy": [vp],
     "culipx_kkt_operator_create": [vp, i32, i32, i32, ctypes.c_longlong, vp, vp, vp, vp, f64, i32, vp, vp],
     "culipx_kkt_operator_multiply": [vp, vp, vp, f64, f64],
     "culipx_kkt_operator_destroy": [vp],

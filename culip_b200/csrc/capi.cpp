@@ -1,5 +1,6 @@
 // extern "C" entry points of libculipx (declared in include/culipx.h).
 #include "factor.h"
+#include "ldu.h"
 #include "operators.h"
 #include "pattern.h"
 #include "permute.h"
@@ -616,6 +617,49 @@ CULIPX_API int culipx_server_stats(culipx_server s, long long* stats8)
 CULIPX_API int culipx_server_set_large_rows(culipx_server s, int rows)
 {
     return server_set_large_rows(s, rows);
+}
+
+CULIPX_API int culipx_ldu_create(culipx_handle h, int n, const int* d_rowptr, const int* d_colidx, const double* d_val,
+                                 const double* d_tri, const int* d_is_piv, const int* d_perm, const double* d_scale,
+                                 culipx_ldu* out)
+{
+    if (!h || !out) return fail(CULIPX_INVALID_ARG, "culipx_ldu_create: null argument");
+    if (h->device < 0) return fail(CULIPX_INVALID_ARG, "culipx_ldu_create: host-only handle");
+    GUARD_BEGIN
+    CULIPX_TRY(use_device(h));
+    Ldu* P = nullptr;
+    CULIPX_TRY(ldu_create(h, n, d_rowptr, d_colidx, d_val, d_tri, d_is_piv, d_perm, d_scale, &P));
+    *out = static_cast<culipx_ldu>(P);
+    return CULIPX_OK;
+    GUARD_END
+}
+
+CULIPX_API int culipx_ldu_apply(culipx_ldu P, int stage, const double* d_b, double* d_x)
+{
+    if (!P) return fail(CULIPX_INVALID_ARG, "null preconditioner");
+    GUARD_BEGIN
+    CULIPX_TRY(use_device(P->h));
+    return ldu_apply(P, stage, d_b, d_x, P->h->stream);
+    GUARD_END
+}
+
+CULIPX_API int culipx_sqmr_solve_ldu(culipx_handle h, culipx_csr A, culipx_ldu P, const double* d_b, double* d_x,
+                                     double tol, int max_it, double* residual, int* iterations)
+{
+    if (!h) return fail(CULIPX_INVALID_ARG, "null handle");
+    GUARD_BEGIN
+    CULIPX_TRY(use_device(h));
+    return sqmr_solve_ldu(h, A, P, d_b, d_x, tol, max_it, residual, iterations, h->sqmr);
+    GUARD_END
+}
+
+CULIPX_API int culipx_ldu_destroy(culipx_ldu P)
+{
+    if (P) {
+        if (P->h->device >= 0) cudaSetDevice(P->h->device);
+        delete P;
+    }
+    return CULIPX_OK;
 }
 
 CULIPX_API int culipx_kkt_operator_create(culipx_handle h, int kind, int m, int n, long long nnz, const int* d_rowptr,

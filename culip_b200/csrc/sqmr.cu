@@ -21,9 +21,11 @@
 // counts match the reference's.
 #include "sqmr.h"
 #include "factor.h"
+#include "ldu.h"
 #include "kernels_common.cuh"
 
 #include <cmath>
+#include <functional>
 
 namespace culipx {
 
@@ -124,6 +126,8 @@ struct DOp {  // D as seen by the SQMR kernels (null tri: identity)
     const double* tri;
     const int* is_piv;
 };
+
+using PrecFn = std::function<int(int stage, const double* in, double* out)>;
 
 #define SQMR_GUARD \
     if (S->done) return;
@@ -389,6 +393,11 @@ int sqmr_workspace(Sqmr* w, culipx_handle_t* h, int n)
     return CULIPX_OK;
 }
 
+namespace {
+int sqmr_phases(culipx_handle_t* h, Csr* A, DOp D, const PrecFn* pre, const double* b, double* x, double tol,
+                int max_it, double* residual, int* iterations, Sqmr* w);
+}
+
 int sqmr_solve(culipx_handle_t* h, Csr* A, Factor* M, const double* b, double* x, double tol, int max_it,
                double* residual, int* iterations, Sqmr* w)
 {
@@ -404,6 +413,20 @@ int sqmr_solve(culipx_handle_t* h, Csr* A, Factor* M, const double* b, double* x
         return sqmr_solve_persistent(h, A, M, b, x, tol, max_it, residual, iterations, w);
     if (M && M->precision != CULIPX_F64)
         return fail(CULIPX_NOT_SUPPORTED, "culipx_sqmr_solve: the multi-kernel solver needs an FP64 factor");
+    cudaStream_t s = h->stream;
+    const DOp D = M ? DOp{M->tri.as<double>(), M->is_piv.as<int>()} : DOp{nullptr, nullptr};
+    const PrecFn prec = [&](int stage, const double* in, double* out) { return prec_apply(M, stage, in, out, s); };
+    return sqmr_phases(h, A, D, M ? &prec : nullptr, b, x, tol, max_it, residual, iterations, w);
+}
+
+namespace {
+
+// The per-phase SQMR (one kernel per BLAS-1 step, as SQMR<T>::solve) with
+// any split preconditioner: D (tri / is_piv, applied inside the fused
+// kernels) and the left / middle / right applies through pre (null: none).
+int sqmr_phases(culipx_handle_t* h, Csr* A, DOp D, const PrecFn* pre, const double* b, double* x, double tol,
+                int max_it, double* residual, int* iterations, Sqmr* w)
+{
     const int n = A->m;
     cudaStream_t s = h->stream;
     CULIPX_TRY(sqmr_workspace(w, h, n));
@@ -424,11 +447,9 @@ int sqmr_solve(culipx_handle_t* h, Csr* A, Factor* M, const double* b, double* x
     CULIPX_CUDA(cudaMemsetAsync(x, 0, (size_t)n * sizeof(double), s));
     k_init_scalars<<<1, 1, 0, s>>>(S, tol, max_it);
     h->launches += 4;
-    DOp D{nullptr, nullptr};
-    if (M) D = DOp{M->tri.as<double>(), M->is_piv.as<int>()};
 
     auto prec = [&](int stage, const double* in, double* out) -> int {
-        if (M) return prec_apply(M, stage, in, out, s);
+        if (pre) return (*pre)(stage, in, out);
         CULIPX_CUDA(cudaMemcpyAsync(out, in, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, s));
         return CULIPX_OK;
     };
@@ -476,9 +497,9 @@ int sqmr_solve(culipx_handle_t* h, Csr* A, Factor* M, const double* b, double* x
     o.breakdown = hs.breakdown;
     if (max_it == 0) o.iters = 0;
     CULIPX_CUDA(cudaMemcpyAsync(Av, x, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, s));
-    if (M) {
-        CULIPX_TRY(prec_apply(M, CULIPX_MIDDLE, Av, tmp, s));
-        CULIPX_TRY(prec_apply(M, CULIPX_RIGHT, tmp, x, s));
+    if (pre) {
+        CULIPX_TRY((*pre)(CULIPX_MIDDLE, Av, tmp));
+        CULIPX_TRY((*pre)(CULIPX_RIGHT, tmp, x));
     }
     CULIPX_CUDA(cudaStreamSynchronize(s));
     if (residual) *residual = o.gamma / o.norm_pb;
@@ -486,6 +507,23 @@ int sqmr_solve(culipx_handle_t* h, Csr* A, Factor* M, const double* b, double* x
     if (o.breakdown) return fail(CULIPX_BREAKDOWN, "culipx_sqmr_solve: breakdown (non-finite scalar) at iteration %d", hs.it);
     if (!(hs.snap0 || hs.snap1) && o.iters >= max_it && max_it > 0) return CULIPX_MAXIT;
     return CULIPX_OK;
+}
+
+}  // namespace
+
+// SQMR with an imported L D L' preconditioner (the per-phase solver: D inside
+// the fused kernels, the triangular applies level by level)
+int sqmr_solve_ldu(culipx_handle_t* h, Csr* A, Ldu* P, const double* b, double* x, double tol, int max_it,
+                   double* residual, int* iterations, Sqmr* w)
+{
+    if (!A || !P || !b || !x || !w) return fail(CULIPX_INVALID_ARG, "culipx_sqmr_solve_ldu: null argument");
+    if (A->precision != CULIPX_F64 || A->m != A->n || A->m != P->n)
+        return fail(CULIPX_INVALID_ARG, "culipx_sqmr_solve_ldu: A must be square FP64 of the preconditioner's size");
+    if (max_it < 0) return fail(CULIPX_INVALID_ARG, "culipx_sqmr_solve_ldu: max_it < 0");
+    cudaStream_t s = h->stream;
+    const DOp D{P->tri.as<double>(), P->is_piv.as<int>()};
+    const PrecFn prec = [&](int stage, const double* in, double* out) { return ldu_apply(P, stage, in, out, s); };
+    return sqmr_phases(h, A, D, &prec, b, x, tol, max_it, residual, iterations, w);
 }
 
 }  // namespace culipx

@@ -66,6 +66,10 @@ int sqmr_refine_multi(culipx_handle_t* h, Csr* A, Factor* M, int nrhs, const dou
 
 int sqmr_workspace(Sqmr* w, culipx_handle_t* h, int n);
 
+struct Ldu;
+int sqmr_solve_ldu(culipx_handle_t* h, Csr* A, Ldu* P, const double* b, double* x, double tol, int max_it,
+                   double* residual, int* iterations, Sqmr* w);
+
 int tune_kkt_block(culipx_handle_t* h, int n, int m, const int* rowptr, const int* colidx, const double* d_vals,
                    const double* d_b, int precision, const int* candidates, int num_candidates, double tol, int max_it,
                    int* best_block, double* h_ms, int* h_iterations, int* h_status, double* h_residual);

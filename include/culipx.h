@@ -331,6 +331,27 @@ int culipx_server_stats(culipx_server s, long long *stats8);
 /* requests on patterns with n >= rows use the whole-GPU solver (rows >= 1;
  * default 131072); applies to batches admitted afterwards */
 int culipx_server_set_large_rows(culipx_server s, int rows);
+/* Imported L D L' preconditioner (ImportLDUPreconditioner<T>,
+ * libs/la/preconditioner/import_ldu_preconditioner.impl.cuh, as the
+ * reference's tests/la/test_sqmr.cc:192-293 use it): L lower-triangular CSR
+ * (n rows, device, FP64; its diagonal divides, 1 where absent), D as
+ * tri[3n] / is_piv[n] (the block factor's storage), perm[n] (P) and scale[n]
+ * (S), all device arrays, copied at create (which synchronizes).
+ *   LEFT   x = L^-1 P' (S .* b)
+ *   MIDDLE x = D^-1 b
+ *   RIGHT  x = S .* P (L'^-1 b)
+ * Both substitutions run level by level; each row sums its terms in the order
+ * of a serial sweep.  b and x must not overlap. */
+typedef struct culipx_ldu_t *culipx_ldu;
+int culipx_ldu_create(culipx_handle h, int n, const int *d_rowptr, const int *d_colidx, const double *d_val,
+                      const double *d_tri, const int *d_is_piv, const int *d_perm, const double *d_scale,
+                      culipx_ldu *out);
+int culipx_ldu_apply(culipx_ldu P, int stage, const double *d_b, double *d_x);
+/* SQMR (as culipx_sqmr_solve) with the imported preconditioner */
+int culipx_sqmr_solve_ldu(culipx_handle h, culipx_csr A, culipx_ldu P, const double *d_b, double *d_x, double tol,
+                          int max_it, double *residual, int *iterations);
+int culipx_ldu_destroy(culipx_ldu P);
+
 /* Matrix-free KKT operators over a constraint matrix A (m x n, FP64 CSR on
  * the device, borrowed) and a diagonal D (n, borrowed); they replace
  * AugmentedMatrixSPMV<T> and NormalMatrixSPMV<T> (libs/la/spmv.cuh:75-149,

@@ -64,6 +64,7 @@ def lib():
                                         ctypes.c_int, vp]
         L.orc_sqmr_ldu_d.restype = ctypes.c_int
         L.orc_sqmr_ldu_d.argtypes = [ctypes.c_int] + [vp] * 12 + [ctypes.c_double, ctypes.c_int, vp]
+        L.orc_ldu_apply_d.argtypes = [ctypes.c_int] + [vp] * 7 + [ctypes.c_int, vp, vp]
         L.orc_set_threads.argtypes = [ctypes.c_int]
         L.orc_get_threads.restype = ctypes.c_int
         _lib = L
@@ -217,6 +218,19 @@ def sqmr_ldu(rowptr, colidx, val, L_rowptr, L_colidx, L_val, tri, is_piv, perm, 
     res = np.zeros(1)
     it = lib().orc_sqmr_ldu_d(m, *[_p(v) for v in a], _p(x), float(tol), int(max_it), _p(res))
     return x, float(res[0]), int(it)
+
+
+def ldu_apply(L_rowptr, L_colidx, L_val, tri, is_piv, perm, scale, stage, b):
+    """ImportLDUPreconditioner::solve_left / middle / right (stage 0 / 1 / 2),
+    import_ldu_preconditioner.impl.cuh, with the restatement's ldu_apply."""
+    a = [np.ascontiguousarray(v, t) for v, t in ((L_rowptr, np.int32), (L_colidx, np.int32), (L_val, np.float64),
+                                                  (tri, np.float64), (is_piv, np.int32), (perm, np.int32),
+                                                  (scale, np.float64))]
+    n = len(a[0]) - 1
+    b = np.ascontiguousarray(b, np.float64)
+    x = np.zeros(n)
+    lib().orc_ldu_apply_d(n, *[_p(v) for v in a], int(stage), _p(b), _p(x))
+    return x
 
 
 def permute_scale(rowptr, colidx, val, row_perm, col_perm=None, row_scale=None, col_scale=None,

@@ -305,6 +305,21 @@ int orc_sqmr_jacobi_d(int m, const int *rowptr, const int *colidx, const double 
     return sqmr_core(m, rowptr, colidx, val, &P, b, x, tol, max_it, residual);
 }
 
+void orc_ldu_apply_d(int n, const int *L_rowptr, const int *L_colidx, const double *L_val, const double *tri,
+                     const int *is_piv, const int *perm, const double *scale, int stage, const double *b, double *x)
+{
+    prec_t P;
+    memset(&P, 0, sizeof(P));
+    P.kind = 2;
+    P.n = n;
+    P.L_rowptr = L_rowptr; P.L_colidx = L_colidx; P.L_val = L_val;
+    P.tri = tri; P.is_piv = is_piv; P.perm = perm; P.scale = scale;
+    P.t1 = (double *)calloc(n, sizeof(double));
+    P.t2 = (double *)calloc(n, sizeof(double));
+    ldu_apply(&P, stage, b, x);
+    free(P.t1); free(P.t2);
+}
+
 int orc_sqmr_ldu_d(int m, const int *rowptr, const int *colidx, const double *val,
                    const int *L_rowptr, const int *L_colidx, const double *L_val,
                    const double *tri, const int *is_piv, const int *perm, const double *scale,

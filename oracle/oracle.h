@@ -68,6 +68,10 @@ int orc_sqmr_jacobi_d(int m, const int *rowptr, const int *colidx, const double 
                       int sweeps, const double *b, double *x, double tol, int max_it, double *residual);
 
 /* y = alpha * A x + beta * y (beta == 0: y is not read) */
+/* ImportLDUPreconditioner's solve_left (0) / middle (1) / right (2) */
+void orc_ldu_apply_d(int n, const int *L_rowptr, const int *L_colidx, const double *L_val, const double *tri,
+                     const int *is_piv, const int *perm, const double *scale, int stage, const double *b, double *x);
+
 /* threads of the row-independent loops (results do not depend on it) */
 void orc_set_threads(int n);
 int orc_get_threads(void);
