@@ -1096,8 +1096,10 @@ __global__ void __launch_bounds__(kT, kCtasPerSm) k_sqmr_batched(PArgs<TF> a, Ba
 // factor, matrix and vectors (the serving path): the CTA copies system s's
 // argument block into shared memory and runs the same body over its rows,
 // for nr[s] (1, 2 or 4) right-hand sides of that system at once.  Systems are
-// handed out in index order, so the host lists the longest first.
-template <class TF>
+// handed out in index order, so the host lists the longest first.  MULTI =
+// false compiles the one-right-hand-side body alone (every nr[s] == 1): the
+// 2- and 4-wide bodies in the same kernel cost the common case registers.
+template <class TF, bool MULTI>
 __global__ void __launch_bounds__(kT, kCtasPerSm) k_sqmr_many(const PArgs<TF>* __restrict__ sys_args,
                                                              const int* __restrict__ nr, int num, int* next)
 {
@@ -1117,10 +1119,14 @@ __global__ void __launch_bounds__(kT, kCtasPerSm) k_sqmr_many(const PArgs<TF>* _
         for (int i = threadIdx.x; i < (int)(sizeof(PArgs<TF>) / 8); i += kT) dst[i] = src[i];
         __syncthreads();
         const SysView sv{0, pa.n, pa.lvl_off, pa.lvl_off + 1, pa.out};
-        const int r = __ldg(nr + s);
-        if (r == 4) sqmr_body<TF, 4>(pa, ctx, sv, reinterpret_cast<Scal(&)[4]>(S), sh);
-        else if (r == 2) sqmr_body<TF, 2>(pa, ctx, sv, reinterpret_cast<Scal(&)[2]>(S), sh);
-        else sqmr_body<TF, 1>(pa, ctx, sv, reinterpret_cast<Scal(&)[1]>(S), sh);
+        if constexpr (MULTI) {
+            const int r = __ldg(nr + s);
+            if (r == 4) sqmr_body<TF, 4>(pa, ctx, sv, reinterpret_cast<Scal(&)[4]>(S), sh);
+            else if (r == 2) sqmr_body<TF, 2>(pa, ctx, sv, reinterpret_cast<Scal(&)[2]>(S), sh);
+            else sqmr_body<TF, 1>(pa, ctx, sv, reinterpret_cast<Scal(&)[1]>(S), sh);
+        } else {
+            sqmr_body<TF, 1>(pa, ctx, sv, reinterpret_cast<Scal(&)[1]>(S), sh);
+        }
     }
 }
 
@@ -1521,16 +1527,20 @@ int launch_many_prec(culipx_handle_t* h, const std::vector<int>& ks, const int* 
     CULIPX_CUDA(cudaMemcpyAsync(d_args, args.data(), (size_t)num * sizeof(PArgs<TF>), cudaMemcpyHostToDevice, s));
     CULIPX_CUDA(cudaMemcpyAsync(d_nr, nrs.data(), (size_t)num * sizeof(int), cudaMemcpyHostToDevice, s));
     CULIPX_CUDA(cudaMemsetAsync(d_next, 0, sizeof(int), s));
-    static int G = 0;
+    const bool multi = std::any_of(nrs.begin(), nrs.end(), [](int r) { return r != 1; });
+    static int Gs[2] = {0, 0};
+    int& G = Gs[multi ? 1 : 0];
     if (G == 0) {
         int dev = 0, per_sm = 0, sms = 0;
         CULIPX_CUDA(cudaGetDevice(&dev));
         CULIPX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        CULIPX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sqmr_many<TF>, kT, 0));
+        CULIPX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &per_sm, multi ? (const void*)k_sqmr_many<TF, true> : (const void*)k_sqmr_many<TF, false>, kT, 0));
         if (per_sm < 1) return fail(CULIPX_NOT_SUPPORTED, "batched SQMR kernel does not fit on an SM");
         G = sms * std::min(per_sm, kCtasPerSm);
     }
-    k_sqmr_many<TF><<<std::min(G, num), kT, 0, s>>>(d_args, d_nr, num, d_next);
+    if (multi) k_sqmr_many<TF, true><<<std::min(G, num), kT, 0, s>>>(d_args, d_nr, num, d_next);
+    else k_sqmr_many<TF, false><<<std::min(G, num), kT, 0, s>>>(d_args, d_nr, num, d_next);
     h->launches += 1;
     CULIPX_TRY(launch_check("k_sqmr_many"));
     for (int i = 0; i < num; ++i)
