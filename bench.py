@@ -229,7 +229,7 @@ def run_culipx(args):
     sq_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
 
     def step(i=None):
-        F.compute(d_v, None, cb.PIV_BK, 0.0)
+        F.compute_graph(d_v, cb.PIV_BK, 0.0)  # the factorization's ~31 kernels as one graph launch
         if i is not None:
             sq_ev[i][0].record(stream)
         res, its, st = cb.sqmr_solve(h, A, F, d_b, d_x, 1e-8, args.max_it)
@@ -281,6 +281,8 @@ def run_culipx(args):
     d_b2 = torch.empty_like(d_b)
     A2 = cb.CsrOperator(h, d_rp, d_ci, d_v2)
     e2e_steps = max(2, min(args.steps, 5))
+    d_v2.copy_(d_v)
+    F.compute_graph(d_v2, cb.PIV_BK, 0.0)  # capture for this buffer before the timed region
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -293,7 +295,7 @@ def run_culipx(args):
         e0.record(stream)
         d_v2.copy_(hv, non_blocking=True)
         d_b2.copy_(hb, non_blocking=True)
-        F.compute(d_v2, None, cb.PIV_BK, 0.0)
+        F.compute_graph(d_v2, cb.PIV_BK, 0.0)
         cb.sqmr_solve(h, A2, F, d_b2, d_x, 1e-8, args.max_it)
         hx.copy_(d_x, non_blocking=True)
         e1.record(stream)
@@ -644,7 +646,7 @@ def run_mixed(args):
     stats = {}
 
     def step():
-        F.compute(d_v32, None, cb.PIV_BK, 0.0)
+        F.compute_graph(d_v32, cb.PIV_BK, 0.0)
         rel, its, steps, st = cb.sqmr_refine_multi(h, A, F, d_B, d_X, tol, inner_tol, inner_it, max_ref)
         stats.update(rel=rel, its=its, steps=steps, st=st)
 
@@ -906,7 +908,7 @@ def run_batch(args):
     stats = {}
 
     def step():
-        F.compute(d_v32, None, cb.PIV_BK, 0.0)
+        F.compute_graph(d_v32, cb.PIV_BK, 0.0)
         rel, its, steps, st = cb.batch_sqmr_refine(B, A, F, d_b, d_x, tol, inner_tol, inner_it, max_ref)
         stats.update(rel=rel, its=its, steps=steps, st=st)
 

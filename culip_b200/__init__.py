@@ -228,6 +228,11 @@ class Factor:
             capi.call("culipx_factor_compute", self._h, _dptr(vals), None if ip is None else _p(ip), int(pivot),
                       float(threshold))
 
+    def compute_graph(self, vals, pivot=PIV_BK, threshold=0.0):
+        """compute() replayed from a CUDA graph captured on the first call
+        for this tensor (vals: torch CUDA tensor, pattern precision)."""
+        capi.call("culipx_factor_compute_graph", self._h, _dptr(vals), int(pivot), float(threshold))
+
     def set_solve_algorithm(self, algorithm, sweeps=0):
         capi.call("culipx_factor_set_solve_algorithm", self._h, int(algorithm), int(sweeps))
 

@@ -96,6 +96,7 @@ _SIGS = {
     "culipx_server_set_large_rows": [vp, i32],
     "culipx_server_launch_count": [vp, vp],
     "culipx_server_set_refine": [vp, i32, f64],
+    "culipx_factor_compute_graph": [vp, vp, i32, f64],
     "culipx_ldu_create": [vp, i32, vp, vp, vp, vp, vp, vp, vp, vp],
     "culipx_ldu_apply": [vp, i32, vp, vp],
     "culipx_sqmr_solve_ldu": [vp, vp, vp, vp, vp, f64, i32, vp, vp],

@@ -225,6 +225,15 @@ CULIPX_API int culipx_factor_compute(culipx_factor f, const void* d_vals, const 
     GUARD_END
 }
 
+CULIPX_API int culipx_factor_compute_graph(culipx_factor f, const void* d_vals, int pivot, double threshold)
+{
+    if (!f) return fail(CULIPX_INVALID_ARG, "null factor");
+    GUARD_BEGIN
+    CULIPX_TRY(use_device(f->pat->handle));
+    return factor_compute_graph(f, d_vals, pivot, threshold);
+    GUARD_END
+}
+
 CULIPX_API int culipx_factor_compute_host(culipx_factor f, const double* h_vals, const int* h_is_piv, int pivot,
                                           double threshold)
 {

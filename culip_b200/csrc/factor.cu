@@ -693,8 +693,9 @@ int run_levels(Factor* f, const void* d_vals, cudaStream_t s, int* launches)
 
     const bool thr = f->threshold > 0.0;
     if (thr) {
-        CULIPX_TRY(f->row_norm.alloc(p.handle, (size_t)p.n * sizeof(T)));
-        CULIPX_TRY(f->norm_part.alloc(p.handle, (size_t)std::max(p.max_level_blocks, 1) * 32 * sizeof(T)));
+        const size_t nb = (size_t)p.n * sizeof(T), pb = (size_t)std::max(p.max_level_blocks, 1) * 32 * sizeof(T);
+        if (f->row_norm.bytes() < nb) CULIPX_TRY(f->row_norm.alloc(p.handle, nb));
+        if (f->norm_part.bytes() < pb) CULIPX_TRY(f->norm_part.alloc(p.handle, pb));
     }
     T* row_norm = thr ? f->row_norm.as<T>() : nullptr;
     T* norm_part = thr ? f->norm_part.as<T>() : nullptr;
@@ -849,7 +850,7 @@ int factor_compute(Factor* f, const void* d_vals, const int* h_is_piv, int pivot
         for (int i = 0; i < n; ++i)
             if (h_is_piv[i] != 0 && h_is_piv[i] != 1)
                 return fail(CULIPX_INVALID_ARG, "culipx_factor_compute: is_piv[%d] = %d is not 0/1", i, h_is_piv[i]);
-    CULIPX_CUDA(cudaEventRecord(h->ev_start, s));
+    if (!f->capturing) CULIPX_CUDA(cudaEventRecord(h->ev_start, s));
     CULIPX_CUDA(cudaMemsetAsync(f->val.get(), 0, p.val_slots * f->vbytes, s));
     CULIPX_CUDA(cudaMemcpyAsync(f->idx.get(), p.d_idx_init.get(), p.val_slots * sizeof(int),
                                 cudaMemcpyDeviceToDevice, s));
@@ -865,10 +866,82 @@ int factor_compute(Factor* f, const void* d_vals, const int* h_is_piv, int pivot
     if (f->precision == CULIPX_F64) CULIPX_TRY(run_levels<double>(f, d_vals, s, &launches));
     else CULIPX_TRY(run_levels<float>(f, d_vals, s, &launches));
     CULIPX_TRY(build_sweeps(f, s, &launches));
-    CULIPX_CUDA(cudaEventRecord(h->ev_stop, s));
+    if (!f->capturing) CULIPX_CUDA(cudaEventRecord(h->ev_stop, s));
     f->last_launches = launches;
     h->launches += launches;
     f->computed = true;
+    return CULIPX_OK;
+}
+
+Factor::~Factor()
+{
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (capture_stream) cudaStreamDestroy(capture_stream);
+}
+
+// The numeric factorization from a CUDA graph: the first call for a values
+// pointer / pivot / threshold runs factor_compute once (which sizes every
+// buffer, so the captured run allocates nothing), then captures the same
+// call's launch sequence on the handle's stream; later calls with the same
+// pointer replay it as one graph launch (the values behind the pointer may
+// change in between).  is_piv comes from the factor's last state (no host
+// array: a pageable copy cannot be captured).
+int factor_compute_graph(Factor* f, const void* d_vals, int pivot, double threshold)
+{
+    if (!f || !d_vals) return fail(CULIPX_INVALID_ARG, "culipx_factor_compute_graph: null argument");
+    Pattern& p = *f->pat;
+    culipx_handle_t* h = p.handle;
+    cudaStream_t s = h->stream;
+    if (!f->graph_exec || f->graph_vals != d_vals || f->graph_pivot != pivot || f->graph_threshold != threshold) {
+        CULIPX_TRY(factor_compute(f, d_vals, nullptr, pivot, threshold));
+        if (f->graph_exec) cudaGraphExecDestroy(f->graph_exec);
+        if (f->graph) cudaGraphDestroy(f->graph);
+        f->graph_exec = nullptr;
+        f->graph = nullptr;
+        // captured on a stream of the factor's own (the handle's stream may be
+        // the legacy default stream, which cannot be captured); capturing
+        // runs nothing, so no ordering with the handle's stream is needed
+        if (!f->capture_stream) CULIPX_CUDA(cudaStreamCreateWithFlags(&f->capture_stream, cudaStreamNonBlocking));
+        const long long launches0 = h->launches;
+        CULIPX_CUDA(cudaStreamBeginCapture(f->capture_stream, cudaStreamCaptureModeThreadLocal));
+        h->stream = f->capture_stream;
+        f->capturing = true;
+        const int st = factor_compute(f, d_vals, nullptr, pivot, threshold);
+        f->capturing = false;
+        h->stream = s;
+        h->launches = launches0;  // captured, not launched
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(f->capture_stream, &g);
+        if (st != CULIPX_OK || e != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();
+            return st != CULIPX_OK ? st
+                                   : fail(CULIPX_CUDA_ERROR, "culipx_factor_compute_graph: capture failed: %s",
+                                          cudaGetErrorString(e));
+        }
+        cudaGraphExec_t x = nullptr;
+        if (cudaGraphInstantiate(&x, g, 0) != cudaSuccess) {
+            cudaGraphDestroy(g);
+            cudaGetLastError();
+            return fail(CULIPX_CUDA_ERROR, "culipx_factor_compute_graph: graph instantiation failed");
+        }
+        f->graph = g;
+        f->graph_exec = x;
+        f->graph_vals = d_vals;
+        f->graph_pivot = pivot;
+        f->graph_threshold = threshold;
+        f->graph_launches = f->last_launches;
+        return CULIPX_OK;  // the ordinary run above factored these values
+    }
+    CULIPX_CUDA(cudaEventRecord(h->ev_start, s));
+    CULIPX_CUDA(cudaGraphLaunch(f->graph_exec, s));
+    CULIPX_CUDA(cudaEventRecord(h->ev_stop, s));
+    f->pivot = pivot;
+    f->threshold = threshold;
+    f->computed = true;
+    f->last_launches = f->graph_launches;
+    h->launches += f->graph_launches;
     return CULIPX_OK;
 }
 

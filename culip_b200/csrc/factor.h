@@ -65,10 +65,24 @@ struct Factor {
 
     float last_ms = 0.f;
     int last_launches = 0;
+    // the numeric factorization as a CUDA graph (factor_compute_graph)
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    const void* graph_vals = nullptr;
+    int graph_pivot = -1;
+    double graph_threshold = -1.0;
+    int graph_launches = 0;
+    bool capturing = false;
+    cudaStream_t capture_stream = nullptr;
+    Factor() = default;
+    Factor(const Factor&) = delete;
+    Factor& operator=(const Factor&) = delete;
+    ~Factor();
 };
 
 int factor_create(Pattern* p, Factor** out);
 int factor_compute(Factor* f, const void* d_vals, const int* h_is_piv, int pivot, double threshold);
+int factor_compute_graph(Factor* f, const void* d_vals, int pivot, double threshold);
 int factor_export(Factor* f, int* blk_nnz, long long* blk_off, int* idx, void* val, void* tri,
                   int* is_piv, int* perm, int* got_extra, long long* total);
 int prec_apply(Factor* f, int stage, const void* d_b, void* d_x, cudaStream_t stream);

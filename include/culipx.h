@@ -165,6 +165,15 @@ int culipx_factor_destroy(culipx_factor f);
  * threshold: relative dropping threshold (>= 0). */
 int culipx_factor_compute(culipx_factor f, const void *d_vals, const int *h_is_piv, int pivot,
                           double threshold);
+/* culipx_factor_compute (is_piv NULL) replayed from a CUDA graph; no
+ * counterpart in the reference, which launches the factorization's kernels
+ * one by one.  The first call for a given values pointer, pivot method and
+ * threshold factors normally once, then captures the same launch sequence on
+ * the handle's stream (which must not be capturing already); later calls with
+ * that pointer launch the graph, one launch for the whole factorization, and
+ * read whatever values the pointer then holds.  Another pointer, pivot or
+ * threshold captures anew. */
+int culipx_factor_compute_graph(culipx_factor f, const void *d_vals, int pivot, double threshold);
 /* same, with K's values (double) in host memory; converts to the pattern's precision */
 int culipx_factor_compute_host(culipx_factor f, const double *h_vals, const int *h_is_piv,
                                int pivot, double threshold);
