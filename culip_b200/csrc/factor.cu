@@ -825,6 +825,7 @@ int factor_create(Pattern* p, Factor** out)
     al(f->scan_c, (cm + 1) * sizeof(int));
     al(f->simple_rows, (size_t)n * sizeof(int));
     al(f->cplx, cm * sizeof(int));
+    al(f->citem, std::max(cm, 1) * sizeof(CItem));
     al(f->u_colp, off_slots * sizeof(int));
     al(f->dg, ((size_t)n + 32) * f->vbytes);
     if (st != CULIPX_OK) { delete f; return st; }

@@ -14,6 +14,17 @@ enum RowFlags : int {
     kRowNoUpdates = 8,     // the pivot block received no Schur updates
 };
 
+// A pivot-tile block row as a work item of the sweeps: everything the item
+// needs before its data, read with two 16-byte loads (block row, first row,
+// rows, row flags; packed-tile offset, non-unit diagonal mask)
+struct alignas(16) CItem {
+    int I, fr, h, flags;
+    long long pk_off;
+    unsigned nd;
+    int pad;
+};
+static_assert(sizeof(CItem) == 32, "CItem is two 16-byte words");
+
 struct Factor {
     Pattern* pat = nullptr;
     int precision = CULIPX_F64;
@@ -58,6 +69,8 @@ struct Factor {
     // running counts of simple fine rows / other block rows, so level L owns
     // simple_rows[scan_s[lvl_off[L]] ..) and cplx[scan_c[lvl_off[L]] ..)
     DeviceBuffer scan_s, scan_c, simple_rows, cplx;
+    // per entry of cplx: its block row's metadata in one 32-byte record (CItem)
+    DeviceBuffer citem;
     DeviceBuffer work;                   // n values of apply scratch
     DeviceBuffer jac_a, jac_b;           // SOLVE_JACOBI iterates (n values each, allocated on first use)
     DeviceBuffer scan_tmp;               // scan partial sums

@@ -298,7 +298,9 @@ __global__ void k_split_count(int cm, const int* __restrict__ lvl_rows, const in
 // both in level-list order
 __global__ void k_split_fill(int cm, const int* __restrict__ lvl_rows, const int* __restrict__ bs,
                              const int* __restrict__ rowflags, const int* __restrict__ scan_s,
-                             const int* __restrict__ scan_c, int* __restrict__ simple_rows, int* __restrict__ cplx)
+                             const int* __restrict__ scan_c, int* __restrict__ simple_rows, int* __restrict__ cplx,
+                             const long long* __restrict__ pk_off, const unsigned* __restrict__ ndmask,
+                             CItem* __restrict__ citem)
 {
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < cm; q += gridDim.x * blockDim.x) {
         const int I = lvl_rows[q];
@@ -307,6 +309,15 @@ __global__ void k_split_fill(int cm, const int* __restrict__ lvl_rows, const int
             for (int r = 0; r < h; ++r) simple_rows[scan_s[q] + r] = fr + r;
         } else {
             cplx[scan_c[q]] = I;
+            CItem c;
+            c.I = I;
+            c.fr = bs[I];
+            c.h = bs[I + 1] - c.fr;
+            c.flags = rowflags[I];
+            c.pk_off = pk_off[I];
+            c.nd = ndmask[I];
+            c.pad = 0;
+            citem[scan_c[q]] = c;
         }
     }
 }
@@ -496,7 +507,8 @@ int build_sweeps_t(Factor* f, cudaStream_t s, int* launches)
     CULIPX_TRY(exclusive_scan(f->scan_c.as<int>(), cm + 1, f->scan_tmp, p.handle, s, launches));
     k_split_fill<<<std::min(cm / 256 + 1, 148 * 4), 256, 0, s>>>(cm, lvl_rows, a.bs, rowflags, f->scan_s.as<int>(),
                                                                  f->scan_c.as<int>(), f->simple_rows.as<int>(),
-                                                                 f->cplx.as<int>());
+                                                                 f->cplx.as<int>(), f->pk_off.as<long long>(),
+                                                                 f->ndmask.as<unsigned>(), f->citem.as<CItem>());
     *launches += 1;
     return launch_check("build_sweeps");
 }

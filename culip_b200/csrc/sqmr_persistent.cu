@@ -103,6 +103,7 @@ struct PArgs {
     const int* scan_c;
     const int* simple_rows;
     const int* cplx;
+    const CItem* citem;        // per entry of cplx: the block row's metadata
     double* v[2];              // v_k and v_k-1, v_k+1 overwrites v_k-1 in place
     double* p[2];              // p_k-1 and p_k-2, p_k overwrites p_k-2 in place
     double* Av;
@@ -412,16 +413,54 @@ __device__ __forceinline__ void tile_lower(double (&v)[NR], const TF* P, int h, 
     for (int r = 0; r < NR; ++r) v[r] = (double)t[r];
 }
 
+// A work item's block-row metadata
+struct ItemMeta {
+    int I, fr, h, flags;
+    long long pko;
+    unsigned nd;
+};
+
+// from the block row (sweeps over every block row of a level)
+template <class TF>
+__device__ __forceinline__ ItemMeta meta_of_row(const PArgs<TF>& a, int I)
+{
+    ItemMeta m;
+    m.I = I;
+    m.fr = __ldg(a.bs + I);
+    m.h = __ldg(a.bs + I + 1) - m.fr;
+    m.flags = __ldg(a.rowflags + I);
+    m.pko = __ldg(a.pk_off + I);
+    m.nd = __ldg(a.ndmask + I);
+    return m;
+}
+
+// from entry t of the pivot-tile block rows: two independent 16-byte loads
+// instead of the chain cplx -> (bs, rowflags, pk_off, ndmask)
+template <class TF>
+__device__ __forceinline__ ItemMeta meta_of_item(const PArgs<TF>& a, int t)
+{
+    const int4* p = reinterpret_cast<const int4*>(a.citem + t);
+    const int4 u = __ldg(p), w = __ldg(p + 1);
+    ItemMeta m;
+    m.I = u.x;
+    m.fr = u.y;
+    m.h = u.z;
+    m.flags = u.w;
+    m.pko = (long long)(((unsigned long long)(unsigned)w.y << 32) | (unsigned)w.x);
+    m.nd = (unsigned)w.z;
+    return m;
+}
+
 // One U-sweep work item: block row I (rows fr .. fr+h-1), lane's right-hand
 // sides y: d = D^-1 y; t = U_II^-1 (d - U_I* t); out[perm[r]] = t (NR
 // interleaved).  The gathers of the later levels' t read out through the
 // permuted columns.  d receives D^-1 y (0 on lanes >= h).
 template <class TF, int NR>
-__device__ __forceinline__ void u_item(const PArgs<TF>& a, int I, int fr, int h, const double (&y)[NR], double* out,
+__device__ __forceinline__ void u_item(const PArgs<TF>& a, const ItemMeta& m, const double (&y)[NR], double* out,
                                        double (&d)[NR])
 {
     const int lane = (int)lane_id();
-    const int flags = __ldg(a.rowflags + I);
+    const int fr = m.fr, h = m.h, flags = m.flags;
     DBlock<TF> D;
     D.load(a, fr, h, flags);
 #pragma unroll
@@ -437,7 +476,7 @@ __device__ __forceinline__ void u_item(const PArgs<TF>& a, int I, int fr, int h,
 #pragma unroll
         for (int r = 0; r < NR; ++r) t[r] = (double)acc[r];
     }
-    if (!(flags & kRowIdentity)) tile_upper<TF, NR>(t, a.pk_col + __ldg(a.pk_off + I), h, __ldg(a.ndmask + I));
+    if (!(flags & kRowIdentity)) tile_upper<TF, NR>(t, a.pk_col + m.pko, h, m.nd);
     if (lane < h) {
         const int q = (flags & kRowPermIdentity) ? fr + lane : __ldg(a.perm + fr + lane);
 #pragma unroll
@@ -456,10 +495,11 @@ enum RhsFrom {
 // with the lane's right-hand sides taken as FROM says.  t receives the
 // lane's results (0 for lanes >= h).
 template <class TF, int NR, int FROM>
-__device__ __forceinline__ void ut_item(const PArgs<TF>& a, int I, int fr, int h, int flags, const double* src,
+__device__ __forceinline__ void ut_item(const PArgs<TF>& a, const ItemMeta& m, const double* src,
                                         const double (&sc)[NR], double* dst, double (&t)[NR])
 {
     const int lane = (int)lane_id();
+    const int fr = m.fr, h = m.h, flags = m.flags;
 #pragma unroll
     for (int r = 0; r < NR; ++r) t[r] = 0.0;
     if (lane < h) {
@@ -485,7 +525,7 @@ __device__ __forceinline__ void ut_item(const PArgs<TF>& a, int I, int fr, int h
     }
     // with kRhsPre the lanes read dst inside this block row: all reads before any write
     if (FROM == kRhsPre) __syncwarp();
-    if (!(flags & kRowIdentity)) tile_lower<TF, NR>(t, a.pk_row + __ldg(a.pk_off + I), h, __ldg(a.ndmask + I));
+    if (!(flags & kRowIdentity)) tile_lower<TF, NR>(t, a.pk_row + m.pko, h, m.nd);
     if (lane < h)
 #pragma unroll
         for (int r = 0; r < NR; ++r) dst[(size_t)(fr + lane) * NR + r] = t[r];
@@ -635,10 +675,9 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal 
         for (int L = 0; L < a.nl; ++L) {
             const int r0 = __ldg(sv.qb + L), nr = __ldg(sv.qe + L) - r0;
             for (int t = wid; t < nr; t += nwarps) {
-                const int I = __ldg(a.lvl_rows + r0 + t);
-                const int fr = __ldg(a.bs + I), h = __ldg(a.bs + I + 1) - fr;
+                const ItemMeta m = meta_of_row(a, __ldg(a.lvl_rows + r0 + t));
                 double tt[NR];
-                ut_item<TF, NR, kRhsCaller>(a, I, fr, h, __ldg(a.rowflags + I), a.b, one, a.v[0], tt);
+                ut_item<TF, NR, kRhsCaller>(a, m, a.b, one, a.v[0], tt);
             }
             ctx.sync();
         }
@@ -670,8 +709,8 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal 
         for (int L = a.nl - 1; L >= 0; --L) {
             const int r0 = __ldg(sv.qb + L), nr = __ldg(sv.qe + L) - r0;
             for (int t = wid; t < nr; t += nwarps) {
-                const int I = __ldg(a.lvl_rows + r0 + t);
-                const int fr = __ldg(a.bs + I), h = __ldg(a.bs + I + 1) - fr;
+                const ItemMeta m = meta_of_row(a, __ldg(a.lvl_rows + r0 + t));
+                const int fr = m.fr, h = m.h;
                 double y[NR], d[NR];
 #pragma unroll
                 for (int j = 0; j < NR; ++j) {
@@ -682,7 +721,7 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal 
                         a.v[0][o] = y[j];
                     }
                 }
-                u_item<TF, NR>(a, I, fr, h, y, a.ev, d);
+                u_item<TF, NR>(a, m, y, a.ev, d);
 #pragma unroll
                 for (int j = 0; j < NR; ++j) ww[j] = fma_rn(d[j], d[j], ww[j]);
             }
@@ -703,11 +742,10 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal 
         for (int L = 0; L < a.nl; ++L) {
             const int r0 = __ldg(sv.qb + L), nr = __ldg(sv.qe + L) - r0;
             for (int t = wid; t < nr; t += nwarps) {
-                const int I = __ldg(a.lvl_rows + r0 + t);
-                const int fr = __ldg(a.bs + I), h = __ldg(a.bs + I + 1) - fr;
-                const int flags = __ldg(a.rowflags + I);
+                const ItemMeta m = meta_of_row(a, __ldg(a.lvl_rows + r0 + t));
+                const int fr = m.fr, h = m.h, flags = m.flags;
                 double av[NR];
-                ut_item<TF, NR, kRhsSpmv>(a, I, fr, h, flags, a.ev, one, a.Av, av);
+                ut_item<TF, NR, kRhsSpmv>(a, m, a.ev, one, a.Av, av);
                 DBlock<TF> D;
                 D.load(a, fr, h, flags);
 #pragma unroll
@@ -764,8 +802,8 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal 
                 // block rows with a pivot tile, swaps or 2x2 pivots: warp per block row
                 const int c1 = __ldg(a.scan_c + q1);
                 for (int t = __ldg(a.scan_c + q0) + wid; t < c1; t += nwarps) {
-                    const int I = __ldg(a.cplx + t);
-                    const int fr = __ldg(a.bs + I), h = __ldg(a.bs + I + 1) - fr;
+                    const ItemMeta m = meta_of_item(a, t);
+                    const int fr = m.fr, h = m.h;
                     double y[NR], d[NR];
 #pragma unroll
                     for (int j = 0; j < NR; ++j) {
@@ -780,7 +818,7 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal 
                             y[j] = v;
                         }
                     }
-                    u_item<TF, NR>(a, I, fr, h, y, a.ev, d);
+                    u_item<TF, NR>(a, m, y, a.ev, d);
                 }
                 // rows of simple block rows: thread per row (u_item with D = d,
                 // an identity tile and no swaps)
@@ -862,12 +900,11 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal 
                 const int q0 = __ldg(sv.qb + L), q1 = __ldg(sv.qe + L);
                 const int c1 = __ldg(a.scan_c + q1);
                 for (int t = __ldg(a.scan_c + q0) + wid; t < c1; t += nwarps) {
-                    const int I = __ldg(a.cplx + t);
-                    const int fr = __ldg(a.bs + I), h = __ldg(a.bs + I + 1) - fr;
-                    const int flags = __ldg(a.rowflags + I);
+                    const ItemMeta m = meta_of_item(a, t);
+                    const int fr = m.fr, h = m.h, flags = m.flags;
                     double av[NR];
-                    if (L == 0) ut_item<TF, NR, kRhsSpmv>(a, I, fr, h, flags, a.ev, cf.sc, a.Av, av);
-                    else ut_item<TF, NR, kRhsPre>(a, I, fr, h, flags, a.ev, cf.sc, a.Av, av);
+                    if (L == 0) ut_item<TF, NR, kRhsSpmv>(a, m, a.ev, cf.sc, a.Av, av);
+                    else ut_item<TF, NR, kRhsPre>(a, m, a.ev, cf.sc, a.Av, av);
                     DBlock<TF> D;
                     D.load(a, fr, h, flags);
 #pragma unroll
@@ -924,9 +961,9 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal 
                             if (u < len) break;
                             u -= len;
                         }
-                        const int I = __ldg(a.cplx + __ldg(a.scan_c + __ldg(sv.qb + L2)) + (int)(u >> 5));
-                        const int ln = (int)(u & 31), fr = __ldg(a.bs + I);
-                        if (ln < __ldg(a.bs + I + 1) - fr) {
+                        const ItemMeta m = meta_of_item(a, __ldg(a.scan_c + __ldg(sv.qb + L2)) + (int)(u >> 5));
+                        const int ln = (int)(u & 31), fr = m.fr;
+                        if (ln < m.h) {
                             double y[NR];
                             spmv_row<TF, NR>(a, fr + ln, a.ev, y);
 #pragma unroll
@@ -1022,12 +1059,12 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal 
     for (int L = a.nl - 1; L >= 0; --L) {
         const int r0 = __ldg(sv.qb + L), nr = __ldg(sv.qe + L) - r0;
         for (int t = wid; t < nr; t += nwarps) {
-            const int I = __ldg(a.lvl_rows + r0 + t);
-            const int fr = __ldg(a.bs + I), h = __ldg(a.bs + I + 1) - fr;
+            const ItemMeta m = meta_of_row(a, __ldg(a.lvl_rows + r0 + t));
+            const int fr = m.fr, h = m.h;
             double y[NR], d[NR];
 #pragma unroll
             for (int j = 0; j < NR; ++j) y[j] = (lane < h) ? a.xt[(size_t)(fr + lane) * NR + j] : 0.0;
-            u_item<TF, NR>(a, I, fr, h, y, a.ev, d);
+            u_item<TF, NR>(a, m, y, a.ev, d);
         }
         ctx.sync();
     }
@@ -1167,6 +1204,7 @@ PArgs<TF> make_args(Csr* A, Factor* M, double* base, double* partials, const dou
     a.scan_c = M->scan_c.as<int>();
     a.simple_rows = M->simple_rows.as<int>();
     a.cplx = M->cplx.as<int>();
+    a.citem = M->citem.as<CItem>();
     const size_t vn = (size_t)n * nr;
     for (int i = 0; i < 2; ++i) {
         a.v[i] = base + (size_t)i * vn;
