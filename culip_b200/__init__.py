@@ -24,7 +24,8 @@ from ._capi import (F32, F64, LEFT, MIDDLE, PIV_BK, PIV_ROOK, PIV_STATIC, RIGHT,
 __all__ = ["Handle", "Pattern", "Factor", "CsrOperator", "PermutePlan", "BlockiLDLt", "CSRMatrixSPMV", "SQMR", "kkt_generate",
            "kkt_blocking", "normal_vector", "CulipxError", "KKT_CONFIGS"]
 
-# The benchmark systems: K = [[H + delta I, A'], [A, -gamma I]] (see DESIGN.md for the construction)
+# The benchmark systems: K = [[H + delta I, A'], [A, -gamma I]] with H diagonal, log-uniform in
+# [hmin, hmax], and nnz_per_col N(0,1) entries per column of A (culipx_kkt_generate)
 KKT_CONFIGS = {
     "small": dict(n=2000, m=1000, nnz_per_col=4, band_half=0, hmin=1e-2, hmax=1e2, block=4),
     "scale": dict(n=200000, m=100000, nnz_per_col=6, band_half=32, hmin=1e-6, hmax=1e6, block=32),

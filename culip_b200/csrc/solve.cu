@@ -158,74 +158,201 @@ __global__ void k_count_offdiag(SweepBuild a, const T* val, int nblocks_total, i
     }
 }
 
-// rows of U: warp per block row, blocks in column order, each row in column order
+// The fill kernels below write one fine-row CSR per triangle, skipping stored
+// zeros: the rows of U (warp per block row, blocks in column order, each row
+// in column order) and the rows of U' = the columns of U (warp per block
+// column, blocks in row order, each row in row order).  The warp reads the descriptors of 32 blocks
+// at once (one lane each).  Runs of consecutive sparse blocks of 32 entries
+// or fewer in total go through one batch, a lane per entry: an entry's place
+// in its fine row is the count of batch entries of the same row that precede
+// it in (block, column) order (in (block, row) order for U'), added to the
+// row's next free position kept in shared memory.  Other blocks (dense, or
+// sparse with more than 32 entries, whose columns a pivot permutation may have
+// reordered) are placed in a shared tile and read back row by row.
+
+// per-lane descriptors of the chunk of up to 32 blocks a warp handles
+struct FillChunk {
+    long long off;   // value / index offset of lane's block
+    int first;       // fc (U) or fr (U') of lane's block
+    int ext;         // w (U) or h (U') of lane's block
+    int weight;      // sparse entries, or 33 for a block that takes the tile path
+    int incl;        // inclusive prefix of weight over the lanes
+};
+
+constexpr int kFillBig = 33;
+
+__device__ __forceinline__ int warp_incl_scan(int v)
+{
+    const int lane = lane_id();
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += t;
+    }
+    return v;
+}
+
+// one batch of the small sparse blocks j..k-1 of the chunk; TRANS: U' (rows
+// of U' are columns of the blocks, keyed by block and row)
+template <class T, bool TRANS>
+__device__ __forceinline__ void fill_small_batch(const FillChunk& ch, int j, int k, int base, int wfix,
+                                                 const T* val, const int* idx, int* next, int* out_col,
+                                                 T* out_val)
+{
+    const int lane = lane_id();
+    const int E = shfl(ch.incl, k - 1) - base;
+    int bl = j;  // block of this lane's entry: first l with incl[l] - base > lane
+    for (int l = j; l < k - 1; ++l)
+        if (shfl(ch.incl, l) - base <= lane) bl = l + 1;
+    const int e = lane - (shfl(ch.incl, bl) - shfl(ch.weight, bl) - base);
+    const long long off = shfl(ch.off, bl);
+    const int first = shfl(ch.first, bl);
+    const int w = TRANS ? wfix : shfl(ch.ext, bl);
+    const bool in = lane < E;
+    int li = 0;
+    T v = T(0);
+    if (in) {
+        li = idx[off + e];
+        v = val[off + e];
+    }
+    const int r = li / w, c = li - r * w;
+    const bool nz = in && v != T(0);
+    const unsigned nzm = __ballot_sync(0xffffffffu, nz);
+    const int row = TRANS ? c : r;          // output row within the warp's block row / column
+    const int key = bl * 32 + (TRANS ? r : c);  // order within that output row
+    int rank = 0;
+    for (int t = 0; t < E; ++t) {
+        const int rt = shfl(row, t), kt = shfl(key, t);
+        rank += (int)(((nzm >> t) & 1u) && rt == row && kt < key);
+    }
+    if (nz) {
+        const int p = next[row] + rank;
+        out_col[p] = first + (TRANS ? r : c);
+        out_val[p] = v;
+    }
+    __syncwarp();
+    if (nz) atomicAdd(&next[row], 1);
+    __syncwarp();
+}
+
 template <class T>
 __global__ void __launch_bounds__(32 * kSweepWarps) k_fill_u_rows(SweepBuild a, const T* val, int cm,
                                                                    const int* u_off, int* u_col, T* u_val)
 {
     __shared__ T tiles[kSweepWarps][kTileElems];
+    __shared__ int next_s[kSweepWarps][32];
     const int warp = threadIdx.x >> 5;
     const int I = blockIdx.x * kSweepWarps + warp;
     if (I >= cm) return;
     const int lane = lane_id();
     T* tile = tiles[warp];
+    int* next = next_s[warp];  // next free position of fine row fr + i
     for (int e = lane; e < kTileElems; e += 32) tile[e] = T(0);
-    __syncwarp();
     const int fr = a.bs[I], h = a.bs[I + 1] - fr;
-    int run = 0;  // lane i: entries written so far in row fr + i
-    for (int q = a.cs_off[I] + 1; q < a.cs_off[I + 1]; ++q) {
-        const int J = a.desc[q].col;
-        const int fc = a.bs[J], w = a.bs[J + 1] - fc;
-        load_block(tile, q, a.desc, a.bs, a.boff, a.nnz, a.fmt, val, a.idx, false);
-        for (int i = 0; i < h; ++i) {
-            const T v = (lane < w) ? tile[i * kTileStride + lane] : T(0);
-            const bool nz = v != T(0);
-            const unsigned m = __ballot_sync(0xffffffffu, nz);
-            const int base = u_off[fr + i] + shfl(run, i);
-            if (nz) {
-                const int pos = base + __popc(m & ((1u << lane) - 1u));
-                u_col[pos] = fc + lane;
-                u_val[pos] = v;
-            }
-            if (lane == i) run += __popc(m);
+    next[lane] = (lane < h) ? u_off[fr + lane] : 0;
+    __syncwarp();
+    const int q_end = a.cs_off[I + 1];
+    for (int q0 = a.cs_off[I] + 1; q0 < q_end; q0 += 32) {
+        const int nb = min(32, q_end - q0);
+        FillChunk ch{0, 0, 1, kFillBig, 0};
+        if (lane < nb) {
+            const int q = q0 + lane;
+            const int J = a.desc[q].col;
+            ch.first = a.bs[J];
+            ch.ext = a.bs[J + 1] - ch.first;
+            ch.off = a.boff[q];
+            const int cnt = (a.fmt[q] == 1) ? kFillBig : a.nnz[q];
+            ch.weight = (cnt <= 32) ? cnt : kFillBig;
         }
-        unload_block(tile, q, a.desc, a.bs, a.boff, a.nnz, a.fmt, a.idx);
+        ch.incl = warp_incl_scan(ch.weight);
+        for (int j = 0; j < nb;) {
+            const int base = shfl(ch.incl, j) - shfl(ch.weight, j);
+            const unsigned take = __ballot_sync(0xffffffffu, lane >= j && lane < nb && ch.incl - base <= 32);
+            const int k = j + __popc(take);
+            if (k > j) {
+                fill_small_batch<T, false>(ch, j, k, base, 0, val, a.idx, next, u_col, u_val);
+                j = k;
+                continue;
+            }
+            const int q = q0 + j;
+            const int fc = shfl(ch.first, j), w = shfl(ch.ext, j);
+            load_block(tile, q, a.desc, a.bs, a.boff, a.nnz, a.fmt, val, a.idx, false);
+            int mine = 0;
+            for (int i = 0; i < h; ++i) {
+                const T v = (lane < w) ? tile[i * kTileStride + lane] : T(0);
+                const bool nz = v != T(0);
+                const unsigned m = __ballot_sync(0xffffffffu, nz);
+                if (nz) {
+                    const int p = next[i] + __popc(m & ((1u << lane) - 1u));
+                    u_col[p] = fc + lane;
+                    u_val[p] = v;
+                }
+                if (lane == i) mine = __popc(m);
+            }
+            __syncwarp();
+            if (lane < h) next[lane] += mine;
+            unload_block(tile, q, a.desc, a.bs, a.boff, a.nnz, a.fmt, a.idx);
+            ++j;
+        }
     }
 }
 
-// rows of U' (columns of U): warp per block column, blocks in row order
 template <class T>
 __global__ void __launch_bounds__(32 * kSweepWarps) k_fill_ut_rows(SweepBuild a, const T* val, int cm,
                                                                     const int* ut_off, int* ut_col, T* ut_val)
 {
     __shared__ T tiles[kSweepWarps][kTileElems];
+    __shared__ int next_s[kSweepWarps][32];
     const int warp = threadIdx.x >> 5;
     const int J = blockIdx.x * kSweepWarps + warp;
     if (J >= cm) return;
     const int lane = lane_id();
     T* tile = tiles[warp];
+    int* next = next_s[warp];  // next free position of U' row fc + c
     for (int e = lane; e < kTileElems; e += 32) tile[e] = T(0);
-    __syncwarp();
     const int fc = a.bs[J], w = a.bs[J + 1] - fc;
-    int run = 0;  // lane c: entries written so far in U' row fc + c
-    for (int q = a.csc_off[J]; q < a.csc_off[J + 1] - 1; ++q) {
-        const int b = a.csc_blk[q];
-        const int K = a.desc[b].row;
-        const int fr = a.bs[K], h = a.bs[K + 1] - fr;
-        load_block(tile, b, a.desc, a.bs, a.boff, a.nnz, a.fmt, val, a.idx, false);
-        for (int c = 0; c < w; ++c) {
-            const T v = (lane < h) ? tile[lane * kTileStride + c] : T(0);
-            const bool nz = v != T(0);
-            const unsigned m = __ballot_sync(0xffffffffu, nz);
-            const int base = ut_off[fc + c] + shfl(run, c);
-            if (nz) {
-                const int pos = base + __popc(m & ((1u << lane) - 1u));
-                ut_col[pos] = fr + lane;
-                ut_val[pos] = v;
-            }
-            if (lane == c) run += __popc(m);
+    next[lane] = (lane < w) ? ut_off[fc + lane] : 0;
+    __syncwarp();
+    const int q_end = a.csc_off[J + 1] - 1;  // the pivot block closes the column
+    for (int q0 = a.csc_off[J]; q0 < q_end; q0 += 32) {
+        const int nb = min(32, q_end - q0);
+        FillChunk ch{0, 0, 1, kFillBig, 0};
+        if (lane < nb) {
+            const int b = a.csc_blk[q0 + lane];
+            const int K = a.desc[b].row;
+            ch.first = a.bs[K];
+            ch.ext = a.bs[K + 1] - ch.first;
+            ch.off = a.boff[b];
+            const int cnt = (a.fmt[b] == 1) ? kFillBig : a.nnz[b];
+            ch.weight = (cnt <= 32) ? cnt : kFillBig;
         }
-        unload_block(tile, b, a.desc, a.bs, a.boff, a.nnz, a.fmt, a.idx);
+        ch.incl = warp_incl_scan(ch.weight);
+        for (int j = 0; j < nb;) {
+            const int base = shfl(ch.incl, j) - shfl(ch.weight, j);
+            const unsigned take = __ballot_sync(0xffffffffu, lane >= j && lane < nb && ch.incl - base <= 32);
+            const int k = j + __popc(take);
+            if (k > j) {
+                fill_small_batch<T, true>(ch, j, k, base, w, val, a.idx, next, ut_col, ut_val);
+                j = k;
+                continue;
+            }
+            const int b = a.csc_blk[q0 + j];
+            const int fr = shfl(ch.first, j), h = shfl(ch.ext, j);
+            load_block(tile, b, a.desc, a.bs, a.boff, a.nnz, a.fmt, val, a.idx, false);
+            if (lane < w) {  // lane c owns U' row fc + c; the block's rows in order
+                int p = next[lane];
+                for (int i = 0; i < h; ++i) {
+                    const T v = tile[i * kTileStride + lane];
+                    if (v != T(0)) {
+                        ut_col[p] = fr + i;
+                        ut_val[p] = v;
+                        ++p;
+                    }
+                }
+                next[lane] = p;
+            }
+            unload_block(tile, b, a.desc, a.bs, a.boff, a.nnz, a.fmt, a.idx);
+            ++j;
+        }
     }
 }
 

@@ -97,13 +97,18 @@ def test_factor_scrambled_exact(handle, seed, fill_level):
 
 
 @pytest.mark.parametrize("stage", [cb.LEFT, cb.MIDDLE, cb.RIGHT])
-@pytest.mark.parametrize("case", ["small", "scrambled"])
+@pytest.mark.parametrize("case", ["small", "scrambled", "small_fill1", "b32_fill1"])
 def test_prec_apply(handle, stage, case):
-    if case == "small":
+    """The fill cases give block rows and columns of more than 32 blocks and
+    sparse blocks of more than 32 entries (both paths of the sweep build)."""
+    fill = 1 if case.endswith("fill1") else 0
+    if case.startswith("small"):
         rp, ci, v, bs = kkt("small")
+    elif case == "b32_fill1":
+        rp, ci, v, bs = kkt("small", block=32)
     else:
         rp, ci, v, bs = scrambled_kkt(seed=7)
-    S, OF, P, F = _factor_both(handle, rp, ci, v, bs)
+    S, OF, P, F = _factor_both(handle, rp, ci, v, bs, fill_level=fill)
     b = cb.normal_vector(11, len(rp) - 1)
     xo = OF.apply(stage, b)
     xg = F.apply(stage, torch.from_numpy(b).cuda()).cpu().numpy()
