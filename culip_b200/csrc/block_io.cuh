@@ -52,22 +52,17 @@ __device__ __forceinline__ unsigned load_block(T* tile, int b, const DevBlock* d
     return load_block_at(tile, h, w, dense, boff[b], dense ? 0 : nnz[b], val, idx, zero_first);
 }
 
-// zero what load_block placed (sparse) or the h x w region (dense)
+// zero what load_block_at placed (sparse) or the h x w region (dense)
 template <class T>
-__device__ __forceinline__ void unload_block(T* tile, int b, const DevBlock* desc, const int* bs,
-                                             const long long* boff, const int* nnz, const int* fmt, const int* idx)
+__device__ __forceinline__ void unload_block_at(T* tile, int h, int w, bool dense, long long off, int cnt,
+                                                const int* idx)
 {
     const int lane = lane_id();
-    const DevBlock d = desc[b];
-    const int h = bs[d.row + 1] - bs[d.row];
-    const int w = bs[d.col + 1] - bs[d.col];
     __syncwarp();
-    if (fmt[b] == 1) {
+    if (dense) {
         if (lane < w)
             for (int i = 0; i < h; ++i) tile[i * kTileStride + lane] = T(0);
     } else {
-        const long long off = boff[b];
-        const int cnt = nnz[b];
         for (int e = lane; e < cnt; e += 32) {
             const int li = idx[off + e];
             const int r = li / w, c = li - r * w;
@@ -75,6 +70,18 @@ __device__ __forceinline__ void unload_block(T* tile, int b, const DevBlock* des
         }
     }
     __syncwarp();
+}
+
+// zero what load_block placed
+template <class T>
+__device__ __forceinline__ void unload_block(T* tile, int b, const DevBlock* desc, const int* bs,
+                                             const long long* boff, const int* nnz, const int* fmt, const int* idx)
+{
+    const DevBlock d = desc[b];
+    const int h = bs[d.row + 1] - bs[d.row];
+    const int w = bs[d.col + 1] - bs[d.col];
+    const bool dense = fmt[b] == 1;
+    unload_block_at(tile, h, w, dense, boff[b], dense ? 0 : nnz[b], idx);
 }
 
 }  // namespace culipx

@@ -125,15 +125,77 @@ __global__ void __launch_bounds__(32 * kWarps) k_pivot_blocks(FactorArgs a, T* v
     for (int e = lane; e < kTileElems; e += 32) Q[e] = T(0);
     load_block(Tt, b, a.desc, a.bs, a.boff, a.nnz, a.fmt, val, a.idx, true);
 
+    // The fan-in updates in column order.  The descriptors of 32 update blocks
+    // are read at once (a lane each); the entries of a sparse block of up to 32
+    // entries and the D of its rows are loaded while the previous block's
+    // update runs.  The update order and arithmetic are those of one block at a
+    // time.
     const int q_beg = a.csc_off[I];
     const int q_end = a.csc_off[I + 1] - 1;  // the last block of the column is the pivot
-    for (int q = q_beg; q < q_end; ++q) {
-        const int kb = a.csc_blk[q];
-        const int K = a.desc[kb].row;
-        const int bw = a.bs[K + 1] - a.bs[K];
-        const unsigned cm = load_block(Q, kb, a.desc, a.bs, a.boff, a.nnz, a.fmt, val, a.idx, false);
-        schur_update(Tt, Q, Q, cm, bw, len, tri + 3 * (size_t)a.bs[K]);
-        unload_block(Q, kb, a.desc, a.bs, a.boff, a.nnz, a.fmt, a.idx);
+    for (int q0 = q_beg; q0 < q_end; q0 += 32) {
+        const int nb = min(32, q_end - q0);
+        int c_bw = 0, c_trow = 0, c_cnt = 0, c_dense = 0;
+        long long c_off = 0;
+        if (lane < nb) {
+            const int kb = a.csc_blk[q0 + lane];
+            const int K = a.desc[kb].row;
+            c_trow = a.bs[K];
+            c_bw = a.bs[K + 1] - c_trow;
+            c_off = a.boff[kb];
+            c_dense = a.fmt[kb] == 1;
+            c_cnt = c_dense ? 0 : a.nnz[kb];
+        }
+        // block j's prefetched entry (lane e < cnt) and D rows (lane < bw)
+        auto fetch = [&](int j, int& li, T& v, T& sup, T& dia, T& sub) {
+            const int bw = shfl(c_bw, j), cnt = shfl(c_cnt, j), trow = shfl(c_trow, j);
+            const long long off = shfl(c_off, j);
+            const bool small = !shfl(c_dense, j) && cnt <= 32;
+            li = 0;
+            v = T(0);
+            if (small && lane < cnt) {
+                li = a.idx[off + lane];
+                v = val[off + lane];
+            }
+            sup = dia = sub = T(0);
+            if (lane < bw) {
+                const T* tk = tri + 3 * (size_t)(trow + lane);
+                sup = tk[0];
+                dia = tk[1];
+                sub = tk[2];
+            }
+        };
+        int li;
+        T v, sup, dia, sub;
+        fetch(0, li, v, sup, dia, sub);
+        for (int j = 0; j < nb; ++j) {
+            int nli = 0;
+            T nv = T(0), nsup = T(0), ndia = T(0), nsub = T(0);
+            if (j + 1 < nb) fetch(j + 1, nli, nv, nsup, ndia, nsub);
+            const int bw = shfl(c_bw, j), cnt = shfl(c_cnt, j);
+            const long long off = shfl(c_off, j);
+            const bool dense = shfl(c_dense, j);
+            const bool small = !dense && cnt <= 32;
+            unsigned cm;
+            if (small) {  // the placement load_block_at does, from registers
+                const int r = li / len, c = li - r * len;
+                if (lane < cnt) Q[r * kTileStride + c] = v;
+                cm = (lane < cnt && v != T(0)) ? (1u << c) : 0u;
+                for (int o = 16; o > 0; o >>= 1) cm |= __shfl_xor_sync(0xffffffffu, cm, o);
+                __syncwarp();
+                schur_update_d(Tt, Q, Q, cm, bw, len, sup, dia, sub);
+                if (lane < cnt) Q[r * kTileStride + c] = T(0);
+                __syncwarp();
+            } else {
+                cm = load_block_at(Q, bw, len, dense, off, cnt, val, a.idx, false);
+                schur_update_d(Tt, Q, Q, cm, bw, len, sup, dia, sub);
+                unload_block_at(Q, bw, len, dense, off, cnt, a.idx);
+            }
+            li = nli;
+            v = nv;
+            sup = nsup;
+            dia = ndia;
+            sub = nsub;
+        }
     }
     __syncwarp();
     // A diagonal tile under BK / Rook pivoting takes a 1x1 pivot at every step
@@ -186,70 +248,117 @@ __global__ void __launch_bounds__(32 * kWarps) k_pivot_blocks(FactorArgs a, T* v
                         (no_updates ? kRowNoUpdates : 0);
 }
 
+// U_ij entry (row r of the block) from A_ij's entry v: the Givens-form left
+// solve with the 1x1 pivot D_r
+template <class T>
+__device__ __forceinline__ T offdiag_fast_entry(const T* D, int h, int r, T v)
+{
+    const T d11 = D[3 * r + 1], d12 = D[3 * r + 2];
+    const T d22 = (r < 31) ? ((r + 1 < h) ? D[3 * (r + 1) + 1] : T(0)) : D[3 * 31 + 1];
+    const T gr = sqrt(fma_rn(d11, d11, d12 * d12));
+    const T gc = d11 / gr, gs = d12 / gr;
+    const T td11 = fma_rn(gc, d11, gs * d12);
+    const T td12 = fma_rn(gc, d12, gs * d22);
+    T x1 = fma_rn(gc, v, gs * T(0));
+    x1 = fma_rn(-td12, T(0), x1) / td11;
+    return x1;
+}
+
 // Off-diagonal blocks of rows with no fan-in updates, an identity pivot tile,
 // 1x1 pivots only and no swaps: U_ij = D_i^-1 A_ij entry by entry, with the
 // same Givens-form arithmetic as the tiled path (d_left_solve_with_D_Ut
 // :1536-1557 reduces to x = (c a) / |d|); |u| <= NZ_EPS dropped, compacted in
 // place in row-major order.  Every other block goes to the slow list that
 // k_offdiag<kFirst> processes.
+//
+// A warp takes 32 consecutive blocks of the level's list, a lane each for the
+// descriptors; fast blocks of up to kLaneEntries entries are done by their
+// lane (the entries in order, so the compaction is the warp path's), larger
+// ones by the whole warp.  The level's leftover capacity is summed per warp
+// and added once.
+constexpr int kLaneEntries = 8;
+
 template <class T>
 __global__ void k_offdiag_fast(FactorArgs a, T* val, const T* tri, int lb_first, int noff, int allow)
 {
     const int lane = lane_id();
     const int nw = (gridDim.x * blockDim.x) >> 5;
-    for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < noff; t += nw) {
-        const int b = a.lb[lb_first + t];
-        const DevBlock d = a.desc[b];
-        const int flags = a.rowflags[d.row];
-        const bool fast = allow && a.fmt[b] == 0 &&
-                          (flags & (kRowIdentity | kRowHas2x2 | kRowPermIdentity | kRowNoUpdates)) ==
-                              (kRowIdentity | kRowPermIdentity | kRowNoUpdates);
-        if (!fast) {
-            if (lane == 0) {
-                const int slot = (int)atomicAdd(reinterpret_cast<unsigned long long*>(&a.state[kStSlow]), 1ull);
-                a.slowlist[slot] = t;
-            }
-            continue;
+    unsigned long long left = 0;  // this lane's share of the level's leftover capacity
+    for (int t0 = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; t0 < noff; t0 += nw * 32) {
+        const int t = t0 + lane;
+        int b = 0, cnt = 0, from = 0, h = 0, w = 1;
+        long long off = 0;
+        bool fast = false;
+        if (t < noff) {
+            b = a.lb[lb_first + t];
+            const DevBlock d = a.desc[b];
+            const int flags = a.rowflags[d.row];
+            fast = allow && a.fmt[b] == 0 &&
+                   (flags & (kRowIdentity | kRowHas2x2 | kRowPermIdentity | kRowNoUpdates)) ==
+                       (kRowIdentity | kRowPermIdentity | kRowNoUpdates);
+            from = a.bs[d.row];
+            h = a.bs[d.row + 1] - from;
+            w = a.bs[d.col + 1] - a.bs[d.col];
+            off = d.val_off;
+            cnt = a.nnz_init[b];
         }
-        const int from = a.bs[d.row], h = a.bs[d.row + 1] - from;
-        const int w = a.bs[d.col + 1] - a.bs[d.col];
-        const T* D = tri + 3 * (size_t)from;
-        const long long off = d.val_off;
-        const int cnt = a.nnz_init[b];
-        int o = 0;
-        for (int base = 0; base < cnt; base += 32) {
-            const int e = base + lane;
-            const bool valid = e < cnt;
-            const int li = valid ? a.idx[off + e] : 0;
-            const T v = valid ? val[off + e] : T(0);
-            T u = T(0);
-            if (valid) {
-                const int r = li / w;
-                const T d11 = D[3 * r + 1], d12 = D[3 * r + 2];
-                const T d22 = (r < 31) ? ((r + 1 < h) ? D[3 * (r + 1) + 1] : T(0)) : D[3 * 31 + 1];
-                const T gr = sqrt(fma_rn(d11, d11, d12 * d12));
-                const T gc = d11 / gr, gs = d12 / gr;
-                const T td11 = fma_rn(gc, d11, gs * d12);
-                const T td12 = fma_rn(gc, d12, gs * d22);
-                T x1 = fma_rn(gc, v, gs * T(0));
-                x1 = fma_rn(-td12, T(0), x1) / td11;
-                u = x1;
-            }
-            const bool nz = valid && fabs(u) > T(kNzEps);
-            const unsigned m = __ballot_sync(0xffffffffu, nz);
-            if (nz) {
-                const int pos = o + __popc(m & ((1u << lane) - 1u));
-                val[off + pos] = u;
-                a.idx[off + pos] = li;
-            }
-            o += __popc(m);
+        // every other block goes to the slow list
+        const bool slow = t < noff && !fast;
+        const unsigned sm = __ballot_sync(0xffffffffu, slow);
+        if (sm) {
+            int base = 0;
+            if (lane == 0)
+                base = (int)atomicAdd(reinterpret_cast<unsigned long long*>(&a.state[kStSlow]),
+                                      (unsigned long long)__popc(sm));
+            base = shfl(base, 0);
+            if (slow) a.slowlist[base + __popc(sm & ((1u << lane) - 1u))] = t;
         }
-        if (lane == 0) {
+        if (fast && cnt <= kLaneEntries) {
+            const T* D = tri + 3 * (size_t)from;
+            int o = 0;
+            for (int e = 0; e < cnt; ++e) {
+                const int li = a.idx[off + e];
+                const T u = offdiag_fast_entry(D, h, li / w, val[off + e]);
+                if (fabs(u) > T(kNzEps)) {
+                    val[off + o] = u;
+                    a.idx[off + o] = li;
+                    ++o;
+                }
+            }
             a.nnz[b] = o;
-            atomicAdd(reinterpret_cast<unsigned long long*>(&a.state[kStLevelAcc]),
-                      (unsigned long long)(long long)(a.cap[b] - o));
+            left += (unsigned long long)(long long)(a.cap[b] - o);
+        }
+        unsigned big = __ballot_sync(0xffffffffu, fast && cnt > kLaneEntries);
+        while (big) {
+            const int src = __ffs(big) - 1;
+            big &= big - 1;
+            const int bb = shfl(b, src), bcnt = shfl(cnt, src), bh = shfl(h, src), bw = shfl(w, src);
+            const long long boff = shfl(off, src);
+            const T* D = tri + 3 * (size_t)shfl(from, src);
+            int o = 0;
+            for (int base = 0; base < bcnt; base += 32) {
+                const int e = base + lane;
+                const bool valid = e < bcnt;
+                const int li = valid ? a.idx[boff + e] : 0;
+                const T v = valid ? val[boff + e] : T(0);
+                const T u = valid ? offdiag_fast_entry(D, bh, li / bw, v) : T(0);
+                const bool nz = valid && fabs(u) > T(kNzEps);
+                const unsigned m = __ballot_sync(0xffffffffu, nz);
+                if (nz) {
+                    const int pos = o + __popc(m & ((1u << lane) - 1u));
+                    val[boff + pos] = u;
+                    a.idx[boff + pos] = li;
+                }
+                o += __popc(m);
+            }
+            if (lane == 0) {
+                a.nnz[bb] = o;
+                left += (unsigned long long)(long long)(a.cap[bb] - o);
+            }
         }
     }
+    for (int o = 16; o > 0; o >>= 1) left += __shfl_xor_sync(0xffffffffu, left, o);
+    if (lane == 0 && left) atomicAdd(reinterpret_cast<unsigned long long*>(&a.state[kStLevelAcc]), left);
 }
 
 // Off-diagonal block (I, J) up to its final values in Tt: fan-in updates over
@@ -643,24 +752,53 @@ __global__ void k_pivot_columns(FactorArgs a, T* val, int lvl0, int nrows)
         if (v == lane) inv = l;
     }
     if (__all_sync(0xffffffffu, lane >= bw || inv == lane)) return;
-    for (int q = a.csc_off[I]; q < a.csc_off[I + 1] - 1; ++q) {
-        const int b = a.csc_blk[q];
-        const int hh = a.bs[a.desc[b].row + 1] - a.bs[a.desc[b].row];
-        const long long off = a.boff[b];
-        if (a.fmt[b] == 0) {
-            const int cnt = a.nnz[b];
-            for (int base = 0; base < cnt; base += 32) {
-                const int e = base + lane;
-                const int li = (e < cnt) ? a.idx[off + e] : 0;
+    __shared__ int inv_s[kWarps][32];
+    inv_s[warp][lane] = inv;
+    __syncwarp();
+    // 32 blocks of the column at a time, a lane each for the descriptors;
+    // sparse blocks of up to kLaneEntries entries are renumbered by their lane,
+    // the others by the whole warp
+    const int q_end = a.csc_off[I + 1] - 1;
+    for (int q0 = a.csc_off[I]; q0 < q_end; q0 += 32) {
+        const int nb = min(32, q_end - q0);
+        int hh = 0, cnt = 0;
+        bool dense = false;
+        long long off = 0;
+        if (lane < nb) {
+            const int b = a.csc_blk[q0 + lane];
+            const int K = a.desc[b].row;
+            hh = a.bs[K + 1] - a.bs[K];
+            off = a.boff[b];
+            dense = a.fmt[b] != 0;
+            cnt = dense ? 0 : a.nnz[b];
+        }
+        if (lane < nb && !dense && cnt <= kLaneEntries)
+            for (int e = 0; e < cnt; ++e) {
+                const int li = a.idx[off + e];
                 const int r = li / bw, c = li - r * bw;
-                const int nc = shfl(inv, c);
-                if (e < cnt) a.idx[off + e] = r * bw + nc;
+                a.idx[off + e] = r * bw + inv_s[warp][c];
             }
-        } else {
-            for (int i = 0; i < hh; ++i) {
-                const T v = (lane < bw) ? val[off + (long long)i * bw + lane] : T(0);
-                const T nv = shfl(v, lp);
-                if (lane < bw) val[off + (long long)i * bw + lane] = nv;
+        unsigned rest = __ballot_sync(0xffffffffu, lane < nb && (dense || cnt > kLaneEntries));
+        while (rest) {
+            const int src = __ffs(rest) - 1;
+            rest &= rest - 1;
+            const long long boff = shfl(off, src);
+            if (!shfl((int)dense, src)) {
+                const int bcnt = shfl(cnt, src);
+                for (int base = 0; base < bcnt; base += 32) {
+                    const int e = base + lane;
+                    const int li = (e < bcnt) ? a.idx[boff + e] : 0;
+                    const int r = li / bw, c = li - r * bw;
+                    const int nc = shfl(inv, c);
+                    if (e < bcnt) a.idx[boff + e] = r * bw + nc;
+                }
+            } else {
+                const int bh = shfl(hh, src);
+                for (int i = 0; i < bh; ++i) {
+                    const T v = (lane < bw) ? val[boff + (long long)i * bw + lane] : T(0);
+                    const T nv = shfl(v, lp);
+                    if (lane < bw) val[boff + (long long)i * bw + lane] = nv;
+                }
             }
         }
     }
@@ -737,7 +875,7 @@ int run_levels(Factor* f, const void* d_vals, cudaStream_t s, int* launches)
         if (noff > 0) {
             const int lbf = lb0 + npiv;
             const int dgrid = (std::min(noff, 148 * 16) + kWarps - 1) / kWarps;
-            k_offdiag_fast<T><<<std::min((noff + 7) / 8, 148 * 32), 256, 0, s>>>(a, val, tri, lbf, noff, thr ? 0 : 1);
+            k_offdiag_fast<T><<<std::min((noff + 255) / 256, 148 * 8), 256, 0, s>>>(a, val, tri, lbf, noff, thr ? 0 : 1);
             k_offdiag<T, kFirst><<<dgrid, 32 * kWarps, s3, s>>>(a, val, tri, lbf, noff, pivoting, row_norm, norm_part,
                                                                thv);
             *launches += 2;

@@ -16,17 +16,13 @@ __device__ __forceinline__ T bk_alpha() { return (T)((1.0f + sqrtf(17.0f)) / 8.0
 // Out[a][b] -= sum_r R[r][b] * (Q' D_k)[a][r] for a in colmask(Q), lanes b < rh.
 // Q: U_ki (bw x .), R: U_kj (bw x rh); D_k from tri at the rows of block k.
 // d_multiply_block_by_block_diagonal (:372-411) + d_apply_left_right_update.
+// schur_update_d takes lane r's entries of D_k (super, diagonal, sub; zero
+// for r >= bw) already loaded.
 template <class T>
-__device__ __forceinline__ void schur_update(T* out, const T* Q, const T* R, unsigned colmask, int bw, int rh,
-                             const T* tri_k)
+__device__ __forceinline__ void schur_update_d(T* out, const T* Q, const T* R, unsigned colmask, int bw, int rh,
+                                               T sup, T dia, T sub)
 {
     const int lane = lane_id();
-    T sup = T(0), dia = T(0), sub = T(0);
-    if (lane < bw) {
-        sup = tri_k[3 * lane];
-        dia = tri_k[3 * lane + 1];
-        sub = tri_k[3 * lane + 2];
-    }
     while (colmask) {
         const int a = __ffs(colmask) - 1;
         colmask &= colmask - 1;
@@ -48,6 +44,20 @@ __device__ __forceinline__ void schur_update(T* out, const T* Q, const T* R, uns
         if (lane < rh) out[a * kTileStride + lane] -= acc;
     }
     __syncwarp();
+}
+
+template <class T>
+__device__ __forceinline__ void schur_update(T* out, const T* Q, const T* R, unsigned colmask, int bw, int rh,
+                                             const T* tri_k)
+{
+    const int lane = lane_id();
+    T sup = T(0), dia = T(0), sub = T(0);
+    if (lane < bw) {
+        sup = tri_k[3 * lane];
+        dia = tri_k[3 * lane + 1];
+        sub = tri_k[3 * lane + 2];
+    }
+    schur_update_d(out, Q, R, colmask, bw, rh, sup, dia, sub);
 }
 
 // ---- dense pivot-block factorization (d_factor_pivot_factorize, :956-1083) ----

@@ -123,36 +123,66 @@ struct SweepBuild {
     const int* idx;
 };
 
-// per fine row of U and of U': number of non-zero off-diagonal entries
+// per fine row of U and of U': number of non-zero off-diagonal entries.  A
+// warp takes 32 consecutive blocks, a lane each for the descriptors; sparse
+// blocks of up to kCountLane entries are counted by their lane, the others by
+// the whole warp.
+constexpr int kCountLane = 8;
+
 template <class T>
 __global__ void k_count_offdiag(SweepBuild a, const T* val, int nblocks_total, int* cnt_u, int* cnt_ut)
 {
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
     const int lane = lane_id();
-    for (int b = warp; b < nblocks_total; b += nwarps) {
-        const DevBlock d = a.desc[b];
-        if (d.row == d.col) continue;
-        const int fr = a.bs[d.row], h = a.bs[d.row + 1] - fr;
-        const int fc = a.bs[d.col], w = a.bs[d.col + 1] - fc;
-        const long long off = a.boff[b];
-        if (a.fmt[b] == 1) {
-            int colcount = 0;
-            for (int i = 0; i < h; ++i) {
-                const bool nz = lane < w && val[off + (long long)i * w + lane] != T(0);
-                const unsigned m = __ballot_sync(0xffffffffu, nz);
-                if (lane == 0 && m) atomicAdd(&cnt_u[fr + i], __popc(m));
-                colcount += nz;
-            }
-            if (lane < w && colcount) atomicAdd(&cnt_ut[fc + lane], colcount);
-        } else {
-            const int cnt = a.nnz[b];
-            for (int e = lane; e < cnt; e += 32) {
+    for (int b0 = warp * 32; b0 < nblocks_total; b0 += nwarps * 32) {
+        const int b = b0 + lane;
+        int fr = 0, h = 0, fc = 0, w = 1, cnt = 0;
+        bool use = false, dense = false;
+        long long off = 0;
+        if (b < nblocks_total) {
+            const DevBlock d = a.desc[b];
+            use = d.row != d.col;
+            fr = a.bs[d.row];
+            h = a.bs[d.row + 1] - fr;
+            fc = a.bs[d.col];
+            w = a.bs[d.col + 1] - fc;
+            off = a.boff[b];
+            dense = a.fmt[b] == 1;
+            cnt = dense ? 0 : a.nnz[b];
+        }
+        if (use && !dense && cnt <= kCountLane)
+            for (int e = 0; e < cnt; ++e) {
                 if (val[off + e] == T(0)) continue;
                 const int li = a.idx[off + e];
                 const int r = li / w, c = li - r * w;
                 atomicAdd(&cnt_u[fr + r], 1);
                 atomicAdd(&cnt_ut[fc + c], 1);
+            }
+        unsigned rest = __ballot_sync(0xffffffffu, use && (dense || cnt > kCountLane));
+        while (rest) {
+            const int src = __ffs(rest) - 1;
+            rest &= rest - 1;
+            const int bfr = shfl(fr, src), bh = shfl(h, src), bfc = shfl(fc, src), bw = shfl(w, src);
+            const long long boff = shfl(off, src);
+            if (shfl((int)dense, src)) {
+                int colcount = 0;
+                for (int i = 0; i < bh; ++i) {
+                    const bool nz = lane < bw && val[boff + (long long)i * bw + lane] != T(0);
+                    const unsigned m = __ballot_sync(0xffffffffu, nz);
+                    if (lane == 0 && m) atomicAdd(&cnt_u[bfr + i], __popc(m));
+                    colcount += nz;
+                }
+                if (lane < bw && colcount) atomicAdd(&cnt_ut[bfc + lane], colcount);
+            } else {
+                const int bcnt = shfl(cnt, src);
+                for (int e = lane; e < bcnt; e += 32) {
+                    if (val[boff + e] == T(0)) continue;
+                    const int li = a.idx[boff + e];
+                    const int r = li / bw, c = li - r * bw;
+                    atomicAdd(&cnt_u[bfr + r], 1);
+                    atomicAdd(&cnt_ut[bfc + c], 1);
+                }
             }
         }
     }

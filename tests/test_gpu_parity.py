@@ -24,14 +24,15 @@ def handle():
     return cb.Handle(0)
 
 
-def _factor_both(handle, rp, ci, v, bs, fill_level=0, pivot=cb.PIV_BK, precision=cb.F64, is_piv=None):
+def _factor_both(handle, rp, ci, v, bs, fill_level=0, pivot=cb.PIV_BK, precision=cb.F64, is_piv=None,
+                 threshold=0.0):
     dt = np.float64 if precision == cb.F64 else np.float32
     S = oracle.Sym(rp, ci, bs, fill_level, 1.0, dtype=dt)
-    OF = S.factor(v.astype(dt), is_piv=is_piv, pivot=pivot)
+    OF = S.factor(v.astype(dt), is_piv=is_piv, pivot=pivot, threshold=threshold)
     P = cb.Pattern(handle, rp, ci, bs, fill_level, 1.0, precision)
     F = cb.Factor(P)
     tv = torch.from_numpy(v.astype(dt)).cuda()
-    F.compute(tv, is_piv=is_piv, pivot=pivot)
+    F.compute(tv, is_piv=is_piv, pivot=pivot, threshold=threshold)
     return S, OF, P, F
 
 
@@ -48,6 +49,24 @@ def test_factor_small_kkt_exact(handle, pivot):
     rp, ci, v, bs = kkt("small")
     S, OF, P, F = _factor_both(handle, rp, ci, v, bs, pivot=pivot)
     _assert_factor_equal(OF.export(), F.export())
+
+
+@pytest.mark.parametrize("precision", [cb.F64, cb.F32])
+@pytest.mark.parametrize("threshold", [0.0, 1e-3])
+def test_factor_banded_b32_exact(handle, precision, threshold):
+    """32-row blocks with a banded half of A: update columns of more than 32
+    blocks, sparse blocks of more than 8 and of more than 32 entries (every
+    path of the pivot-block updates and of the entrywise off-diagonal pass);
+    with a drop threshold every off-diagonal block takes the tiled pass."""
+    rp, ci, v, bs = kkt("small", block=32, band_half=16)
+    S, OF, P, F = _factor_both(handle, rp, ci, v, bs, precision=precision, threshold=threshold)
+    _assert_factor_equal(OF.export(), F.export())
+    b = cb.normal_vector(5, len(rp) - 1)
+    dt = np.float64 if precision == cb.F64 else np.float32
+    for stage in (cb.LEFT, cb.MIDDLE, cb.RIGHT):
+        xo = OF.apply(stage, b.astype(dt))
+        xg = F.apply(stage, torch.from_numpy(b.astype(dt)).cuda()).cpu().numpy()
+        assert np.array_equal(xo, xg), stage
 
 
 @pytest.mark.parametrize("precision", [cb.F64, cb.F32])
