@@ -614,6 +614,7 @@ struct SysView {
 template <int NR>
 struct Coef {
     double sc[NR], nbrr[NR], ne[NR], ir[NR], tau[NR];
+    double na[NR], nb[NR];  // the U sweep's -alpha, -beta_k
     bool act[NR];  // right-hand sides still iterating (x of the others is final)
 };
 
@@ -624,7 +625,7 @@ struct Coef {
 template <class TF, int NR>
 __device__ __forceinline__ void simple_epilogue(const PArgs<TF>& a, int g, const double (&av)[NR], const double* vk,
                                                 double* vk1, const double* pkm1, const double* pkm2, double* pk,
-                                                const Coef<NR>& cf, double (&r)[4 * NR])
+                                                const volatile Coef<NR>& cf, double (&r)[4 * NR])
 {
     const double dd = (double)__ldg(a.dg + g);
 #pragma unroll
@@ -660,6 +661,7 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal 
     const int tid = threadIdx.x, lane = (int)lane_id();
     const int wid = ctx.wid, nwarps = ctx.nwarps;
     const int row0 = sv.row0, row1 = sv.row1;
+    __shared__ Coef<NR> cfs;  // the U' phase's coefficients, written by thread 0
     if (tid == 0)
         for (int j = 0; j < NR; ++j) {
             memset(&S[j], 0, sizeof(Scal));
@@ -782,12 +784,16 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal 
         if (!any || it >= a.max_it) break;
         const int k0 = acc3(it), k1 = acc3(it + 1), km1 = acc3(it - 1);
         if (NR == 1) stamp(a.ts, it, 0);
-        double na[NR], nb[NR];
-#pragma unroll
-        for (int j = 0; j < NR; ++j) {
-            na[j] = -S[j].alpha_next;
-            nb[j] = -S[j].beta[k0];
-        }
+        // -alpha and -beta_k of each right-hand side, read from shared memory
+        // where used (registers are the kernel's scarce resource)
+        if (tid == 0)
+            for (int j = 0; j < NR; ++j) {
+                cfs.na[j] = -S[j].alpha_next;
+                cfs.nb[j] = -S[j].beta[k0];
+            }
+        __syncthreads();
+        const volatile double* const na = cfs.na;
+        const volatile double* const nb = cfs.nb;
         const double* const vk = a.v[it & 1];
         double* const vk1 = a.v[(it + 1) & 1];
         const double* const vkm1 = vk1;  // read, then overwritten element by element
@@ -872,6 +878,15 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal 
                     Q.tau = c * Q.gamma;
                     Q.gamma = s * Q.gamma;
                 }
+            if (tid == 0)
+                for (int j = 0; j < NR; ++j) {
+                    cfs.sc[j] = S[j].inv_delta;
+                    cfs.nbrr[j] = -S[j].beta_rr;
+                    cfs.ne[j] = -S[j].epsilon;
+                    cfs.ir[j] = S[j].inv_rho;
+                    cfs.tau[j] = S[j].tau;
+                    cfs.act[j] = !S[j].done;
+                }
             __syncthreads();
         }
         if (NR == 1) {
@@ -883,16 +898,7 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal 
             double r[4 * NR];
 #pragma unroll
             for (int j = 0; j < 4 * NR; ++j) r[j] = 0.0;
-            Coef<NR> cf;
-#pragma unroll
-            for (int j = 0; j < NR; ++j) {
-                cf.sc[j] = S[j].inv_delta;
-                cf.nbrr[j] = -S[j].beta_rr;
-                cf.ne[j] = -S[j].epsilon;
-                cf.ir[j] = S[j].inv_rho;
-                cf.tau[j] = S[j].tau;
-                cf.act[j] = !S[j].done;
-            }
+            const volatile Coef<NR>& cf = cfs;
             double* const pk = a.p[it & 1];
             const double* const pkm1 = a.p[(it + 1) & 1];
             const double* const pkm2 = pk;  // read, then overwritten element by element
@@ -903,8 +909,11 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal 
                     const ItemMeta m = meta_of_item(a, t);
                     const int fr = m.fr, h = m.h, flags = m.flags;
                     double av[NR];
-                    if (L == 0) ut_item<TF, NR, kRhsSpmv>(a, m, a.ev, cf.sc, a.Av, av);
-                    else ut_item<TF, NR, kRhsPre>(a, m, a.ev, cf.sc, a.Av, av);
+                    double scv[NR];
+#pragma unroll
+                    for (int j = 0; j < NR; ++j) scv[j] = cf.sc[j];
+                    if (L == 0) ut_item<TF, NR, kRhsSpmv>(a, m, a.ev, scv, a.Av, av);
+                    else ut_item<TF, NR, kRhsPre>(a, m, a.ev, scv, a.Av, av);
                     DBlock<TF> D;
                     D.load(a, fr, h, flags);
 #pragma unroll
