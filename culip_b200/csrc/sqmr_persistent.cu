@@ -615,6 +615,10 @@ template <int NR>
 struct Coef {
     double sc[NR], nbrr[NR], ne[NR], ir[NR], tau[NR];
     double na[NR], nb[NR];  // the U sweep's -alpha, -beta_k
+    const double* vk;       // the iteration's v_k, v_k+1 (= v_k-1 on entry), p_k (= p_k-2 on entry), p_k-1
+    double* vk1;
+    double* pk;
+    const double* pkm1;
     bool act[NR];  // right-hand sides still iterating (x of the others is final)
 };
 
@@ -655,6 +659,21 @@ __device__ __forceinline__ void simple_epilogue(const PArgs<TF>& a, int g, const
 // at once (see the top of the file): every work item loads the factor and
 // K once for all of them; each right-hand side has its own scalars and stops
 // on its own test (its x is final from then on).
+// A level's work lists: pivot-tile items [c0, c1) of citem, simple rows
+// [s0, s1) of simple_rows.  The first kLvlCache levels' bounds are kept in
+// shared memory for the whole solve (each phase starts by reading them).
+struct LvlBounds {
+    int c0, c1, s0, s1;
+};
+constexpr int kLvlCache = 32;
+
+template <class TF>
+__device__ __forceinline__ LvlBounds level_bounds(const PArgs<TF>& a, const SysView& sv, int L)
+{
+    const int q0 = __ldg(sv.qb + L), q1 = __ldg(sv.qe + L);
+    return LvlBounds{__ldg(a.scan_c + q0), __ldg(a.scan_c + q1), __ldg(a.scan_s + q0), __ldg(a.scan_s + q1)};
+}
+
 template <class TF, int NR, class Ctx>
 __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal (&S)[NR], double (*sh)[kW])
 {
@@ -662,12 +681,23 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal 
     const int wid = ctx.wid, nwarps = ctx.nwarps;
     const int row0 = sv.row0, row1 = sv.row1;
     __shared__ Coef<NR> cfs;  // the U' phase's coefficients, written by thread 0
-    if (tid == 0)
+    __shared__ LvlBounds lvb[kLvlCache];
+    __shared__ long long npre_s;  // rows of the pivot-tile items of levels >= 1
+    if (tid < kLvlCache && tid < a.nl) lvb[tid] = level_bounds(a, sv, tid);
+    if (tid == 0) {
         for (int j = 0; j < NR; ++j) {
             memset(&S[j], 0, sizeof(Scal));
             S[j].c[0] = -1.0;
         }
+        long long np = 0;
+        for (int L = 1; L < a.nl; ++L) {
+            const LvlBounds b = level_bounds(a, sv, L);
+            np += 32LL * (b.c1 - b.c0);
+        }
+        npre_s = np;
+    }
     __syncthreads();
+    auto lvl = [&](int L) -> LvlBounds { return L < kLvlCache ? lvb[L] : level_bounds(a, sv, L); };
 
     // ---- init: v0 = U'^-1 P' b; ||v0|| ----
     {
@@ -786,17 +816,20 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal 
         if (NR == 1) stamp(a.ts, it, 0);
         // -alpha and -beta_k of each right-hand side, read from shared memory
         // where used (registers are the kernel's scarce resource)
-        if (tid == 0)
+        if (tid == 0) {
             for (int j = 0; j < NR; ++j) {
                 cfs.na[j] = -S[j].alpha_next;
                 cfs.nb[j] = -S[j].beta[k0];
             }
+            cfs.vk = a.v[it & 1];
+            cfs.vk1 = a.v[(it + 1) & 1];
+            cfs.pk = a.p[it & 1];
+            cfs.pkm1 = a.p[(it + 1) & 1];
+        }
         __syncthreads();
+        const volatile Coef<NR>& cv = cfs;
         const volatile double* const na = cfs.na;
         const volatile double* const nb = cfs.nb;
-        const double* const vk = a.v[it & 1];
-        double* const vk1 = a.v[(it + 1) & 1];
-        const double* const vkm1 = vk1;  // read, then overwritten element by element
         // ---- U sweep on v+ = Av - alpha v - beta v- (each item computes and
         //      stores its rows' v+, kept unscaled), ||v+||^2 ----
         {
@@ -804,10 +837,10 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal 
 #pragma unroll
             for (int j = 0; j < NR; ++j) r[j] = 0.0;
             for (int L = a.nl - 1; L >= 0; --L) {
-                const int q0 = __ldg(sv.qb + L), q1 = __ldg(sv.qe + L);
+                const LvlBounds lb = lvl(L);
                 // block rows with a pivot tile, swaps or 2x2 pivots: warp per block row
-                const int c1 = __ldg(a.scan_c + q1);
-                for (int t = __ldg(a.scan_c + q0) + wid; t < c1; t += nwarps) {
+                const int c1 = lb.c1;
+                for (int t = lb.c0 + wid; t < c1; t += nwarps) {
                     const ItemMeta m = meta_of_item(a, t);
                     const int fr = m.fr, h = m.h;
                     double y[NR], d[NR];
@@ -817,8 +850,9 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal 
                         if (lane < h) {
                             const size_t o = (size_t)(fr + lane) * NR + j;
                             double v = a.Av[o];
-                            v = fma_rn(na[j], vk[o], v);
-                            v = fma_rn(nb[j], vkm1[o], v);
+                            double* const vk1 = cv.vk1;  // vk1 holds v_k-1 until written
+                            v = fma_rn(na[j], cv.vk[o], v);
+                            v = fma_rn(nb[j], vk1[o], v);
                             vk1[o] = v;
                             r[j] = fma_rn(v, v, r[j]);
                             y[j] = v;
@@ -828,8 +862,8 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal 
                 }
                 // rows of simple block rows: thread per row (u_item with D = d,
                 // an identity tile and no swaps)
-                const int s1 = __ldg(a.scan_s + q1);
-                for (int i = __ldg(a.scan_s + q0) + ctx.g0; i < s1; i += ctx.gstride) {
+                const int s1 = lb.s1;
+                for (int i = lb.s0 + ctx.g0; i < s1; i += ctx.gstride) {
                     const int g = __ldg(a.simple_rows + i);
                     const double dd = (double)__ldg(a.dg + g);
                     TF acc[NR];
@@ -837,8 +871,9 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal 
                     for (int j = 0; j < NR; ++j) {
                         const size_t o = (size_t)g * NR + j;
                         double v = a.Av[o];
-                        v = fma_rn(na[j], vk[o], v);
-                        v = fma_rn(nb[j], vkm1[o], v);
+                        double* const vk1 = cv.vk1;
+                        v = fma_rn(na[j], cv.vk[o], v);
+                        v = fma_rn(nb[j], vk1[o], v);
                         vk1[o] = v;
                         r[j] = fma_rn(v, v, r[j]);
                         acc[j] = (TF)(v / dd);
@@ -899,13 +934,10 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal 
 #pragma unroll
             for (int j = 0; j < 4 * NR; ++j) r[j] = 0.0;
             const volatile Coef<NR>& cf = cfs;
-            double* const pk = a.p[it & 1];
-            const double* const pkm1 = a.p[(it + 1) & 1];
-            const double* const pkm2 = pk;  // read, then overwritten element by element
             for (int L = 0; L < a.nl; ++L) {
-                const int q0 = __ldg(sv.qb + L), q1 = __ldg(sv.qe + L);
-                const int c1 = __ldg(a.scan_c + q1);
-                for (int t = __ldg(a.scan_c + q0) + wid; t < c1; t += nwarps) {
+                const LvlBounds lb = lvl(L);
+                const int c1 = lb.c1;
+                for (int t = lb.c0 + wid; t < c1; t += nwarps) {
                     const ItemMeta m = meta_of_item(a, t);
                     const int fr = m.fr, h = m.h, flags = m.flags;
                     double av[NR];
@@ -921,14 +953,16 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal 
                         double vkr = 0.0, vs = 0.0;
                         if (lane < h) {
                             const size_t o = (size_t)(fr + lane) * NR + j;
-                            vkr = vk[o];
+                            double* const vk1 = cv.vk1;
+                            vkr = cv.vk[o];
                             vs = vk1[o] * cf.sc[j];
                             vk1[o] = vs;
                             if (cf.act[j]) {
                                 // p_k = (v_k - beta_rr p_k-1 - epsilon p_k-2) / rho, x += tau p_k
                                 double p = vkr;
-                                p = fma_rn(cf.nbrr[j], pkm1[o], p);
-                                p = fma_rn(cf.ne[j], pkm2[o], p);
+                                double* const pk = cv.pk;  // holds p_k-2 until written
+                                p = fma_rn(cf.nbrr[j], cv.pkm1[o], p);
+                                p = fma_rn(cf.ne[j], pk[o], p);
                                 p = p * cf.ir[j];
                                 pk[o] = p;
                                 const double xv = fma_rn(cf.tau[j], p, a.xt[o]);
@@ -948,29 +982,27 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal 
                 // update wait for the next level's phase, whose threads are
                 // mostly free (the last level does them at once)
                 const bool last = (L == a.nl - 1);
-                const int s0 = __ldg(a.scan_s + q0), s1 = __ldg(a.scan_s + q1);
+                const int s0 = lb.s0, s1 = lb.s1;
                 // Level 0 also computes (K ev) / delta for the rows of the later
                 // levels' pivot-tile block rows and leaves it in Av at those rows:
                 // their items read it there instead of running the product on
                 // the critical path of a level of few, long items.  Units
                 // [0, npre) are those rows (lane ln of item t), the rest this
                 // level's simple rows, both spread over all threads.
-                long long npre = 0;
-                if (L == 0)
-                    for (int L2 = 1; L2 < a.nl; ++L2)
-                        npre += 32LL * (__ldg(a.scan_c + __ldg(sv.qe + L2)) - __ldg(a.scan_c + __ldg(sv.qb + L2)));
+                const long long npre = (L == 0) ? npre_s : 0;
                 const long long nunits = npre + (s1 - s0);
                 for (long long k = ctx.g0; k < nunits; k += ctx.gstride) {
                     if (k < npre) {
                         long long u = k;
                         int L2 = 1;
-                        for (;; ++L2) {
-                            const long long len =
-                                32LL * (__ldg(a.scan_c + __ldg(sv.qe + L2)) - __ldg(a.scan_c + __ldg(sv.qb + L2)));
+                        LvlBounds b2 = lvl(L2);
+                        for (;;) {
+                            const long long len = 32LL * (b2.c1 - b2.c0);
                             if (u < len) break;
                             u -= len;
+                            b2 = lvl(++L2);
                         }
-                        const ItemMeta m = meta_of_item(a, __ldg(a.scan_c + __ldg(sv.qb + L2)) + (int)(u >> 5));
+                        const ItemMeta m = meta_of_item(a, b2.c0 + (int)(u >> 5));
                         const int ln = (int)(u & 31), fr = m.fr;
                         if (ln < m.h) {
                             double y[NR];
@@ -993,24 +1025,24 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal 
                         av[j] = (double)acc[j];
                         a.Av[(size_t)g * NR + j] = av[j];
                     }
-                    if (last) simple_epilogue<TF, NR>(a, g, av, vk, vk1, pkm1, pkm2, pk, cf, r);
+                    if (last) simple_epilogue<TF, NR>(a, g, av, cv.vk, cv.vk1, cv.pkm1, cv.pk, cv.pk, cf, r);
                 }
                 if (L > 0) {
                     // warps without a block row in this level take the tails;
                     // if every warp has one, all threads do, after their items
-                    const int p0 = __ldg(sv.qb + L - 1), p1 = __ldg(sv.qe + L - 1);
-                    const int e1 = __ldg(a.scan_s + p1);
-                    const int items = c1 - __ldg(a.scan_c + q0);
+                    const LvlBounds pb = lvl(L - 1);
+                    const int e1 = pb.s1;
+                    const int items = c1 - lb.c0;
                     const bool spare = items < nwarps;
                     if (!spare || wid >= items) {
                         const int t0 = spare ? (wid - items) * 32 + lane : ctx.g0;
                         const int ts = spare ? (nwarps - items) * 32 : ctx.gstride;
-                        for (int i = __ldg(a.scan_s + p0) + t0; i < e1; i += ts) {
+                        for (int i = pb.s0 + t0; i < e1; i += ts) {
                             const int g = __ldg(a.simple_rows + i);
                             double av[NR];
 #pragma unroll
                             for (int j = 0; j < NR; ++j) av[j] = a.Av[(size_t)g * NR + j];
-                            simple_epilogue<TF, NR>(a, g, av, vk, vk1, pkm1, pkm2, pk, cf, r);
+                            simple_epilogue<TF, NR>(a, g, av, cv.vk, cv.vk1, cv.pkm1, cv.pk, cv.pk, cf, r);
                         }
                     }
                 }
