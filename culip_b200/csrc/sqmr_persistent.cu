@@ -166,12 +166,18 @@ __device__ void grid_reduce(double (&v)[NV], double* partials, int& red, double 
             buf[k * gridDim.x + blockIdx.x] = t;
         }
     grid.sync();
+    // the NV partials of a CTA position are loaded together (one round trip
+    // to L2 for all NV sums); each sum keeps its order over c
+    double t[NV];
+#pragma unroll
+    for (int k = 0; k < NV; ++k) t[k] = 0.0;
+    for (int c = threadIdx.x; c < (int)gridDim.x; c += kT)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) t[k] += __ldcg(buf + k * gridDim.x + c);
 #pragma unroll
     for (int k = 0; k < NV; ++k) {
-        double t = 0.0;
-        for (int c = threadIdx.x; c < (int)gridDim.x; c += kT) t += __ldcg(buf + k * gridDim.x + c);
-        for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(kFull, t, o);
-        if (lane == 0) sh[k][w] = t;
+        for (int o = 16; o > 0; o >>= 1) t[k] += __shfl_down_sync(kFull, t[k], o);
+        if (lane == 0) sh[k][w] = t[k];
     }
     __syncthreads();
     if (threadIdx.x == 0)
