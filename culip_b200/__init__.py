@@ -226,12 +226,23 @@ class Factor:
             capi.call("culipx_factor_compute_host", self._h, _p(v), None if ip is None else _p(ip), int(pivot),
                       float(threshold))
         else:
+            self._check_values(vals)
             capi.call("culipx_factor_compute", self._h, _dptr(vals), None if ip is None else _p(ip), int(pivot),
                       float(threshold))
+
+    def _check_values(self, vals):
+        """The C ABI takes raw pointers: refuse a values tensor whose type or
+        length differs from the pattern's, which the kernels would misread."""
+        if vals.dtype != self.dtype:
+            raise TypeError(f"values must be {self.dtype} for this pattern's precision, got {vals.dtype}")
+        nnz = int(self.pattern.rowptr[-1])
+        if vals.numel() < nnz:
+            raise ValueError(f"values hold {vals.numel()} entries, the pattern has {nnz}")
 
     def compute_graph(self, vals, pivot=PIV_BK, threshold=0.0):
         """compute() replayed from a CUDA graph captured on the first call
         for this tensor (vals: torch CUDA tensor, pattern precision)."""
+        self._check_values(vals)
         capi.call("culipx_factor_compute_graph", self._h, _dptr(vals), int(pivot), float(threshold))
 
     def set_solve_algorithm(self, algorithm, sweeps=0):

@@ -82,10 +82,13 @@ __device__ __forceinline__ void pivot_swap(T* Tt, int* perm, int p1, int p2, int
     __syncwarp();
 }
 
-// argmax of v over lanes, ties to the lowest index (value, index) = (v, i)
+// argmax of v over lanes, ties to the lowest index (value, index) = (v, i).
+// A NaN score counts as 0 (no candidate): with NaNs the comparisons are no
+// total order and the lanes' butterflies would end at different results.
 template <class T>
 __device__ __forceinline__ void warp_argmax(T& v, int& i)
 {
+    if (v != v) v = T(0);
     for (int o = 16; o > 0; o >>= 1) {
         const T ov = __shfl_xor_sync(0xffffffffu, v, o);
         const int oi = __shfl_xor_sync(0xffffffffu, i, o);
@@ -96,6 +99,7 @@ __device__ __forceinline__ void warp_argmax(T& v, int& i)
 template <class T>
 __device__ __forceinline__ T warp_max(T v)
 {
+    if (v != v) v = T(0);  // as in warp_argmax: every lane ends at the same value
     for (int o = 16; o > 0; o >>= 1) {
         const T ov = __shfl_xor_sync(0xffffffffu, v, o);
         v = (ov > v) ? ov : v;
@@ -231,6 +235,17 @@ __device__ __forceinline__ void factorize_tile(T* Tt, int len, int* is_piv, T* D
         if (p < len - 1 && method == CULIPX_PIV_BK) select_bk(Tt, p, len, order, p0, p1);
         else if (p < len - 1 && method == CULIPX_PIV_ROOK) select_rook(Tt, p, len, order, p0, p1);
         else order = (p < len - 1 && !is_piv[p + 1]) ? 2 : 1;
+        // lane 0 decides for the warp; for finite tiles every lane already
+        // agrees, and the clamp keeps the pivot rows inside the tile whatever
+        // the values (non-finite input yields a non-finite factor, no stray
+        // swap)
+        order = shfl(order, 0);
+        p0 = shfl(p0, 0);
+        p1 = shfl(p1, 0);
+        if (p0 < p || p0 >= len || (order == 2 && (p1 <= p || p1 >= len))) {
+            order = 1;
+            p0 = p;
+        }
         __syncwarp();
         if (order == 1) {
             if (use_piv && p != p0) pivot_swap(Tt, perm, p, p0, len);

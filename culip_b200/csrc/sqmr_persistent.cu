@@ -56,6 +56,7 @@
 #include <cooperative_groups.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdlib>
 
@@ -1295,6 +1296,33 @@ int persistent_grid(int dev, int* G)
     return CULIPX_OK;
 }
 
+// Grid sizes depend on the device (SM count, occupancy), so each launch
+// site keeps one entry per device of the current process.  Entries are
+// written at most once with the same value, so concurrent first calls from
+// several host threads at worst compute the size twice.
+constexpr int kMaxDevices = 64;
+
+struct DeviceGridCache {
+    std::atomic<int> g[kMaxDevices];
+};
+
+// *G = the cached grid for the current device, computed by size(dev, &g) once
+template <class SizeFn>
+int cached_grid(DeviceGridCache& c, SizeFn size, int* G, int* dev_out = nullptr)
+{
+    int dev = 0;
+    CULIPX_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) return fail(CULIPX_NOT_SUPPORTED, "device %d beyond %d devices", dev, kMaxDevices);
+    int g = c.g[dev].load(std::memory_order_acquire);
+    if (g == 0) {
+        CULIPX_TRY(size(dev, &g));
+        c.g[dev].store(g, std::memory_order_release);
+    }
+    *G = g;
+    if (dev_out) *dev_out = dev;
+    return CULIPX_OK;
+}
+
 // launch and wait; out_host receives 8 values per right-hand side
 template <class TF, int NR>
 int run_persistent(culipx_handle_t* h, PArgs<TF>& a, int G, double* out_host, bool wait = true)
@@ -1322,13 +1350,9 @@ int launch_persistent(culipx_handle_t* h, Csr* A, Factor* M, const double* b, do
         CULIPX_TRY(w->vecs.alloc(h, need));
         w->n = -1;  // the single-RHS workspace size is no longer known
     }
-    static int grid_cache[2][kMaxNR + 1] = {};
-    int& G = grid_cache[sizeof(TF) == 8 ? 0 : 1][NR];
-    if (G == 0) {
-        int dev = 0;
-        CULIPX_CUDA(cudaGetDevice(&dev));
-        CULIPX_TRY((persistent_grid<TF, NR>(dev, &G)));
-    }
+    static DeviceGridCache grid_cache;  // one per <TF, NR> instantiation
+    int G = 0;
+    CULIPX_TRY(cached_grid(grid_cache, persistent_grid<TF, NR>, &G));
     if ((size_t)(2 * kMaxNV * G) * sizeof(double) > w->partials.bytes())
         CULIPX_TRY(w->partials.alloc(h, (size_t)2 * kMaxNV * G * sizeof(double)));
     PArgs<TF> a = make_args<TF>(A, M, w->vecs.as<double>(), w->partials.as<double>(), b, x, tol, max_it, NR);
@@ -1458,16 +1482,19 @@ int launch_batched(Batch* bt, Csr* A, Factor* M, const double* b, double* x, dou
     cudaStream_t s = h->stream;
     const int n = A->m;
     CULIPX_TRY(sqmr_workspace(w, h, n));
-    static int grid_cache[2] = {0, 0};
-    int& G = grid_cache[sizeof(TF) == 8 ? 0 : 1];
-    if (G == 0) {
-        int dev = 0, per_sm = 0, sms = 0;
-        CULIPX_CUDA(cudaGetDevice(&dev));
-        CULIPX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        CULIPX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sqmr_batched<TF>, kT, 0));
-        if (per_sm < 1) return fail(CULIPX_NOT_SUPPORTED, "batched SQMR kernel does not fit on an SM");
-        G = sms * std::min(per_sm, kCtasPerSm);
-    }
+    static DeviceGridCache grid_cache;  // one per factor precision
+    int G = 0;
+    CULIPX_TRY(cached_grid(
+        grid_cache,
+        [](int dev, int* g) {
+            int per_sm = 0, sms = 0;
+            CULIPX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+            CULIPX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sqmr_batched<TF>, kT, 0));
+            if (per_sm < 1) return fail(CULIPX_NOT_SUPPORTED, "batched SQMR kernel does not fit on an SM");
+            *g = sms * std::min(per_sm, kCtasPerSm);
+            return (int)CULIPX_OK;
+        },
+        &G));
     PArgs<TF> a = make_args<TF>(A, M, w->vecs.as<double>(), w->partials.as<double>(), b, x, tol, max_it);
     BatchArgs ba;
     ba.num = bt->num;
@@ -1613,17 +1640,20 @@ int launch_many_prec(culipx_handle_t* h, const std::vector<int>& ks, const int* 
     CULIPX_CUDA(cudaMemcpyAsync(d_nr, nrs.data(), (size_t)num * sizeof(int), cudaMemcpyHostToDevice, s));
     CULIPX_CUDA(cudaMemsetAsync(d_next, 0, sizeof(int), s));
     const bool multi = std::any_of(nrs.begin(), nrs.end(), [](int r) { return r != 1; });
-    static int Gs[2] = {0, 0};
-    int& G = Gs[multi ? 1 : 0];
-    if (G == 0) {
-        int dev = 0, per_sm = 0, sms = 0;
-        CULIPX_CUDA(cudaGetDevice(&dev));
-        CULIPX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        CULIPX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            &per_sm, multi ? (const void*)k_sqmr_many<TF, true> : (const void*)k_sqmr_many<TF, false>, kT, 0));
-        if (per_sm < 1) return fail(CULIPX_NOT_SUPPORTED, "batched SQMR kernel does not fit on an SM");
-        G = sms * std::min(per_sm, kCtasPerSm);
-    }
+    static DeviceGridCache grid_caches[2];  // single / multi right-hand-side variant, per factor precision
+    auto many_grid = [](const void* kern) {
+        return [kern](int dev, int* g) {
+            int per_sm = 0, sms = 0;
+            CULIPX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+            CULIPX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kT, 0));
+            if (per_sm < 1) return fail(CULIPX_NOT_SUPPORTED, "batched SQMR kernel does not fit on an SM");
+            *g = sms * std::min(per_sm, kCtasPerSm);
+            return (int)CULIPX_OK;
+        };
+    };
+    int G = 0;
+    if (multi) CULIPX_TRY(cached_grid(grid_caches[1], many_grid((const void*)k_sqmr_many<TF, true>), &G));
+    else CULIPX_TRY(cached_grid(grid_caches[0], many_grid((const void*)k_sqmr_many<TF, false>), &G));
     if (multi) k_sqmr_many<TF, true><<<std::min(G, num), kT, 0, s>>>(d_args, d_nr, num, d_next);
     else k_sqmr_many<TF, false><<<std::min(G, num), kT, 0, s>>>(d_args, d_nr, num, d_next);
     h->launches += 1;
@@ -1759,13 +1789,11 @@ constexpr size_t kNoAllocSlots = kNoAllocVecs + (size_t)2 * kMaxNV * kNoAllocMax
 
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocSlots];
 
-double* g_noalloc_ptr[64] = {nullptr};  // per-device address of g_noalloc_scratch
-int g_noalloc_grid[64][2] = {{0, 0}};   // per-device grid size per factor precision
+std::atomic<double*> g_noalloc_ptr[kMaxDevices];  // per-device address of g_noalloc_scratch
 
 int noalloc_setup(int dev)
 {
-    if (dev < 0 || dev >= 64) return fail(CULIPX_INVALID_ARG, "culipx_sqmr_solve_noalloc: device %d out of range", dev);
-    if (g_noalloc_ptr[dev]) return CULIPX_OK;
+    if (g_noalloc_ptr[dev].load(std::memory_order_acquire)) return CULIPX_OK;
     void* ptr = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
     if (e != cudaSuccess || !ptr) {
@@ -1773,41 +1801,31 @@ int noalloc_setup(int dev)
         return fail(CULIPX_CUDA_ERROR, "culipx_sqmr_solve_noalloc: cudaGetSymbolAddress failed: %s",
                     cudaGetErrorString(e));
     }
-    g_noalloc_ptr[dev] = static_cast<double*>(ptr);
+    g_noalloc_ptr[dev].store(static_cast<double*>(ptr), std::memory_order_release);
     return CULIPX_OK;
 }
 
 template <class TF>
 int noalloc_grid(int dev, int* G)
 {
-    int& g = g_noalloc_grid[dev][sizeof(TF) == 8 ? 0 : 1];
-    if (g == 0) {
-        CULIPX_TRY((persistent_grid<TF, 1>(dev, &g)));
-        g = std::min(g, kNoAllocMaxGrid);
-    }
-    *G = g;
+    CULIPX_TRY((persistent_grid<TF, 1>(dev, G)));
+    *G = std::min(*G, kNoAllocMaxGrid);
     return CULIPX_OK;
 }
 
+// out[0..3] = residual estimate, iterations, breakdown flag, converged flag
 template <class TF>
 int launch_noalloc(culipx_handle_t* h, Csr* A, Factor* M, const double* b, double* x, double tol, int max_it,
-                   double* residual, int* iterations, bool* converged, bool* breakdown)
+                   double (&out)[8])
 {
-    int dev = 0;
-    CULIPX_CUDA(cudaGetDevice(&dev));
+    static DeviceGridCache grid_cache;  // one per factor precision
+    int G = 0, dev = 0;
+    CULIPX_TRY(cached_grid(grid_cache, noalloc_grid<TF>, &G, &dev));
     CULIPX_TRY(noalloc_setup(dev));
-    int G = 0;
-    CULIPX_TRY(noalloc_grid<TF>(dev, &G));
-    double* base = g_noalloc_ptr[dev];
+    double* base = g_noalloc_ptr[dev].load(std::memory_order_acquire);
     // run_persistent clears the recurrence vectors the scratch kept from the last call
     PArgs<TF> a = make_args<TF>(A, M, base, base + kNoAllocVecs, b, x, tol, max_it);
-    double out[8];
-    CULIPX_TRY((run_persistent<TF, 1>(h, a, G, out)));
-    if (residual) *residual = out[0];
-    if (iterations) *iterations = (int)out[1];
-    *breakdown = out[2] != 0.0;
-    *converged = out[3] != 0.0;
-    return CULIPX_OK;
+    return run_persistent<TF, 1>(h, a, G, out);
 }
 
 }  // namespace
@@ -1827,16 +1845,14 @@ int sqmr_solve_noalloc(culipx_handle_t* h, Csr* A, Factor* M, const double* b, d
                     "culipx_sqmr_solve_noalloc: n = %d exceeds the fixed scratch of %d rows; use culipx_sqmr_solve",
                     A->m, kNoAllocMaxRows);
     if (max_it < 0) return fail(CULIPX_INVALID_ARG, "culipx_sqmr_solve_noalloc: max_it < 0");
-    bool conv = false, bd = false;
-    int st;
-    if (M->precision == CULIPX_F64)
-        st = launch_noalloc<double>(h, A, M, b, x, tol, max_it, residual, iterations, &conv, &bd);
-    else
-        st = launch_noalloc<float>(h, A, M, b, x, tol, max_it, residual, iterations, &conv, &bd);
+    double out[8] = {};
+    const int st = M->precision == CULIPX_F64 ? launch_noalloc<double>(h, A, M, b, x, tol, max_it, out)
+                                              : launch_noalloc<float>(h, A, M, b, x, tol, max_it, out);
     if (st != CULIPX_OK) return st;
-    if (bd) return fail(CULIPX_BREAKDOWN, "culipx_sqmr_solve_noalloc: breakdown (non-finite scalar)");
-    if (!conv && max_it > 0 && iterations && *iterations >= max_it) return CULIPX_MAXIT;
-    return CULIPX_OK;
+    if (residual) *residual = out[0];
+    if (iterations) *iterations = (int)out[1];
+    if (out[2] != 0.0) return fail(CULIPX_BREAKDOWN, "culipx_sqmr_solve_noalloc: breakdown (non-finite scalar)");
+    return status_of(out, max_it);
 }
 
 }  // namespace culipx

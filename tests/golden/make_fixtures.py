@@ -7,7 +7,7 @@ exists only where the fixtures are generated; the .npz files are committed).
 MatrixMarket semantics follow libs/test/test.impl.h: 1-based coordinates,
 symmetric files expanded to both triangles (:73-89), rows sorted; dense
 "array" vectors read as written (shift 0, :233-290).
-Run:  python tests/golden/make_fixtures.py [/path/to/culip]
+Run:  python tests/golden/make_fixtures.py /path/to/culip
 """
 from __future__ import annotations
 
@@ -68,4 +68,6 @@ def main(root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_fixtures.py <path to the culip checkout>")
+    main(sys.argv[1])
