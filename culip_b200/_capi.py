@@ -79,6 +79,11 @@ _SIGS = {
     "culipx_spmv": [vp, vp, vp, f64, f64, i32],
     "culipx_sqmr_solve": [vp, vp, vp, vp, vp, f64, i32, ctypes.POINTER(f64), ctypes.POINTER(i32)],
     "culipx_sqmr_solve_noalloc": [vp, vp, vp, vp, vp, f64, i32, ctypes.POINTER(f64), ctypes.POINTER(i32)],
+    "culipx_vec_dot": [vp, i32, i64, vp, vp, ctypes.POINTER(f64)],
+    "culipx_vec_nrm2": [vp, i32, i64, vp, ctypes.POINTER(f64)],
+    "culipx_vec_axpy": [vp, i32, i64, f64, vp, vp],
+    "culipx_vec_scal": [vp, i32, i64, f64, vp],
+    "culipx_vec_convert": [vp, i64, i32, vp, i32, vp],
     "culipx_batch_create": [vp, i32, vp, ctypes.POINTER(vp)],
     "culipx_batch_destroy": [vp],
     "culipx_batch_sqmr_solve": [vp, vp, vp, vp, vp, f64, i32, vp, vp, vp],

@@ -24,7 +24,47 @@ using namespace culipx;
     catch (const std::bad_alloc&) { return fail(CULIPX_OOM, "host allocation failed"); }     \
     catch (...) { return fail(CULIPX_CUDA_ERROR, "unexpected exception"); }
 
+namespace culipx {
+
+void handle_retain(culipx_handle_t* h)
+{
+    if (h) h->refs.fetch_add(1, std::memory_order_relaxed);
+}
+
+void handle_release(culipx_handle_t* h)
+{
+    if (!h || h->refs.fetch_sub(1, std::memory_order_acq_rel) != 1) return;
+    if (h->device >= 0 && cudaSetDevice(h->device) != cudaSuccess) cudaGetLastError();
+    delete h->sqmr;
+    if (h->vec_scratch) cudaFree(h->vec_scratch);
+    if (h->ev_start) cudaEventDestroy(h->ev_start);
+    if (h->ev_stop) cudaEventDestroy(h->ev_stop);
+    delete h;
+}
+
+}  // namespace culipx
+
 namespace {
+
+// references on a pattern (Pattern::refs); the last release frees it and
+// drops its reference on the handle
+void pattern_retain(Pattern* p) { p->refs.fetch_add(1, std::memory_order_relaxed); }
+
+void pattern_release(Pattern* p)
+{
+    if (!p || p->refs.fetch_sub(1, std::memory_order_acq_rel) != 1) return;
+    culipx_handle_t* h = p->handle;
+    if (h && h->device >= 0 && cudaSetDevice(h->device) != cudaSuccess) cudaGetLastError();
+    delete static_cast<culipx_pattern_t*>(p);
+    handle_release(h);
+}
+
+// makes the object's device current before it frees device memory
+void set_device_of(const culipx_handle_t* h)
+{
+    if (h && h->device >= 0 && cudaSetDevice(h->device) != cudaSuccess) cudaGetLastError();
+}
+
 int use_device(culipx_handle_t* h)
 {
     if (h->device < 0) return CULIPX_OK;  // host-only handle
@@ -73,12 +113,8 @@ CULIPX_API int culipx_handle_create(culipx_handle* out, int device, void* cuda_s
 
 CULIPX_API int culipx_handle_destroy(culipx_handle h)
 {
-    if (!h) return CULIPX_OK;
-    if (h->device >= 0) cudaSetDevice(h->device);
-    delete h->sqmr;
-    if (h->ev_start) cudaEventDestroy(h->ev_start);
-    if (h->ev_stop) cudaEventDestroy(h->ev_stop);
-    delete h;
+    // objects created on the handle keep it alive until they are destroyed
+    handle_release(h);
     return CULIPX_OK;
 }
 
@@ -129,6 +165,7 @@ CULIPX_API int culipx_pattern_analyze(culipx_handle h, int n, const int* h_rowpt
     Pattern* p = nullptr;
     CULIPX_TRY(analyze_pattern(h, n, h_rowptr, h_colidx, num_blocks, h_block_starts, fill_level, fill_factor,
                                precision, &p));
+    handle_retain(h);
     *out = static_cast<culipx_pattern>(p);
     return CULIPX_OK;
     GUARD_END
@@ -146,6 +183,7 @@ CULIPX_API int culipx_pattern_analyze_systems(culipx_handle h, int n, const int*
     Pattern* p = nullptr;
     CULIPX_TRY(analyze_pattern(h, n, h_rowptr, h_colidx, num_blocks, h_block_starts, fill_level, fill_factor,
                                precision, &p, num_systems, h_row_offsets));
+    handle_retain(h);
     *out = static_cast<culipx_pattern>(p);
     return CULIPX_OK;
     GUARD_END
@@ -153,10 +191,8 @@ CULIPX_API int culipx_pattern_analyze_systems(culipx_handle h, int n, const int*
 
 CULIPX_API int culipx_pattern_destroy(culipx_pattern p)
 {
-    if (p) {
-        if (p->handle->device >= 0) cudaSetDevice(p->handle->device);
-        delete p;
-    }
+    // factors and batches made from the pattern keep it alive until they are destroyed
+    pattern_release(p);
     return CULIPX_OK;
 }
 
@@ -201,6 +237,7 @@ CULIPX_API int culipx_factor_create(culipx_pattern p, culipx_factor* out)
     CULIPX_TRY(use_device(p->handle));
     Factor* f = nullptr;
     CULIPX_TRY(factor_create(p, &f));
+    pattern_retain(p);
     *out = static_cast<culipx_factor>(f);
     return CULIPX_OK;
     GUARD_END
@@ -209,8 +246,10 @@ CULIPX_API int culipx_factor_create(culipx_pattern p, culipx_factor* out)
 CULIPX_API int culipx_factor_destroy(culipx_factor f)
 {
     if (f) {
-        cudaSetDevice(f->pat->handle->device);
+        Pattern* p = f->pat;
+        set_device_of(p->handle);
         delete f;
+        pattern_release(p);
     }
     return CULIPX_OK;
 }
@@ -371,6 +410,7 @@ CULIPX_API int culipx_csr_create(culipx_handle h, int m, int n, long long nnz, c
         const int st = csr_build_transpose(A);
         if (st) { delete A; return st; }
     }
+    handle_retain(h);
     *out = A;
     return CULIPX_OK;
     GUARD_END
@@ -385,6 +425,7 @@ CULIPX_API int culipx_permute_create(culipx_handle h, int n, long long nnz, cons
     CULIPX_TRY(use_device(h));
     PermutePlan* p = nullptr;
     CULIPX_TRY(permute_plan_create(h, n, nnz, d_rowptr, d_colidx, h_row_perm, h_col_perm, perm_is_old_to_new, &p));
+    handle_retain(h);
     *out = static_cast<culipx_permute>(p);
     return CULIPX_OK;
     GUARD_END
@@ -393,8 +434,10 @@ CULIPX_API int culipx_permute_create(culipx_handle h, int n, long long nnz, cons
 CULIPX_API int culipx_permute_destroy(culipx_permute p)
 {
     if (p) {
-        if (p->handle->device >= 0) cudaSetDevice(p->handle->device);
+        culipx_handle_t* h = p->handle;
+        set_device_of(h);
         delete p;
+        handle_release(h);
     }
     return CULIPX_OK;
 }
@@ -433,7 +476,12 @@ CULIPX_API int culipx_permute_apply(culipx_permute p, int precision, const void*
 
 CULIPX_API int culipx_csr_destroy(culipx_csr A)
 {
-    delete A;
+    if (A) {
+        culipx_handle_t* h = A->h;
+        set_device_of(h);
+        delete A;
+        handle_release(h);
+    }
     return CULIPX_OK;
 }
 
@@ -498,6 +546,8 @@ CULIPX_API int culipx_batch_create(culipx_pattern p, int num_systems, const int*
     CULIPX_TRY(use_device(p->handle));
     Batch* b = nullptr;
     CULIPX_TRY(batch_create(p->handle, p, num_systems, h_row_offsets, &b));
+    pattern_retain(p);
+    b->pat_ref = p;
     *out = static_cast<culipx_batch>(b);
     return CULIPX_OK;
     GUARD_END
@@ -506,8 +556,10 @@ CULIPX_API int culipx_batch_create(culipx_pattern p, int num_systems, const int*
 CULIPX_API int culipx_batch_destroy(culipx_batch b)
 {
     if (b) {
-        cudaSetDevice(b->h->device);
+        Pattern* p = b->pat_ref;
+        set_device_of(b->h);
         delete b;
+        pattern_release(p);
     }
     return CULIPX_OK;
 }
@@ -638,6 +690,7 @@ CULIPX_API int culipx_ldu_create(culipx_handle h, int n, const int* d_rowptr, co
     CULIPX_TRY(use_device(h));
     Ldu* P = nullptr;
     CULIPX_TRY(ldu_create(h, n, d_rowptr, d_colidx, d_val, d_tri, d_is_piv, d_perm, d_scale, &P));
+    handle_retain(h);
     *out = static_cast<culipx_ldu>(P);
     return CULIPX_OK;
     GUARD_END
@@ -665,8 +718,10 @@ CULIPX_API int culipx_sqmr_solve_ldu(culipx_handle h, culipx_csr A, culipx_ldu P
 CULIPX_API int culipx_ldu_destroy(culipx_ldu P)
 {
     if (P) {
-        if (P->h->device >= 0) cudaSetDevice(P->h->device);
+        culipx_handle_t* h = P->h;
+        set_device_of(h);
         delete P;
+        handle_release(h);
     }
     return CULIPX_OK;
 }
@@ -681,6 +736,7 @@ CULIPX_API int culipx_kkt_operator_create(culipx_handle h, int kind, int m, int 
     CULIPX_TRY(use_device(h));
     KktOperator* op = nullptr;
     CULIPX_TRY(kkt_operator_create(h, kind, m, n, nnz, d_rowptr, d_colidx, d_val, d_d, delta, num_ix, d_ix, &op));
+    handle_retain(h);
     *out = static_cast<culipx_kkt_operator>(op);
     return CULIPX_OK;
     GUARD_END
@@ -699,8 +755,10 @@ CULIPX_API int culipx_kkt_operator_multiply(culipx_kkt_operator op, const double
 CULIPX_API int culipx_kkt_operator_destroy(culipx_kkt_operator op)
 {
     if (op) {
-        if (op->h->device >= 0) cudaSetDevice(op->h->device);
+        culipx_handle_t* h = op->h;
+        set_device_of(h);
         delete op;
+        handle_release(h);
     }
     return CULIPX_OK;
 }

@@ -22,6 +22,11 @@ struct culipx_handle_t {
     std::atomic<long long> used{0};     // bytes held by this handle's buffers
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
     long long launches = 0;             // kernels launched through this handle
+    double* vec_scratch = nullptr;      // reduction partials of the vector operations (vecops.cu)
+    // the creator's reference plus one per object the C ABI created on this
+    // handle (patterns, operators, plans, ...): culipx_handle_destroy and
+    // those objects' destroy calls may come in any order, the last one frees
+    std::atomic<int> refs{1};
 };
 
 namespace culipx {
@@ -39,6 +44,10 @@ namespace culipx {
         int s_ = (expr);            \
         if (s_ != CULIPX_OK) return s_; \
     } while (0)
+
+// References on a handle (see culipx_handle_t::refs); the last release frees it.
+void handle_retain(culipx_handle_t* h);
+void handle_release(culipx_handle_t* h);
 
 // Checks the last launch error on this thread.
 int launch_check(const char* what);

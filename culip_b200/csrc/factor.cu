@@ -432,7 +432,7 @@ __device__ void offdiag_tile(const FactorArgs& a, const T* val, const T* tri, in
     const T gc = d11 / gr, gs = d12 / gr;
     const T td11 = fma_rn(gc, d11, gs * d12);
     const T td12 = fma_rn(gc, d12, gs * d22);
-    const T td22 = fma_rn(-gs, d12, gc * d22);
+    const T td22 = fma_rn(gc, d22, -(gs * d12));
     while (colmask) {
         const int j = __ffs(colmask) - 1;
         colmask &= colmask - 1;
@@ -446,7 +446,7 @@ __device__ void offdiag_tile(const FactorArgs& a, const T* val, const T* tri, in
         if (lane >= h) rhs = T(0);
         const T right = shfl(rhs, (lane < 31) ? lane + 1 : 31);
         T x1 = fma_rn(gc, rhs, gs * right);
-        T x2 = fma_rn(-gs, rhs, gc * right);
+        T x2 = fma_rn(gc, right, -(gs * rhs));
         x2 = piv2 ? (x2 / td22) : T(0);
         x1 = fma_rn(-td12, x2, x1) / td11;
         __syncwarp();
@@ -645,11 +645,16 @@ __global__ void k_row_norms(FactorArgs a, T* row_norm, const T* norm_part, int l
     row_norm[from + lane] = acc;
 }
 
-// Serialized dual-dropping bookkeeping of one level in block order
-// (:1949-2008): grants from the leftover pool, capacity updates and arena
-// relocation of the blocks granted extra slots.  One CTA; the leftover
-// recurrence x -> max(x + a, b) composes, so per-thread chunks are composed,
-// scanned, then replayed.
+// Dual-dropping bookkeeping of one level (:1949-2008): grants from the
+// leftover pool, capacity updates and arena relocation of the blocks granted
+// extra slots.  In the reference every block of a level is a CTA that takes
+// from one atomic counter before it returns its own spare slots, so a level's
+// requests are served from the pool the earlier levels left, and the level's
+// spare slots join the pool for the levels after it; which of a level's
+// requests wins a contended slot is a race there.  Here the requests are
+// served in level-list order.  One CTA; a request is x -> max(x - req, 0),
+// which composes as x -> max(x + a, b): per-thread chunks are composed,
+// scanned, then replayed; the spare slots are summed on the side.
 constexpr long long kNeg = LLONG_MIN / 4;
 constexpr int kScanT = 1024;
 
@@ -663,19 +668,30 @@ __global__ void __launch_bounds__(kScanT) k_level_scan(FactorArgs a, int lb_firs
     }
     const int chunk = (noff + kScanT - 1) / kScanT;
     const int t0 = min(noff, tid * chunk), t1 = min(noff, t0 + chunk);
-    long long A = 0, B = kNeg;
+    long long A = 0, B = kNeg, spare = 0;
     for (int t = t0; t < t1; ++t) {
         const int b = a.lb[lb_first + t];
         if (a.fmt[b] != 0) continue;
         const long long c = a.nnz[b], m = a.cap[b];
-        const long long ea = (c > m) ? -(c - m) : (m - c);
-        const long long eb = (c > m) ? 0 : kNeg;
-        A = A + ea;
-        B = max(B + ea, eb);
-        B = max(B, kNeg);
+        if (c > m) {  // a request of c - m slots: x -> max(x - (c - m), 0)
+            A = A - (c - m);
+            B = max(max(B - (c - m), 0LL), kNeg);
+        } else {
+            spare += m - c;
+        }
     }
     fa[tid] = A;
     fb[tid] = B;
+    rel[tid] = spare;
+    __syncthreads();
+    if (tid == 0) {
+        // the level's spare slots, for the pool after the level
+        long long s = 0;
+        for (int k = 0; k < kScanT; ++k) s += rel[k];
+        rel[0] = s;
+    }
+    __syncthreads();
+    const long long level_spare = rel[0];
     __syncthreads();
     if (tid == 0) {
         // exclusive scan of the compositions: prefix_t = f_{t-1} o ... o f_0
@@ -706,13 +722,11 @@ __global__ void __launch_bounds__(kScanT) k_level_scan(FactorArgs a, int lb_firs
             a.got_extra[b] = (int)g;
             a.cap[b] = (int)(m + g);
             if (g > 0) my_rel += m + g;
-        } else {
-            x += m - c;
         }
     }
     rel[tid] = my_rel;
     __syncthreads();
-    if (tid == kScanT - 1) a.state[kStLeftover] = x;  // the last chunk ends the level
+    if (tid == kScanT - 1) a.state[kStLeftover] = x + level_spare;  // the last chunk ends the level
     if (tid == 0) {
         long long s = 0;
         for (int k = 0; k < kScanT; ++k) {

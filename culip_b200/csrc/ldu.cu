@@ -78,8 +78,8 @@ __global__ void k_ldu_d(int n, const double* __restrict__ tri, const int* __rest
     const double r1 = b[g], r2 = (g < n - 1) ? b[g + 1] : 0.0;
     const double gr = sqrt(fma_rn(p11, p11, p12 * p12));
     const double gc = p11 / gr, gs = p12 / gr;
-    double g1 = fma_rn(gc, r1, gs * r2), g2 = fma_rn(-gs, r1, gc * r2);
-    const double tp12 = fma_rn(gc, p12, gs * p22), tp22 = fma_rn(-gs, p12, gc * p22);
+    double g1 = fma_rn(gc, r1, gs * r2), g2 = fma_rn(gc, r2, -(gs * r1));
+    const double tp12 = fma_rn(gc, p12, gs * p22), tp22 = fma_rn(gc, p22, -(gs * p12));
     g2 = g2 / tp22;
     g1 = fma_rn(-tp12, g2, g1) / gr;
     if (this_piv) x[g] = g1;

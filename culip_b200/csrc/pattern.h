@@ -21,6 +21,9 @@ struct BlockDesc {
 
 struct Pattern {
     culipx_handle_t* handle = nullptr;
+    // the creator's reference plus one per factor / batch made from it through
+    // the C ABI; the last release frees the pattern (and releases the handle)
+    std::atomic<int> refs{1};
     int n = 0;
     long long nnz = 0;
     int precision = CULIPX_F64;

@@ -197,10 +197,10 @@ __device__ __forceinline__ void step_2x2(T* Tt, T* D, int row, int len)
     const T gr = sqrt(fma_rn(d11, d11, d12 * d12));
     const T gc = d11 / gr, gs = d12 / gr;
     T x1 = fma_rn(gc, a1, gs * a2);
-    T x2 = fma_rn(-gs, a1, gc * a2);
+    T x2 = fma_rn(gc, a2, -(gs * a1));
     const T td11 = fma_rn(gc, d11, gs * d12);
     const T td12 = fma_rn(gc, d12, gs * d22);
-    const T td22 = fma_rn(-gs, d12, gc * d22);
+    const T td22 = fma_rn(gc, d22, -(gs * d12));
     x2 = x2 / td22;
     x1 = fma_rn(-td12, x2, x1) / td11;
     __syncwarp();

@@ -598,9 +598,9 @@ __global__ void k_solve_D(const T* __restrict__ tri, const int* __restrict__ is_
         const T gr = sqrt(fma_rn(p11, p11, p12 * p12));
         const T gc = p11 / gr, gs = p12 / gr;
         T g1 = fma_rn(gc, r1, gs * r2);
-        T g2 = fma_rn(-gs, r1, gc * r2);
+        T g2 = fma_rn(gc, r2, -(gs * r1));
         const T tp12 = fma_rn(gc, p12, gs * p22);
-        const T tp22 = fma_rn(-gs, p12, gc * p22);
+        const T tp22 = fma_rn(gc, p22, -(gs * p12));
         g2 = g2 / tp22;
         g1 = fma_rn(-tp12, g2, g1) / gr;
         if (this_piv) out[g] = g1;

@@ -115,9 +115,9 @@ __device__ __forceinline__ void dsolve_pair(const double* tri, const int* is_piv
     const double gr = sqrt(fma_rn(p11, p11, p12 * p12));
     const double gc = p11 / gr, gs = p12 / gr;
     g1 = fma_rn(gc, r1, gs * r2);
-    g2 = fma_rn(-gs, r1, gc * r2);
+    g2 = fma_rn(gc, r2, -(gs * r1));
     const double tp12 = fma_rn(gc, p12, gs * p22);
-    const double tp22 = fma_rn(-gs, p12, gc * p22);
+    const double tp22 = fma_rn(gc, p22, -(gs * p12));
     g2 = g2 / tp22;
     g1 = fma_rn(-tp12, g2, g1) / gr;
 }

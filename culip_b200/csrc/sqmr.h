@@ -32,6 +32,7 @@ struct Pattern;
 struct Batch {
     culipx_handle_t* h = nullptr;
     const Pattern* pat = nullptr;
+    Pattern* pat_ref = nullptr;               // the C ABI's reference on pat (released with the batch)
     int num = 0, nl = 0;
     std::vector<int> row_off;                 // num + 1
     DeviceBuffer d_row_off, d_qb, d_qe;       // num + 1, num x nl, num x nl

@@ -223,7 +223,7 @@ struct DBlock {
         gc = p11 / gr;
         gs = p12 / gr;
         tp12 = fma_rn(gc, p12, gs * p22);
-        tp22 = fma_rn(-gs, p12, gc * p22);
+        tp22 = fma_rn(gc, p22, -(gs * p12));
     }
 
     __device__ __forceinline__ double apply(double y, int h) const
@@ -235,7 +235,7 @@ struct DBlock {
         if (lane < h) {
             const double r2 = (lane + 1 < h) ? ynext : 0.0;
             g1 = fma_rn(gc, y, gs * r2);
-            g2 = fma_rn(-gs, y, gc * r2);
+            g2 = fma_rn(gc, r2, -(gs * y));
             g2 = g2 / tp22;
             g1 = fma_rn(-tp12, g2, g1) / gr;
         }

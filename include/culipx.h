@@ -243,6 +243,21 @@ int culipx_csr_destroy(culipx_csr A);
 int culipx_spmv(culipx_csr A, const void *d_x, void *d_y, double alpha, double beta, int transpose);
 
 /* ------------------------------------------------------------------------ */
+/* Vector operations on device vectors of n values in `precision`, on the
+ * handle's stream: the BLAS-1 helpers T_doti / T_nrm2 / T_axpy / T_scal of
+ * libs/la/dense_la.cuh:35-85 (cuBLAS calls there).  Reductions sum in FP64 in
+ * a fixed order (deterministic) and return their result to host memory,
+ * synchronizing the stream.  culipx_vec_convert copies between FP64 and FP32
+ * (no counterpart; the class facade uses it for SQMR<float>). */
+int culipx_vec_dot(culipx_handle h, int precision, long long n, const void *d_x, const void *d_y,
+                   double *h_result);
+int culipx_vec_nrm2(culipx_handle h, int precision, long long n, const void *d_x, double *h_result);
+int culipx_vec_axpy(culipx_handle h, int precision, long long n, double alpha, const void *d_x, void *d_y);
+int culipx_vec_scal(culipx_handle h, int precision, long long n, double alpha, void *d_x);
+int culipx_vec_convert(culipx_handle h, long long n, int src_precision, const void *d_src, int dst_precision,
+                       void *d_dst);
+
+/* ------------------------------------------------------------------------ */
 /* SQMR with the factor as split preconditioner M = (P U') D (U P')
  * (SQMR<double>::solve, sqmr.impl.cuh:109-355).  A must be FP64; M may be
  * FP64, FP32 (mixed precision: applies in FP32, recurrence in FP64) or NULL.

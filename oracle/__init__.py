@@ -49,6 +49,9 @@ def lib():
             f = getattr(L, "orc_factor" + sfx)
             f.restype = vp
             f.argtypes = [vp, vp, vp, ctypes.c_int, real, ctypes.c_int]
+            ff = getattr(L, "orc_factor_forced" + sfx)
+            ff.restype = vp
+            ff.argtypes = [vp, vp, vp, ctypes.c_int, real, ctypes.c_int, vp]
             getattr(L, "orc_fac_free" + sfx).argtypes = [vp]
             g = getattr(L, "orc_fac_export_size" + sfx)
             g.restype = ctypes.c_long
@@ -130,21 +133,30 @@ class Sym:
             _lib.orc_sym_free(ctypes.cast(h, ctypes.c_void_p))
             self._h = None
 
-    def factor(self, vals, is_piv=None, pivot=1, threshold=0.0, literal=False) -> "Fac":
-        return Fac(self, vals, is_piv, pivot, threshold, literal)
+    def factor(self, vals, is_piv=None, pivot=1, threshold=0.0, literal=False, forced_grants=None) -> "Fac":
+        """forced_grants: per block (block-id order) the extra slots a block
+        that outgrows its capacity receives, as another run decided them."""
+        return Fac(self, vals, is_piv, pivot, threshold, literal, forced_grants)
 
 
 class Fac:
     """Numeric factor (BlockiLDLt::factorize) and its applies."""
 
-    def __init__(self, sym: Sym, vals, is_piv, pivot, threshold, literal):
+    def __init__(self, sym: Sym, vals, is_piv, pivot, threshold, literal, forced_grants=None):
         self.sym = sym
         self.sfx = "_d" if sym.dtype == np.float64 else "_s"
         self.vals = np.ascontiguousarray(vals, dtype=sym.dtype)
         ip = np.ones(sym.n, np.int32) if is_piv is None else np.ascontiguousarray(is_piv, dtype=np.int32)
-        f = getattr(lib(), "orc_factor" + self.sfx)
-        self._h = f(ctypes.cast(sym._h, ctypes.c_void_p), _p(self.vals), _p(ip), int(pivot), float(threshold),
-                    1 if literal else 0)
+        if forced_grants is None:
+            f = getattr(lib(), "orc_factor" + self.sfx)
+            self._h = f(ctypes.cast(sym._h, ctypes.c_void_p), _p(self.vals), _p(ip), int(pivot), float(threshold),
+                        1 if literal else 0)
+        else:
+            self._forced = np.ascontiguousarray(forced_grants, dtype=np.int32)
+            assert len(self._forced) == sym.coarse_nnz
+            f = getattr(lib(), "orc_factor_forced" + self.sfx)
+            self._h = f(ctypes.cast(sym._h, ctypes.c_void_p), _p(self.vals), _p(ip), int(pivot), float(threshold),
+                        1 if literal else 0, _p(self._forced))
 
     def __del__(self):
         h = getattr(self, "_h", None)

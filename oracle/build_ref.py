@@ -21,8 +21,15 @@ With the reference's flags (build_parameters_device.cmake: -O3 -lineinfo
 prototypes, a Matrix Market reader, helper_cuda.h).
 
 Outputs:
-  oracle/_ref/ref_dump            the dump driver (oracle/ref_dump.cu)
-  oracle/_ref/culip-block-ildlt   apps/block_ildlt as the reference ships it
+  oracle/_ref/ref_dump               the dump driver (oracle/ref_dump.cu)
+  oracle/_ref/culip-block-ildlt      apps/block_ildlt as the reference ships it
+  oracle/_ref/culip-block-ildlt-b200 the same unmodified driver source compiled
+                                     against culip_b200's class facade
+                                     (include/culip_la.hpp through
+                                     include/culip_compat/) and linked to
+                                     culip_b200/lib/libculipx.so: the drop-in
+                                     check; nothing of the reference's libs/
+                                     is on its include path
 """
 from __future__ import annotations
 
@@ -119,7 +126,39 @@ def build(culip: str, jobs: int | None = None) -> dict:
             if r.returncode != 0:
                 raise RuntimeError(f"reference build: linking {name} failed:\n{r.stdout}\n{r.stderr[-4000:]}")
         outs[name] = exe
+    outs["culip-block-ildlt-b200"] = build_facade_driver(culip)
     return outs
+
+
+def build_facade_driver(culip: str) -> str:
+    """apps/block_ildlt/block_ildlt.cc against the culip_b200 facade.  Its
+    include root holds only a link to the checkout's apps/ folder, so every
+    <libs/...> header it includes comes from include/culip_compat."""
+    import tempfile
+
+    repo = os.path.dirname(HERE)
+    lib_dir = os.path.join(repo, "culip_b200", "lib")
+    if not os.path.exists(os.path.join(lib_dir, "libculipx.so")):
+        raise FileNotFoundError("build libculipx.so first (culip_b200/build.py)")
+    exe = os.path.join(OUT, "culip-block-ildlt-b200")
+    src = os.path.join(culip, DRIVER)
+    deps = [src, os.path.join(culip, "apps/block_ildlt/block_ildlt_invariants.h"),
+            os.path.join(repo, "include", "culip_la.hpp"), os.path.join(repo, "include", "culipx.h"),
+            os.path.join(lib_dir, "libculipx.so")]
+    if os.path.exists(exe) and os.path.getmtime(exe) >= max(os.path.getmtime(d) for d in deps):
+        return exe
+    cuda = os.path.dirname(os.path.dirname(_nvcc()))
+    os.makedirs(OUT, exist_ok=True)
+    with tempfile.TemporaryDirectory() as root:
+        os.symlink(os.path.join(culip, "apps"), os.path.join(root, "apps"))
+        cmd = ["g++", "-std=c++17", "-O2", "-w", "-I", os.path.join(repo, "include", "culip_compat"),
+               "-I", os.path.join(repo, "include"), "-I", root, "-I", os.path.join(cuda, "include"), src,
+               "-o", exe, "-L", lib_dir, "-lculipx", "-Wl,-rpath,$ORIGIN/../../culip_b200/lib",
+               "-L", os.path.join(cuda, "lib64"), "-lcudart"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"facade driver build failed:\n{r.stdout}\n{r.stderr[-6000:]}")
+    return exe
 
 
 def main() -> int:

@@ -81,8 +81,8 @@ static void ldu_apply(const prec_t *P, int stage, const double *b, double *x)
             const double r1 = b[g], r2 = (g < n - 1) ? b[g + 1] : 0.0;
             const double gr = sqrt(fma(p11, p11, p12 * p12));
             const double gc = p11 / gr, gs = p12 / gr;
-            double g1 = fma(gc, r1, gs * r2), g2 = fma(-gs, r1, gc * r2);
-            const double tp12 = fma(gc, p12, gs * p22), tp22 = fma(-gs, p12, gc * p22);
+            double g1 = fma(gc, r1, gs * r2), g2 = fma(gc, r2, -(gs * r1));
+            const double tp12 = fma(gc, p12, gs * p22), tp22 = fma(gc, p22, -(gs * p12));
             g2 = g2 / tp22;
             g1 = fma(-tp12, g2, g1) / gr;
             if (this_piv) x[g] = g1;

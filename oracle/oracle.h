@@ -46,6 +46,11 @@ orc_fac_d *orc_factor_d(const orc_sym *s, const double *vals, const int *is_piv_
                         int pivot, double threshold, int literal);
 orc_fac_s *orc_factor_s(const orc_sym *s, const float *vals, const int *is_piv_init,
                         int pivot, float threshold, int literal);
+/* the same with each outgrowing block's extra slots given (coarse_nnz ints) */
+orc_fac_d *orc_factor_forced_d(const orc_sym *s, const double *vals, const int *is_piv_init,
+                               int pivot, double threshold, int literal, const int *forced_grants);
+orc_fac_s *orc_factor_forced_s(const orc_sym *s, const float *vals, const int *is_piv_init,
+                               int pivot, float threshold, int literal, const int *forced_grants);
 void orc_fac_free_d(orc_fac_d *f);
 void orc_fac_free_s(orc_fac_s *f);
 

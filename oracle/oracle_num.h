@@ -7,6 +7,11 @@
  * Arithmetic is written with explicit fma() where the reference's CUDA source
  * has a multiply feeding an add (nvcc contracts those by default) and the
  * file is compiled with -ffp-contract=off, so every rounding is spelled out.
+ * nvcc's choices, as the reference's own sm_100a build computes them
+ * (oracle/_ref, tests/test_ref_parity.py): a*b + c*d -> fma(a, b, c*d);
+ * x - a*b -> fma(-a, b, x); -a*b + c*d (a negated product first) ->
+ * fma(c, d, -(a*b)): the negation is moved out of the product, the sum
+ * becomes c*d - a*b and the first product is the fused one.
  * Reference kernels followed (libs/la/preconditioner/block_ildlt_kernels.impl.cuh
  * unless noted):
  *   d_load_block                      :22-81
@@ -31,8 +36,10 @@
  *   k_sym_ortho                       libs/la/helper_kernels.impl.cuh:662-700
  *
  * Deterministic choices where the reference is racy:
- *   - dual dropping: blocks of a level are serialized in level-list order
- *     (the reference's CTAs race on one leftover counter, :1949-2008);
+ *   - dual dropping: a level's requests are served from the pool the earlier
+ *     levels left, in level-list order, and the level's spare slots join the
+ *     pool after the level (the reference's CTAs race on one leftover
+ *     counter, :1949-2008: each takes before it returns its own spare slots);
  *   - row norms: off-diagonal contributions are added in level-list order
  *     (the reference uses atomicAdd, :1792);
  *   - triangular sweeps: each fine row subtracts its off-diagonal terms in
@@ -64,7 +71,9 @@ typedef struct CAT(orc_fac, SUFFIX) {
     REAL *tri;
     int *is_piv, *perm;
     REAL *row_norm;
-    long leftover;
+    const int *forced_grants; /* per block: grants taken from another run, or NULL */
+    long leftover;        /* pool the blocks of the current level draw from */
+    long level_leftover;  /* spare slots the current level's blocks return */
 } F(fac_t);
 
 static int F(bsize)(const orc_sym *s, int blockrow) { return s->bs[blockrow + 1] - s->bs[blockrow]; }
@@ -168,13 +177,13 @@ static void F(step_2x2)(REAL T[32][32], REAL *D, int row, int len)
     const REAL gc = d11 / gr, gs = d12 / gr;
     const REAL td11 = FMA(gc, d11, gs * d12);
     const REAL td12 = FMA(gc, d12, gs * d22);
-    const REAL td22 = FMA(-gs, d12, gc * d22);
+    const REAL td22 = FMA(gc, d22, -(gs * d12));
     REAL u1[32], u2[32], r1[32], r2[32];
     for (int l = 0; l < 32; ++l) {
         const REAL a1 = (l < row) ? (REAL)0 : T[row][l];
         const REAL a2 = (l < row) ? (REAL)0 : ((l == row) ? d12 : T[row + 1][l]);
         REAL x1 = FMA(gc, a1, gs * a2);
-        REAL x2 = FMA(-gs, a1, gc * a2);
+        REAL x2 = FMA(gc, a2, -(gs * a1));
         x2 = x2 / td22;
         x1 = FMA(-td12, x2, x1) / td11;
         u1[l] = x1; u2[l] = x2;
@@ -340,10 +349,10 @@ static void F(left_solve_D_Ut)(REAL U[32][32], const REAL *D, REAL A[32][32],
             const REAL gr = SQRT(FMA(d11, d11, d12 * d12));
             const REAL gc = d11 / gr, gs = d12 / gr;
             REAL x1 = FMA(gc, rhs[l], gs * right);
-            REAL x2 = FMA(-gs, rhs[l], gc * right);
+            REAL x2 = FMA(gc, right, -(gs * rhs[l]));
             const REAL td11 = FMA(gc, d11, gs * d12);
             const REAL td12 = FMA(gc, d12, gs * d22);
-            const REAL td22 = FMA(-gs, d12, gc * d22);
+            const REAL td22 = FMA(gc, d22, -(gs * d12));
             x2 = two ? (x2 / td22) : (REAL)0;
             x1 = FMA(-td12, x2, x1) / td11;
             x1v[l] = x1; x2v[l] = x2;
@@ -384,12 +393,13 @@ static void F(drop_and_save)(F(fac_t) *f, int b, REAL T[32][32])
         const long req = nnz - mx;
         long granted = (req < f->leftover) ? req : f->leftover;
         if (granted < 0) granted = 0;
+        if (f->forced_grants) granted = f->forced_grants[b];
         f->leftover -= granted;
         mx += (int)granted;
         f->got_extra[b] = (int)granted;
     }
     f->maxnnz[b] = mx;
-    f->leftover += (mx - nnz > 0) ? (mx - nnz) : 0;
+    f->level_leftover += (mx - nnz > 0) ? (mx - nnz) : 0;
     const int cap = (nnz < mx) ? nnz : mx;
     free(f->idx[b]); free(f->val[b]);
     f->idx[b] = (int *)malloc(sizeof(int) * (cap ? cap : 1));
@@ -428,9 +438,19 @@ static void F(drop_and_save)(F(fac_t) *f, int b, REAL T[32][32])
 F(fac_t) *F(orc_factor)(const orc_sym *s, const REAL *vals, const int *is_piv_init,
                         int pivot, REAL threshold, int literal)
 {
+    return F(orc_factor_forced)(s, vals, is_piv_init, pivot, threshold, literal, NULL);
+}
+
+/* forced_grants (coarse_nnz entries, or NULL): the extra slots each block that
+ * outgrows its capacity receives, taken from another run (the reference's
+ * own grants race between a level's CTAs); NULL follows the pool */
+F(fac_t) *F(orc_factor_forced)(const orc_sym *s, const REAL *vals, const int *is_piv_init,
+                               int pivot, REAL threshold, int literal, const int *forced_grants)
+{
     F(fac_t) *f = (F(fac_t) *)calloc(1, sizeof(F(fac_t)));
     const int n = s->n, cnz = s->coarse_nnz;
     f->s = s; f->pivot = pivot; f->threshold = threshold; f->literal = literal;
+    f->forced_grants = forced_grants;
     f->nnz = (int *)calloc(cnz, sizeof(int));
     f->maxnnz = (int *)malloc(sizeof(int) * cnz);
     f->got_extra = (int *)calloc(cnz, sizeof(int));
@@ -574,6 +594,9 @@ F(fac_t) *F(orc_factor)(const orc_sym *s, const REAL *vals, const int *is_piv_in
                 }
             }
         }
+        /* the level's spare slots join the pool for the later levels */
+        f->leftover += f->level_leftover;
+        f->level_leftover = 0;
     }
     F(build_rowlists)(f, &f->U, &f->Ut);
     return f;
@@ -765,9 +788,9 @@ static void F(solve_D)(int n, const REAL *tri, const int *is_piv, const REAL *in
         const REAL gr = SQRT(FMA(p11, p11, p12 * p12));
         const REAL gc = p11 / gr, gs = p12 / gr;
         REAL g1 = FMA(gc, r1, gs * r2);
-        REAL g2 = FMA(-gs, r1, gc * r2);
+        REAL g2 = FMA(gc, r2, -(gs * r1));
         const REAL tp12 = FMA(gc, p12, gs * p22);
-        const REAL tp22 = FMA(-gs, p12, gc * p22);
+        const REAL tp22 = FMA(gc, p22, -(gs * p12));
         g2 = g2 / tp22;
         g1 = FMA(-tp12, g2, g1) / gr;
         if (this_piv) out[g] = g1;

@@ -183,6 +183,7 @@ public:
         w.put("is_piv", to_host<mat_int_t>(this->m_d_ispiv.get()));
         w.put("block_starts", this->m_h_block_starts->dense_val, (int64_t)this->m_h_block_starts->m);
         put_list(w, "coarse_off", "coarse_col", this->m_h_coarse_csr);
+        put_list(w, "csc_off", "csc_blk", this->m_h_coarse_csc);
         put_list(w, "level_off", "level_rows", this->m_h_levels);
         put_list(w, "lblk_off", "lblk", this->m_h_levels_blocks);
         w.put1<int32_t>("max_level_blks", this->m_max_level_blocks);
