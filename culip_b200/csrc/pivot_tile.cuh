@@ -31,7 +31,7 @@ __device__ __forceinline__ void schur_update_d(T* out, const T* Q, const T* R, u
             const T left = (lane > 0) ? Q[(lane - 1) * kTileStride + a] : T(0);
             const T mid = Q[lane * kTileStride + a];
             const T right = (lane < 31) ? Q[(lane + 1) * kTileStride + a] : T(0);
-            lv = fma_rn(sub, right, fma_rn(sup, left, dia * mid));
+            lv = fma_rn(sub, right, fma_rn(dia, mid, sup * left));  // the reference build's rounding order
         }
         unsigned m = __ballot_sync(0xffffffffu, lv != T(0));
         T acc = T(0);

@@ -137,10 +137,22 @@ static void prec_apply(const prec_t *P, int stage, const double *b, double *x)
 void orc_set_threads(int n) { omp_set_num_threads(n > 0 ? n : 1); }
 int orc_get_threads(void) { return omp_get_max_threads(); }
 
+/* a'b summed in DOT_CHUNKS fixed chunks (each in index order, the chunk sums
+ * in chunk order): the same roundings for any number of threads */
+#define DOT_CHUNKS 64
 static double dot(int n, const double *a, const double *b)
 {
+    double part[DOT_CHUNKS];
+    const int len = (n + DOT_CHUNKS - 1) / DOT_CHUNKS;
+#pragma omp parallel for schedule(static) if (n > 16384)
+    for (int c = 0; c < DOT_CHUNKS; ++c) {
+        const int lo = c * len, hi = (lo + len < n) ? lo + len : n;
+        double s = 0;
+        for (int i = lo; i < hi; ++i) s = fma(a[i], b[i], s);
+        part[c] = s;
+    }
     double s = 0;
-    for (int i = 0; i < n; ++i) s = fma(a[i], b[i], s);
+    for (int c = 0; c < DOT_CHUNKS; ++c) s += part[c];
     return s;
 }
 

@@ -11,7 +11,10 @@
  * (oracle/_ref, tests/test_ref_parity.py): a*b + c*d -> fma(a, b, c*d);
  * x - a*b -> fma(-a, b, x); -a*b + c*d (a negated product first) ->
  * fma(c, d, -(a*b)): the negation is moved out of the product, the sum
- * becomes c*d - a*b and the first product is the fused one.
+ * becomes c*d - a*b and the first product is the fused one;
+ * d_multiply_block_by_block_diagonal's sup*l + dia*m + sub*r ->
+ * fma(sub, r, fma(dia, m, sup*l)) (only rows next to a 2x2 pivot see a
+ * difference: elsewhere sup = sub = 0).
  * Reference kernels followed (libs/la/preconditioner/block_ildlt_kernels.impl.cuh
  * unless noted):
  *   d_load_block                      :22-81
@@ -73,7 +76,6 @@ typedef struct CAT(orc_fac, SUFFIX) {
     REAL *row_norm;
     const int *forced_grants; /* per block: grants taken from another run, or NULL */
     long leftover;        /* pool the blocks of the current level draw from */
-    long level_leftover;  /* spare slots the current level's blocks return */
 } F(fac_t);
 
 static int F(bsize)(const orc_sym *s, int blockrow) { return s->bs[blockrow + 1] - s->bs[blockrow]; }
@@ -113,7 +115,8 @@ static void F(mult_tridiag)(REAL Lt[32][32], const REAL *D, int h, int w)
         for (int r = 0; r < 32; ++r) old[r + 1] = Lt[a][r];
         for (int r = 0; r < w; ++r) {
             const REAL sup = D[3 * r], dia = D[3 * r + 1], sub = D[3 * r + 2];
-            Lt[a][r] = FMA(sub, old[r + 2], FMA(sup, old[r], dia * old[r + 1]));
+            /* sup*l + dia*m + sub*r as the reference's build rounds it */
+            Lt[a][r] = FMA(sub, old[r + 2], FMA(dia, old[r + 1], sup * old[r]));
         }
     }
 }
@@ -364,19 +367,14 @@ static void F(left_solve_D_Ut)(REAL U[32][32], const REAL *D, REAL A[32][32],
     }
 }
 
-/* k_apply_block_dual_dropping + d_save_block for one block, serialized. */
-static void F(drop_and_save)(F(fac_t) *f, int b, REAL T[32][32])
+/* k_apply_block_dual_dropping, first half: threshold dropping of a sparse
+ * block's tile and the count of its remaining entries (|v| > NZ_EPS). */
+static int F(drop_count)(const F(fac_t) *f, int b, REAL T[32][32])
 {
     const orc_sym *s = f->s;
     const int I = s->blk_row[b];
     const int h = F(bsize)(s, I), w = F(bsize)(s, s->blk_col[b]);
     const int from = s->bs[I];
-    if (s->fmt[b] == ORC_DENSE) {
-        for (int i = 0; i < h; ++i)
-            for (int j = 0; j < w; ++j) f->val[b][i * w + j] = T[i][j];
-        f->nnz[b] = 0;
-        return;
-    }
     int nnz = 0;
     for (int i = 0; i < h; ++i) {
         const REAL nrm = (REAL)sqrtf((float)f->row_norm[from + i]);
@@ -388,18 +386,23 @@ static void F(drop_and_save)(F(fac_t) *f, int b, REAL T[32][32])
             nnz += (!drop && nz);
         }
     }
-    int mx = f->maxnnz[b];
-    if (nnz > mx) {
-        const long req = nnz - mx;
-        long granted = (req < f->leftover) ? req : f->leftover;
-        if (granted < 0) granted = 0;
-        if (f->forced_grants) granted = f->forced_grants[b];
-        f->leftover -= granted;
-        mx += (int)granted;
-        f->got_extra[b] = (int)granted;
+    return nnz;
+}
+
+/* second half + d_save_block: store the tile in its final capacity mx
+ * (sparse: its nnz entries, or the mx largest |v| when nnz > mx). */
+static void F(save_block)(F(fac_t) *f, int b, REAL T[32][32], int nnz, int mx)
+{
+    const orc_sym *s = f->s;
+    const int I = s->blk_row[b];
+    const int h = F(bsize)(s, I), w = F(bsize)(s, s->blk_col[b]);
+    if (s->fmt[b] == ORC_DENSE) {
+        for (int i = 0; i < h; ++i)
+            for (int j = 0; j < w; ++j) f->val[b][i * w + j] = T[i][j];
+        f->nnz[b] = 0;
+        return;
     }
     f->maxnnz[b] = mx;
-    f->level_leftover += (mx - nnz > 0) ? (mx - nnz) : 0;
     const int cap = (nnz < mx) ? nnz : mx;
     free(f->idx[b]); free(f->val[b]);
     f->idx[b] = (int *)malloc(sizeof(int) * (cap ? cap : 1));
@@ -407,7 +410,6 @@ static void F(drop_and_save)(F(fac_t) *f, int b, REAL T[32][32])
     if (nnz > mx) {
         /* keep the mx largest |v|, ties to the lower tile index (stable
          * descending radix sort, :2016-2061); stored sorted by local index */
-        int chosen[1024];
         char taken[1024];
         memset(taken, 0, sizeof(taken));
         for (int k = 0; k < mx; ++k) {
@@ -419,12 +421,10 @@ static void F(drop_and_save)(F(fac_t) *f, int b, REAL T[32][32])
                 if (key > bv) { bv = key; best = t; }
             }
             taken[best] = 1;
-            chosen[k] = best;
         }
         int o = 0;
         for (int t = 0; t < 1024; ++t)
             if (taken[t]) { const int rr = t / 32, cc = t % 32; f->idx[b][o] = rr * w + cc; f->val[b][o] = T[rr][cc]; ++o; }
-        (void)chosen;
         f->nnz[b] = mx;
     } else {
         int o = 0;
@@ -434,6 +434,13 @@ static void F(drop_and_save)(F(fac_t) *f, int b, REAL T[32][32])
         f->nnz[b] = o;
     }
 }
+
+/* a sparse block of a level; b >= 0 and tile set when it outgrew its
+ * capacity and waits for the level's grants */
+typedef struct {
+    int b, nnz;
+    REAL (*T)[32];
+} F(pending_t);
 
 F(fac_t) *F(orc_factor)(const orc_sym *s, const REAL *vals, const int *is_piv_init,
                         int pivot, REAL threshold, int literal)
@@ -485,12 +492,20 @@ F(fac_t) *F(orc_factor_forced)(const orc_sym *s, const REAL *vals, const int *is
         }
     }
 
-    static REAL T[32][32], Lt[32][32], R[32][32];
+    /* the rows of a level are independent (each reads the levels before
+     * it): steps 1-3 run over the level's block rows on all threads; only
+     * the grants of the blocks that outgrow their capacity go in level-list
+     * order, so the result does not depend on the thread count */
+    int *row_first = (int *)malloc(sizeof(int) * (s->num_blocks + 1));
+    F(pending_t) *pend = NULL;
+    int pend_cap = 0;
     for (int L = 0; L < s->num_levels; ++L) {
         const int lb0 = s->lb_off[L], lb1 = s->lb_off[L + 1];
         const int npiv = s->lvl_off[L + 1] - s->lvl_off[L];
         /* step 1: pivot blocks (k_factor_pivot_blocks) */
+#pragma omp parallel for schedule(dynamic, 4) if (npiv > 64)
         for (int t = lb0; t < lb0 + npiv; ++t) {
+            REAL T[32][32], Lt[32][32], R[32][32];
             const int b = s->lb[t];
             const int I = s->blk_row[b];
             const int from = s->bs[I], len = F(bsize)(s, I);
@@ -511,19 +526,41 @@ F(fac_t) *F(orc_factor_forced)(const orc_sym *s, const REAL *vals, const int *is
                 for (int j = 0; j < len; ++j) rs = FMA(T[l][j], T[l][j], rs);
                 f->row_norm[from + l] = rs;
             }
-            F(drop_and_save)(f, b, T); /* dense: exact copy */
+            F(save_block)(f, b, T, 0, 0); /* dense: exact copy */
         }
         /* steps 2-4 per block row (off-diagonal blocks are grouped by row) */
-        int t = lb0 + npiv;
-        while (t < lb1) {
+        int nrows = 0;
+        for (int t = lb0 + npiv; t < lb1; ++t)
+            if (t == lb0 + npiv || s->blk_row[s->lb[t]] != s->blk_row[s->lb[t - 1]]) row_first[nrows++] = t;
+        row_first[nrows] = lb1;
+        long spare = 0;
+        int npend = 0;
+        for (int t = lb0 + npiv; t < lb1; ++t) {
+            const int b = s->lb[t];
+            npend += (s->fmt[b] == ORC_SPARSE);
+        }
+        if (npend > pend_cap) {
+            free(pend);
+            pend_cap = npend;
+            pend = (F(pending_t) *)malloc(sizeof(F(pending_t)) * (pend_cap ? pend_cap : 1));
+        }
+        /* pend[k] is the k-th sparse block of the level's list (b < 0: fits) */
+        int *pend_base = (int *)malloc(sizeof(int) * (nrows + 1));
+        pend_base[0] = 0;
+        for (int r = 0; r < nrows; ++r) {
+            int c = 0;
+            for (int t = row_first[r]; t < row_first[r + 1]; ++t) c += (s->fmt[s->lb[t]] == ORC_SPARSE);
+            pend_base[r + 1] = pend_base[r] + c;
+        }
+#pragma omp parallel for schedule(dynamic, 1) reduction(+ : spare) if (nrows > 16)
+        for (int r = 0; r < nrows; ++r) {
+            REAL Lt[32][32], R[32][32], U[32][32];
+            const int t = row_first[r], t_end = row_first[r + 1];
             const int I = s->blk_row[s->lb[t]];
-            int t_end = t;
-            while (t_end < lb1 && s->blk_row[s->lb[t_end]] == I) ++t_end;
             const int nb = t_end - t;
             REAL (*tiles)[32][32] = (REAL (*)[32][32])malloc(sizeof(REAL) * 1024 * (nb ? nb : 1));
             const int from = s->bs[I], h = F(bsize)(s, I);
             /* the row's pivot tile from final (dense) storage */
-            REAL U[32][32];
             const int pb = s->csc_blk[s->csc_off[I + 1] - 1];
             F(load_tile)(f, pb, U, 0);
             for (int k = 0; k < nb; ++k) {
@@ -562,12 +599,52 @@ F(fac_t) *F(orc_factor_forced)(const orc_sym *s, const REAL *vals, const int *is
                         f->row_norm[from + l] += rs;
                     }
             }
-            for (int k = 0; k < nb; ++k) F(drop_and_save)(f, s->lb[t + k], tiles[k]);
+            /* dropping: blocks within capacity are stored now, the others wait
+             * for the level's grants */
+            int pk = pend_base[r];
+            for (int k = 0; k < nb; ++k) {
+                const int b = s->lb[t + k];
+                if (s->fmt[b] == ORC_DENSE) {
+                    F(save_block)(f, b, tiles[k], 0, 0);
+                    continue;
+                }
+                const int nnz = F(drop_count)(f, b, tiles[k]);
+                const int mx = f->maxnnz[b];
+                if (nnz > mx) {
+                    pend[pk].b = b;
+                    pend[pk].nnz = nnz;
+                    pend[pk].T = (REAL (*)[32])malloc(sizeof(REAL) * 1024);
+                    memcpy(pend[pk].T, tiles[k], sizeof(REAL) * 1024);
+                } else {
+                    pend[pk].b = -1;
+                    F(save_block)(f, b, tiles[k], nnz, mx);
+                    spare += mx - nnz;
+                }
+                ++pk;
+            }
             free(tiles);
-            t = t_end;
         }
+        /* the level's requests, in level-list order, from the pool the earlier
+         * levels left */
+        for (int k = 0; k < pend_base[nrows]; ++k) {
+            if (pend[k].b < 0) continue;
+            const int b = pend[k].b, nnz = pend[k].nnz;
+            int mx = f->maxnnz[b];
+            const long req = nnz - mx;
+            long granted = (req < f->leftover) ? req : f->leftover;
+            if (granted < 0) granted = 0;
+            if (f->forced_grants) granted = f->forced_grants[b];
+            f->leftover -= granted;
+            mx += (int)granted;
+            f->got_extra[b] = (int)granted;
+            spare += (mx - nnz > 0) ? (mx - nnz) : 0;
+            F(save_block)(f, b, pend[k].T, nnz, mx);
+            free(pend[k].T);
+        }
+        free(pend_base);
         /* step 3 (k_pivot_col_blocks): propagate pivot permutations upwards */
         if (pivot != ORC_PIV_STATIC) {
+#pragma omp parallel for schedule(dynamic, 8) if (npiv > 64)
             for (int q = s->lvl_off[L]; q < s->lvl_off[L + 1]; ++q) {
                 const int I = s->lvl_rows[q];
                 const int from = s->bs[I], bw = F(bsize)(s, I);
@@ -595,9 +672,10 @@ F(fac_t) *F(orc_factor_forced)(const orc_sym *s, const REAL *vals, const int *is
             }
         }
         /* the level's spare slots join the pool for the later levels */
-        f->leftover += f->level_leftover;
-        f->level_leftover = 0;
+        f->leftover += spare;
     }
+    free(row_first);
+    free(pend);
     F(build_rowlists)(f, &f->U, &f->Ut);
     return f;
 }
@@ -880,19 +958,22 @@ void F(orc_prec_apply)(const F(fac_t) *f, int stage, const REAL *b, REAL *x)
     const int n = s->n;
     if (stage == 1) {
         REAL *t = (REAL *)malloc(sizeof(REAL) * (n ? n : 1));
-        memcpy(t, b, sizeof(REAL) * n);
-        memcpy(x, b, sizeof(REAL) * n);
+#pragma omp parallel for schedule(static) if (n > 16384)
+        for (int g = 0; g < n; ++g) { t[g] = b[g]; x[g] = b[g]; }
         F(solve_D)(n, f->tri, f->is_piv, t, x);
         free(t);
         return;
     }
     if (stage == 0) {
+#pragma omp parallel for schedule(static) if (n > 16384)
         for (int g = 0; g < n; ++g) x[g] = b[f->perm[g]];        /* k_permute_Pt */
         F(solve_Ut)(f, &f->Ut, x);
     } else {
         REAL *t = (REAL *)malloc(sizeof(REAL) * (n ? n : 1));
-        memcpy(t, b, sizeof(REAL) * n);
+#pragma omp parallel for schedule(static) if (n > 16384)
+        for (int g = 0; g < n; ++g) t[g] = b[g];
         F(solve_U)(f, &f->U, t);
+#pragma omp parallel for schedule(static) if (n > 16384)
         for (int g = 0; g < n; ++g) x[f->perm[g]] = t[g];        /* k_permute_P */
         free(t);
     }
