@@ -331,7 +331,15 @@ __device__ __forceinline__ void spmv_row(const PArgs<TF>& a, int q, const double
 // x_c = t_c / U_cc, t_r -= U_rc x_c (r < c), for each right-hand side.  The
 // division is taken only where bit c of nd says U_cc != 1 (t / 1 == t
 // exactly); with nd == 0 the chain is shuffle + fma per step.
-template <class TF, int NR, bool DIV>
+// SM: P is a copy of the column-packed triangle in shared memory
+template <bool SM, class TF>
+__device__ __forceinline__ TF tile_ld(const TF* p)
+{
+    if (SM) return *p;
+    return __ldg(p);
+}
+
+template <class TF, int NR, bool DIV, bool SM>
 __device__ __forceinline__ void tile_upper_t(TF (&t)[NR], const TF* __restrict__ P, int h, unsigned nd)
 {
     const int lane = (int)lane_id();
@@ -341,7 +349,7 @@ __device__ __forceinline__ void tile_upper_t(TF (&t)[NR], const TF* __restrict__
 #pragma unroll
         for (int j = 0; j < B; ++j) {
             const int c = c0 - j;
-            u[j] = (c >= 0 && lane <= c) ? __ldg(P + c * (c + 1) / 2 + lane) : TF(0);
+            u[j] = (c >= 0 && lane <= c) ? tile_ld<SM>(P + c * (c + 1) / 2 + lane) : TF(0);
         }
 #pragma unroll
         for (int j = 0; j < B; ++j) {
@@ -364,8 +372,11 @@ __device__ __forceinline__ void tile_upper_t(TF (&t)[NR], const TF* __restrict__
 
 // Forward substitution with the upper triangle packed row by row (U'
 // sweep): for r = 0 .. h-1: x_r = t_r / U_rr, t_c -= U_rc x_r (r < c < h);
-// divisions as in tile_upper_t
-template <class TF, int NR, bool DIV>
+// divisions as in tile_upper_t.  With SM the triangle is the column-packed
+// copy in shared memory, read along its rows: lane c reads c(c+1)/2 + r, and
+// c(c+1)/2 mod 16 is a permutation of 0..15 on each half-warp, so the
+// 8-byte reads of a half-warp hit distinct banks.
+template <class TF, int NR, bool DIV, bool SM>
 __device__ __forceinline__ void tile_lower_t(TF (&t)[NR], const TF* __restrict__ P, int h, unsigned nd)
 {
     const int lane = (int)lane_id();
@@ -375,7 +386,9 @@ __device__ __forceinline__ void tile_lower_t(TF (&t)[NR], const TF* __restrict__
 #pragma unroll
         for (int j = 0; j < B; ++j) {
             const int r = r0 + j;
-            u[j] = (r < h && lane >= r && lane < h) ? __ldg(P + r * h - r * (r - 1) / 2 + lane - r) : TF(0);
+            u[j] = (r < h && lane >= r && lane < h)
+                       ? (SM ? P[lane * (lane + 1) / 2 + r] : __ldg(P + r * h - r * (r - 1) / 2 + lane - r))
+                       : TF(0);
         }
 #pragma unroll
         for (int j = 0; j < B; ++j) {
@@ -396,26 +409,26 @@ __device__ __forceinline__ void tile_lower_t(TF (&t)[NR], const TF* __restrict__
     }
 }
 
-template <class TF, int NR>
+template <class TF, int NR, bool SM = false>
 __device__ __forceinline__ void tile_upper(double (&v)[NR], const TF* P, int h, unsigned nd)
 {
     TF t[NR];
 #pragma unroll
     for (int r = 0; r < NR; ++r) t[r] = (TF)v[r];
-    if (nd) tile_upper_t<TF, NR, true>(t, P, h, nd);
-    else tile_upper_t<TF, NR, false>(t, P, h, 0u);
+    if (nd) tile_upper_t<TF, NR, true, SM>(t, P, h, nd);
+    else tile_upper_t<TF, NR, false, SM>(t, P, h, 0u);
 #pragma unroll
     for (int r = 0; r < NR; ++r) v[r] = (double)t[r];
 }
 
-template <class TF, int NR>
+template <class TF, int NR, bool SM = false>
 __device__ __forceinline__ void tile_lower(double (&v)[NR], const TF* P, int h, unsigned nd)
 {
     TF t[NR];
 #pragma unroll
     for (int r = 0; r < NR; ++r) t[r] = (TF)v[r];
-    if (nd) tile_lower_t<TF, NR, true>(t, P, h, nd);
-    else tile_lower_t<TF, NR, false>(t, P, h, 0u);
+    if (nd) tile_lower_t<TF, NR, true, SM>(t, P, h, nd);
+    else tile_lower_t<TF, NR, false, SM>(t, P, h, 0u);
 #pragma unroll
     for (int r = 0; r < NR; ++r) v[r] = (double)t[r];
 }
@@ -456,6 +469,71 @@ __device__ __forceinline__ ItemMeta meta_of_item(const PArgs<TF>& a, int t)
     m.pko = (long long)(((unsigned long long)(unsigned)w.y << 32) | (unsigned)w.x);
     m.nd = (unsigned)w.z;
     return m;
+}
+
+// Shared-memory copy of one warp's pivot-tile work item, loaded once per
+// solve.  Each warp of the persistent kernel keeps the same item of a level
+// for the whole solve (item c0 + wid), so the level with the most such items
+// keeps, per warp slot, the item's metadata, its lanes' permuted rows and U /
+// U' row ranges, D's diagonal (block rows without 2x2 pivots) and the pivot
+// tile's upper triangle (column-packed).  The item's per-iteration chain of
+// dependent loads (descriptor, permutation and offsets, four batches of tile
+// values, D) becomes shared-memory reads.
+constexpr int kResSlots = 12;  // warps per CTA with a resident item
+constexpr int kTileMax = 32 * 33 / 2;
+
+template <class TF>
+struct ResSlot {
+    ItemMeta m;  // m.h == 0: the warp has no item of the resident level
+    int q[32];   // perm[fr + lane]
+    int u0[32], u1[32], ut0[32], ut1[32];
+    double d[32];
+    TF tile[kTileMax];
+};
+
+// warp-collective: fills the slot with item t of the citem list (has) or marks it empty
+template <class TF>
+__device__ void res_load(const PArgs<TF>& a, ResSlot<TF>& rs, int t, bool has)
+{
+    const int lane = (int)lane_id();
+    if (!has) {
+        if (lane == 0) rs.m.h = 0;
+        return;
+    }
+    const ItemMeta m = meta_of_item(a, t);
+    if (lane == 0) rs.m = m;
+    const int fr = m.fr, h = m.h;
+    if (lane < h) {
+        const int g = fr + lane;
+        rs.q[lane] = (m.flags & kRowPermIdentity) ? g : __ldg(a.perm + g);
+        rs.u0[lane] = __ldg(a.u_off + g);
+        rs.u1[lane] = __ldg(a.u_off + g + 1);
+        rs.ut0[lane] = __ldg(a.ut_off + g);
+        rs.ut1[lane] = __ldg(a.ut_off + g + 1);
+        rs.d[lane] = (m.flags & kRowHas2x2) ? 1.0 : (double)__ldg(a.dg + g);
+    }
+    if (!(m.flags & kRowIdentity))
+        for (int e = lane; e < h * (h + 1) / 2; e += 32) rs.tile[e] = __ldg(a.pk_col + m.pko + e);
+}
+
+// D of a resident item: its diagonal from the slot, or the Givens form from
+// global memory when the block row has a 2x2 pivot
+template <class TF>
+__device__ __forceinline__ DBlock<TF> dblock_res(const PArgs<TF>& a, const ResSlot<TF>& rs)
+{
+    DBlock<TF> D;
+    const int flags = rs.m.flags, h = rs.m.h;
+    if (flags & kRowHas2x2) {
+        D.load(a, rs.m.fr, h, flags);
+        return D;
+    }
+    const int lane = (int)lane_id();
+    D.two = false;
+    D.d = (lane < h) ? rs.d[lane] : 1.0;
+    D.gc = D.gs = D.tp12 = 0.0;
+    D.tp22 = D.gr = 1.0;
+    D.ip = true;
+    return D;
 }
 
 // One U-sweep work item: block row I (rows fr .. fr+h-1), lane's right-hand
@@ -533,6 +611,71 @@ __device__ __forceinline__ void ut_item(const PArgs<TF>& a, const ItemMeta& m, c
     // with kRhsPre the lanes read dst inside this block row: all reads before any write
     if (FROM == kRhsPre) __syncwarp();
     if (!(flags & kRowIdentity)) tile_lower<TF, NR>(t, a.pk_row + m.pko, h, m.nd);
+    if (lane < h)
+#pragma unroll
+        for (int r = 0; r < NR; ++r) dst[(size_t)(fr + lane) * NR + r] = t[r];
+}
+
+// u_item / ut_item of a resident item (same arithmetic, data from the slot)
+template <class TF, int NR>
+__device__ __forceinline__ void u_item_res(const PArgs<TF>& a, const ResSlot<TF>& rs, const double (&y)[NR],
+                                           double* out, double (&d)[NR])
+{
+    const int lane = (int)lane_id();
+    const int h = rs.m.h, flags = rs.m.flags;
+    const DBlock<TF> D = dblock_res(a, rs);
+#pragma unroll
+    for (int r = 0; r < NR; ++r) d[r] = D.apply(y[r], h);
+    double t[NR];
+#pragma unroll
+    for (int r = 0; r < NR; ++r) t[r] = d[r];
+    if (lane < h) {
+        TF acc[NR];
+#pragma unroll
+        for (int r = 0; r < NR; ++r) acc[r] = (TF)d[r];
+        row_sub<TF, NR>(acc, rs.u0[lane], rs.u1[lane], a.u_colp, a.u_val, out);
+#pragma unroll
+        for (int r = 0; r < NR; ++r) t[r] = (double)acc[r];
+    }
+    if (!(flags & kRowIdentity)) tile_upper<TF, NR, true>(t, rs.tile, h, rs.m.nd);
+    if (lane < h) {
+        const int q = rs.q[lane];
+#pragma unroll
+        for (int r = 0; r < NR; ++r) out[(size_t)q * NR + r] = t[r];
+    }
+}
+
+template <class TF, int NR, int FROM>
+__device__ __forceinline__ void ut_item_res(const PArgs<TF>& a, const ResSlot<TF>& rs, const double* src,
+                                            const double (&sc)[NR], double* dst, double (&t)[NR])
+{
+    const int lane = (int)lane_id();
+    const int fr = rs.m.fr, h = rs.m.h, flags = rs.m.flags;
+#pragma unroll
+    for (int r = 0; r < NR; ++r) t[r] = 0.0;
+    if (lane < h) {
+        const int q = rs.q[lane];
+        double y[NR];
+        if (FROM == kRhsSpmv) {
+            spmv_row<TF, NR>(a, q, src, y);
+#pragma unroll
+            for (int r = 0; r < NR; ++r) y[r] *= sc[r];
+        } else if (FROM == kRhsPre) {
+#pragma unroll
+            for (int r = 0; r < NR; ++r) y[r] = dst[(size_t)q * NR + r];
+        } else {
+#pragma unroll
+            for (int r = 0; r < NR; ++r) y[r] = src[(size_t)r * a.n + q];
+        }
+        TF acc[NR];
+#pragma unroll
+        for (int r = 0; r < NR; ++r) acc[r] = (TF)y[r];
+        row_sub<TF, NR>(acc, rs.ut0[lane], rs.ut1[lane], a.ut_col, a.ut_val, dst);
+#pragma unroll
+        for (int r = 0; r < NR; ++r) t[r] = (double)acc[r];
+    }
+    if (FROM == kRhsPre) __syncwarp();
+    if (!(flags & kRowIdentity)) tile_lower<TF, NR, true>(t, rs.tile, h, rs.m.nd);
     if (lane < h)
 #pragma unroll
         for (int r = 0; r < NR; ++r) dst[(size_t)(fr + lane) * NR + r] = t[r];
@@ -682,7 +825,8 @@ __device__ __forceinline__ LvlBounds level_bounds(const PArgs<TF>& a, const SysV
 }
 
 template <class TF, int NR, class Ctx>
-__device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal (&S)[NR], double (*sh)[kW])
+__device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal (&S)[NR], double (*sh)[kW],
+                          ResSlot<TF>* slots = nullptr)
 {
     const int tid = threadIdx.x, lane = (int)lane_id();
     const int wid = ctx.wid, nwarps = ctx.nwarps;
@@ -705,6 +849,33 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal 
     }
     __syncthreads();
     auto lvl = [&](int L) -> LvlBounds { return L < kLvlCache ? lvb[L] : level_bounds(a, sv, L); };
+
+    // the level with the most pivot-tile items keeps its first kResSlots x
+    // (grid) items in the warps' shared-memory slots
+    __shared__ int res_level_s;
+    if (tid == 0) {
+        int best = -1, most = 0;
+        if (slots)
+            for (int L = 0; L < a.nl; ++L) {
+                const LvlBounds b = lvl(L);
+                if (b.c1 - b.c0 > most) {
+                    most = b.c1 - b.c0;
+                    best = L;
+                }
+            }
+        res_level_s = best;
+    }
+    __syncthreads();
+    const int res_level = res_level_s;
+    ResSlot<TF>* const rs = (res_level >= 0 && (tid >> 5) < kResSlots) ? slots + (tid >> 5) : nullptr;
+    int res_t = -1;  // the item of the resident level this warp holds
+    if (rs) {
+        const LvlBounds rb = lvl(res_level);
+        const int t = rb.c0 + wid;
+        res_load(a, *rs, t, t < rb.c1);
+        if (t < rb.c1) res_t = t;
+    }
+    __syncthreads();
 
     // ---- init: v0 = U'^-1 P' b; ||v0|| ----
     {
@@ -848,7 +1019,8 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal 
                 // block rows with a pivot tile, swaps or 2x2 pivots: warp per block row
                 const int c1 = lb.c1;
                 for (int t = lb.c0 + wid; t < c1; t += nwarps) {
-                    const ItemMeta m = meta_of_item(a, t);
+                    const bool res = (t == res_t && L == res_level);
+                    const ItemMeta m = res ? rs->m : meta_of_item(a, t);
                     const int fr = m.fr, h = m.h;
                     double y[NR], d[NR];
 #pragma unroll
@@ -865,7 +1037,8 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal 
                             y[j] = v;
                         }
                     }
-                    u_item<TF, NR>(a, m, y, a.ev, d);
+                    if (res) u_item_res<TF, NR>(a, *rs, y, a.ev, d);
+                    else u_item<TF, NR>(a, m, y, a.ev, d);
                 }
                 // rows of simple block rows: thread per row (u_item with D = d,
                 // an identity tile and no swaps)
@@ -945,16 +1118,23 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal 
                 const LvlBounds lb = lvl(L);
                 const int c1 = lb.c1;
                 for (int t = lb.c0 + wid; t < c1; t += nwarps) {
-                    const ItemMeta m = meta_of_item(a, t);
+                    const bool res = (t == res_t && L == res_level);
+                    const ItemMeta m = res ? rs->m : meta_of_item(a, t);
                     const int fr = m.fr, h = m.h, flags = m.flags;
                     double av[NR];
                     double scv[NR];
 #pragma unroll
                     for (int j = 0; j < NR; ++j) scv[j] = cf.sc[j];
-                    if (L == 0) ut_item<TF, NR, kRhsSpmv>(a, m, a.ev, scv, a.Av, av);
-                    else ut_item<TF, NR, kRhsPre>(a, m, a.ev, scv, a.Av, av);
                     DBlock<TF> D;
-                    D.load(a, fr, h, flags);
+                    if (res) {
+                        if (L == 0) ut_item_res<TF, NR, kRhsSpmv>(a, *rs, a.ev, scv, a.Av, av);
+                        else ut_item_res<TF, NR, kRhsPre>(a, *rs, a.ev, scv, a.Av, av);
+                        D = dblock_res(a, *rs);
+                    } else {
+                        if (L == 0) ut_item<TF, NR, kRhsSpmv>(a, m, a.ev, scv, a.Av, av);
+                        else ut_item<TF, NR, kRhsPre>(a, m, a.ev, scv, a.Av, av);
+                        D.load(a, fr, h, flags);
+                    }
 #pragma unroll
                     for (int j = 0; j < NR; ++j) {
                         double vkr = 0.0, vs = 0.0;
@@ -1133,16 +1313,24 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal 
     __syncthreads();
 }
 
+// launched with kResSlots ResSlot<TF> of dynamic shared memory
 template <class TF, int CTAS, int NR>
 __global__ void __launch_bounds__(kT, CTAS) k_sqmr_persistent(PArgs<TF> a)
 {
     __shared__ Scal S[NR];
     __shared__ double sh[kMaxNV][kW];
+    extern __shared__ __align__(16) unsigned char res_smem[];
     const int G = gridDim.x;
     GridCtx ctx{cg::this_grid(), a.partials, 0, (int)(threadIdx.x >> 5) * G + (int)blockIdx.x,  // items interleaved
                 G * kW, (int)(blockIdx.x * kT + threadIdx.x), G * kT};
     const SysView sv{0, a.n, a.lvl_off, a.lvl_off + 1, blockIdx.x == 0 ? a.out : nullptr};
-    sqmr_body<TF, NR>(a, ctx, sv, S, sh);
+    sqmr_body<TF, NR>(a, ctx, sv, S, sh, reinterpret_cast<ResSlot<TF>*>(res_smem));
+}
+
+template <class TF>
+constexpr size_t res_smem_bytes()
+{
+    return (size_t)kResSlots * sizeof(ResSlot<TF>);
 }
 
 // Batched solves of independent systems stored as one block-diagonal union
@@ -1290,7 +1478,11 @@ int persistent_grid(int dev, int* G)
 {
     int per_sm = 0, sms = 0;
     CULIPX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    CULIPX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, persistent_kernel<TF, NR>(), kT, 0));
+    // the resident item slots need more than the default 48 KB of dynamic shared memory
+    CULIPX_CUDA(cudaFuncSetAttribute(persistent_kernel<TF, NR>(), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)res_smem_bytes<TF>()));
+    CULIPX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, persistent_kernel<TF, NR>(), kT,
+                                                              res_smem_bytes<TF>()));
     if (per_sm < 1) return fail(CULIPX_NOT_SUPPORTED, "persistent SQMR kernel does not fit on an SM");
     *G = sms * std::min(per_sm, ctas_per_sm());
     return CULIPX_OK;
@@ -1332,7 +1524,8 @@ int run_persistent(culipx_handle_t* h, PArgs<TF>& a, int G, double* out_host, bo
     CULIPX_CUDA(cudaMemsetAsync(a.v[0], 0, (size_t)kVecs * a.n * NR * sizeof(double), s));
     CULIPX_CUDA(cudaMemsetAsync(a.x, 0, (size_t)a.n * NR * sizeof(double), s));
     void* args[] = {&a};
-    CULIPX_CUDA(cudaLaunchCooperativeKernel(persistent_kernel<TF, NR>(), dim3(G), dim3(kT), args, 0, s));
+    CULIPX_CUDA(cudaLaunchCooperativeKernel(persistent_kernel<TF, NR>(), dim3(G), dim3(kT), args,
+                                            res_smem_bytes<TF>(), s));
     h->launches += 1;
     CULIPX_CUDA(cudaMemcpyAsync(out_host, a.out, (size_t)8 * NR * sizeof(double), cudaMemcpyDeviceToHost, s));
     if (wait) CULIPX_CUDA(cudaStreamSynchronize(s));
