@@ -18,8 +18,8 @@ import ctypes
 import numpy as np
 
 from . import _capi as capi
-from ._capi import (F32, F64, LEFT, MIDDLE, PIV_BK, PIV_ROOK, PIV_STATIC, RIGHT, SOLVE_BLOCK,  # noqa: F401
-                    SOLVE_JACOBI, SOLVE_SCALAR, SOLVE_STRIPE, CulipxError, KktSpec)
+from ._capi import (F32, F64, FMT_CSR, FMT_SELL, LEFT, MIDDLE, PIV_BK, PIV_ROOK, PIV_STATIC, RIGHT,  # noqa: F401
+                    SOLVE_BLOCK, SOLVE_JACOBI, SOLVE_SCALAR, SOLVE_STRIPE, CulipxError, KktSpec)
 
 __all__ = ["Handle", "Pattern", "Factor", "CsrOperator", "PermutePlan", "BlockiLDLt", "CSRMatrixSPMV", "SQMR", "kkt_generate",
            "kkt_blocking", "normal_vector", "CulipxError", "KKT_CONFIGS"]
@@ -248,6 +248,12 @@ class Factor:
     def set_solve_algorithm(self, algorithm, sweeps=0):
         capi.call("culipx_factor_set_solve_algorithm", self._h, int(algorithm), int(sweeps))
 
+    def set_pivot_fp64(self, bound):
+        """FP32 factors: 2x2 pivots with |d11 d22 - d12^2| / (|d11 d22| + d12^2)
+        below bound are inverted in FP64 (default 1e-3; 0 = the reference's
+        FP32 arithmetic).  Used by the next compute."""
+        capi.call("culipx_factor_set_pivot_fp64", self._h, float(bound))
+
     def stats(self):
         ms = ctypes.c_double()
         nl = ctypes.c_int()
@@ -349,6 +355,14 @@ class CsrOperator:
     def spmv(self, x, y, alpha=1.0, beta=0.0, transpose=False):
         capi.call("culipx_spmv", self._h, _dptr(x), _dptr(y), float(alpha), float(beta), 1 if transpose else 0)
         return y
+
+    def set_format(self, fmt):
+        """FMT_CSR (the borrowed arrays) or FMT_SELL (a SELL-32 copy of
+        structure and values, built now; refresh() after changing val)."""
+        capi.call("culipx_csr_set_format", self._h, int(fmt))
+
+    def refresh(self):
+        capi.call("culipx_csr_refresh", self._h)
 
     def __del__(self):
         try:
@@ -634,13 +648,14 @@ def sqmr_refine(handle: Handle, A: CsrOperator, M: Factor, b, x, tol=1e-8, inner
                 max_refine=20):
     """FP64 iterative refinement around SQMR (mixed precision with an FP32
     factor).  Returns (relres, total SQMR iterations, corrections, status);
-    status is OK or MAXIT."""
+    status is OK, MAXIT or STALLED (two corrections in a row did not lower
+    the true residual); x is the iterate of smallest residual."""
     rel = ctypes.c_double()
     its = ctypes.c_int()
     steps = ctypes.c_int()
     st = capi.call("culipx_sqmr_refine", handle._h, A._h, M._h, _dptr(b), _dptr(x), float(tol), float(inner_tol),
                    int(inner_max_it), int(max_refine), ctypes.byref(rel), ctypes.byref(its), ctypes.byref(steps),
-                   allow=(capi.OK, capi.MAXIT))
+                   allow=(capi.OK, capi.MAXIT, capi.STALLED))
     return rel.value, its.value, steps.value, st
 
 

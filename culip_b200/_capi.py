@@ -12,14 +12,15 @@ import os
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "lib", "libculipx.so")
 
-OK, INVALID_ARG, OOM, BREAKDOWN, MAXIT, TIMEOUT, CUDA_ERROR, NOT_SUPPORTED, PENDING = range(9)
+OK, INVALID_ARG, OOM, BREAKDOWN, MAXIT, TIMEOUT, CUDA_ERROR, NOT_SUPPORTED, PENDING, STALLED = range(10)
 F64, F32 = 0, 1
 PIV_STATIC, PIV_BK, PIV_ROOK = 0, 1, 2
 LEFT, MIDDLE, RIGHT = 0, 1, 2
 SOLVE_STRIPE, SOLVE_BLOCK, SOLVE_SCALAR, SOLVE_JACOBI = 0, 1, 2, 3
+FMT_CSR, FMT_SELL = 0, 1
 
 STATUS_NAMES = {0: "OK", 1: "INVALID_ARG", 2: "OOM", 3: "BREAKDOWN", 4: "MAXIT", 5: "TIMEOUT", 6: "CUDA_ERROR",
-                7: "NOT_SUPPORTED", 8: "PENDING"}
+                7: "NOT_SUPPORTED", 8: "PENDING", 9: "STALLED"}
 
 
 class CulipxError(RuntimeError):
@@ -69,6 +70,7 @@ _SIGS = {
     "culipx_factor_info": [vp, vp],
     "culipx_prec_apply": [vp, i32, vp, vp],
     "culipx_factor_set_solve_algorithm": [vp, i32, i32],
+    "culipx_factor_set_pivot_fp64": [vp, f64],
     "culipx_permute_create": [vp, i32, i64, vp, vp, vp, vp, i32, ctypes.POINTER(vp)],
     "culipx_permute_destroy": [vp],
     "culipx_permute_structure": [vp, ctypes.POINTER(vp), ctypes.POINTER(vp)],
@@ -77,6 +79,8 @@ _SIGS = {
     "culipx_csr_create": [vp, i32, i32, i64, vp, vp, vp, i32, i32, ctypes.POINTER(vp)],
     "culipx_csr_destroy": [vp],
     "culipx_spmv": [vp, vp, vp, f64, f64, i32],
+    "culipx_csr_set_format": [vp, i32],
+    "culipx_csr_refresh": [vp],
     "culipx_sqmr_solve": [vp, vp, vp, vp, vp, f64, i32, ctypes.POINTER(f64), ctypes.POINTER(i32)],
     "culipx_sqmr_solve_noalloc": [vp, vp, vp, vp, vp, f64, i32, ctypes.POINTER(f64), ctypes.POINTER(i32)],
     "culipx_vec_dot": [vp, i32, i64, vp, vp, ctypes.POINTER(f64)],

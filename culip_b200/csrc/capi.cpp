@@ -377,6 +377,14 @@ CULIPX_API int culipx_factor_set_solve_algorithm(culipx_factor f, int algorithm,
     return CULIPX_OK;
 }
 
+CULIPX_API int culipx_factor_set_pivot_fp64(culipx_factor f, double bound)
+{
+    if (!f) return fail(CULIPX_INVALID_ARG, "null factor");
+    if (!(bound >= 0.0) || bound > 1.0) return fail(CULIPX_INVALID_ARG, "culipx_factor_set_pivot_fp64: bound not in [0, 1]");
+    f->pivot_fp64 = bound;
+    return CULIPX_OK;
+}
+
 CULIPX_API int culipx_prec_apply(culipx_factor f, int stage, const void* d_b, void* d_x)
 {
     if (!f) return fail(CULIPX_INVALID_ARG, "null factor");
@@ -483,6 +491,30 @@ CULIPX_API int culipx_csr_destroy(culipx_csr A)
         handle_release(h);
     }
     return CULIPX_OK;
+}
+
+CULIPX_API int culipx_csr_set_format(culipx_csr A, int format)
+{
+    if (!A) return fail(CULIPX_INVALID_ARG, "null operator");
+    if (format != CULIPX_FMT_CSR && format != CULIPX_FMT_SELL)
+        return fail(CULIPX_INVALID_ARG, "culipx_csr_set_format: bad format %d", format);
+    GUARD_BEGIN
+    CULIPX_TRY(use_device(A->h));
+    if (format == CULIPX_FMT_CSR) {
+        A->sell = Sell();
+        return CULIPX_OK;
+    }
+    return csr_build_sell(A);
+    GUARD_END
+}
+
+CULIPX_API int culipx_csr_refresh(culipx_csr A)
+{
+    if (!A) return fail(CULIPX_INVALID_ARG, "null operator");
+    GUARD_BEGIN
+    CULIPX_TRY(use_device(A->h));
+    return csr_refresh_sell(A, A->h->stream);
+    GUARD_END
 }
 
 CULIPX_API int culipx_spmv(culipx_csr A, const void* d_x, void* d_y, double alpha, double beta, int transpose)

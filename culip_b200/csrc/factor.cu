@@ -70,6 +70,7 @@ struct FactorArgs {
     int* deferred;
     int* slowlist;        // off-diagonal positions left to the tiled kernel
     long long val_slots;  // first arena slot
+    double piv64;         // FP32 factors: 2x2 pivots below this ratio are inverted in FP64
 };
 
 template <class T>
@@ -218,7 +219,7 @@ __global__ void __launch_bounds__(32 * kWarps) k_pivot_blocks(FactorArgs a, T* v
         }
         __syncwarp();
     } else {
-        factorize_tile(Tt, len, a.is_piv + from, tri + 3 * (size_t)from, a.perm + from, method);
+        factorize_tile(Tt, len, a.is_piv + from, tri + 3 * (size_t)from, a.perm + from, method, a.piv64);
     }
     const bool perm_ident = __all_sync(0xffffffffu, lane >= len || a.perm[from + lane] == from + lane);
     const bool no_updates = (q_end == q_beg);
@@ -433,6 +434,13 @@ __device__ void offdiag_tile(const FactorArgs& a, const T* val, const T* tri, in
     const T td11 = fma_rn(gc, d11, gs * d12);
     const T td12 = fma_rn(gc, d12, gs * d22);
     const T td22 = fma_rn(gc, d22, -(gs * d12));
+    // an ill-conditioned 2x2 pivot of an FP32 factor: the same solve in FP64
+    const bool wide = piv2 && wide_2x2(d11, d12, d22, a.piv64);
+    const double wr = sqrt(fma_rn((double)d11, (double)d11, (double)d12 * (double)d12));
+    const double wc = (double)d11 / wr, ws = (double)d12 / wr;
+    const double w11 = fma_rn(wc, (double)d11, ws * (double)d12);
+    const double w12 = fma_rn(wc, (double)d12, ws * (double)d22);
+    const double w22 = fma_rn(wc, (double)d22, -(ws * (double)d12));
     while (colmask) {
         const int j = __ffs(colmask) - 1;
         colmask &= colmask - 1;
@@ -445,10 +453,20 @@ __device__ void offdiag_tile(const FactorArgs& a, const T* val, const T* tri, in
         }
         if (lane >= h) rhs = T(0);
         const T right = shfl(rhs, (lane < 31) ? lane + 1 : 31);
-        T x1 = fma_rn(gc, rhs, gs * right);
-        T x2 = fma_rn(gc, right, -(gs * rhs));
-        x2 = piv2 ? (x2 / td22) : T(0);
-        x1 = fma_rn(-td12, x2, x1) / td11;
+        T x1, x2;
+        if (wide) {
+            double y1 = fma_rn(wc, (double)rhs, ws * (double)right);
+            double y2 = fma_rn(wc, (double)right, -(ws * (double)rhs));
+            y2 = y2 / w22;
+            y1 = fma_rn(-w12, y2, y1) / w11;
+            x1 = T(y1);
+            x2 = T(y2);
+        } else {
+            x1 = fma_rn(gc, rhs, gs * right);
+            x2 = fma_rn(gc, right, -(gs * rhs));
+            x2 = piv2 ? (x2 / td22) : T(0);
+            x1 = fma_rn(-td12, x2, x1) / td11;
+        }
         __syncwarp();
         if (piv1) Tt[lane * kTileStride + j] = x1;
         if (piv2) Tt[(lane + 1) * kTileStride + j] = x2;
@@ -875,6 +893,7 @@ int run_levels(Factor* f, const void* d_vals, cudaStream_t s, int* launches)
     a.deferred = f->deferred.as<int>();
     a.slowlist = f->slowlist.as<int>();
     a.val_slots = p.val_slots;
+    a.piv64 = f->pivot_fp64;
     const int pivoting = (f->pivot != CULIPX_PIV_STATIC);
     const size_t s3 = kWarps * 3 * kTileElems * sizeof(T);
     const T thv = (T)f->threshold;
@@ -1046,7 +1065,8 @@ int factor_compute_graph(Factor* f, const void* d_vals, int pivot, double thresh
     Pattern& p = *f->pat;
     culipx_handle_t* h = p.handle;
     cudaStream_t s = h->stream;
-    if (!f->graph_exec || f->graph_vals != d_vals || f->graph_pivot != pivot || f->graph_threshold != threshold) {
+    if (!f->graph_exec || f->graph_vals != d_vals || f->graph_pivot != pivot || f->graph_threshold != threshold ||
+        f->graph_piv64 != f->pivot_fp64) {
         CULIPX_TRY(factor_compute(f, d_vals, nullptr, pivot, threshold));
         if (f->graph_exec) cudaGraphExecDestroy(f->graph_exec);
         if (f->graph) cudaGraphDestroy(f->graph);
@@ -1084,6 +1104,7 @@ int factor_compute_graph(Factor* f, const void* d_vals, int pivot, double thresh
         f->graph_vals = d_vals;
         f->graph_pivot = pivot;
         f->graph_threshold = threshold;
+        f->graph_piv64 = f->pivot_fp64;
         f->graph_launches = f->last_launches;
         return CULIPX_OK;  // the ordinary run above factored these values
     }

@@ -34,6 +34,7 @@ struct Factor {
     double threshold = 0.0;
     int solve_algorithm = CULIPX_SOLVE_BLOCK;  // set_solve_algorithm
     int jacobi_sweeps = 0;
+    double pivot_fp64 = kPivotFp64Default;     // FP32 factors: FP64 inversion of 2x2 pivots below this ratio
 
     // block storage (pattern layout + relocation arena for blocks that were
     // granted extra slots by dual dropping)
@@ -84,6 +85,7 @@ struct Factor {
     const void* graph_vals = nullptr;
     int graph_pivot = -1;
     double graph_threshold = -1.0;
+    double graph_piv64 = -1.0;
     int graph_launches = 0;
     bool capturing = false;
     cudaStream_t capture_stream = nullptr;

@@ -1,6 +1,8 @@
 // Device helpers shared by the culipx kernels.
 #pragma once
 
+#include "common.h"
+
 #include <cuda_runtime.h>
 #include <cstdint>
 
@@ -17,6 +19,17 @@ __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
 
 template <class T>
 __device__ __forceinline__ T shfl(T v, int src) { return __shfl_sync(0xffffffffu, v, src); }
+
+// true when an FP32 factor inverts this 2x2 pivot in FP64 (kPivotFp64Default);
+// the products of two floats are exact in double, so host and device decide
+// alike
+template <class T>
+__device__ __forceinline__ bool wide_2x2(T d11, T d12, T d22, double bound)
+{
+    if (sizeof(T) != 4) return false;
+    const double p = (double)d11 * (double)d22, q = (double)d12 * (double)d12;
+    return fabs(p - q) < bound * (fabs(p) + q);
+}
 
 // per-block descriptor, mirror of BlockDesc (pattern.h)
 struct DevBlock {

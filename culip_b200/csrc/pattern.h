@@ -41,6 +41,10 @@ struct Pattern {
 
     int num_levels = 0;
     std::vector<int> lvl_off, lvl_rows, row_level;
+    // every level-0 block row's diagonal block of K is diagonal (no entry
+    // between two rows of the same level-0 block row): a level-0 row's K row
+    // then reads only itself and rows of later levels
+    bool l0_diagonal = false;
     std::vector<int> lb_off, lb;  // factor order per level: pivots, then off-diagonal (CSR order)
     // per row position t of lvl_rows: index of the row's first off-diagonal
     // block inside its level's off-diagonal list

@@ -183,8 +183,39 @@ __device__ __forceinline__ void step_1x1(T* Tt, T* D, int row, int len)
     __syncwarp();
 }
 
+// The Givens-form 2x2 solve of d_ldlt_2x2_step (:589-675) with its
+// arithmetic in C: T itself, or double for an ill-conditioned pivot of an FP32
+// factor (wide_2x2); the stored U entries and the Schur update are rounded to
+// T once.  With C = T every operation is the reference's.
+template <class T, class C>
+__device__ __forceinline__ void step_2x2_in(T* Tt, int row, int len, C d11, C d12, C d22)
+{
+    const int l = lane_id();
+    const C a1 = (l < row) ? C(0) : C(Tt[row * kTileStride + l]);
+    const C a2 = (l < row) ? C(0) : ((l == row) ? d12 : C(Tt[(row + 1) * kTileStride + l]));
+    const C gr = sqrt(fma_rn(d11, d11, d12 * d12));
+    const C gc = d11 / gr, gs = d12 / gr;
+    C x1 = fma_rn(gc, a1, gs * a2);
+    C x2 = fma_rn(gc, a2, -(gs * a1));
+    const C td11 = fma_rn(gc, d11, gs * d12);
+    const C td12 = fma_rn(gc, d12, gs * d22);
+    const C td22 = fma_rn(gc, d22, -(gs * d12));
+    x2 = x2 / td22;
+    x1 = fma_rn(-td12, x2, x1) / td11;
+    __syncwarp();
+    Tt[row * kTileStride + l] = (l < row) ? T(0) : T(x1);
+    Tt[(row + 1) * kTileStride + l] = (l < row) ? T(0) : T(x2);
+    const C r1 = fma_rn(x1, d11, x2 * d12);
+    const C r2 = fma_rn(x1, d12, x2 * d22);
+    for (int i = row + 2; i < len; ++i) {
+        const C l1 = shfl(r1, i), l2 = shfl(r2, i);
+        Tt[i * kTileStride + l] = T(C(Tt[i * kTileStride + l]) - fma_rn(l1, x1, l2 * x2));
+    }
+    __syncwarp();
+}
+
 template <class T>
-__device__ __forceinline__ void step_2x2(T* Tt, T* D, int row, int len)
+__device__ __forceinline__ void step_2x2(T* Tt, T* D, int row, int len, double piv64)
 {
     const int l = lane_id();
     T d11 = Tt[row * kTileStride + row];
@@ -192,27 +223,10 @@ __device__ __forceinline__ void step_2x2(T* Tt, T* D, int row, int len)
     T d22 = Tt[(row + 1) * kTileStride + row + 1];
     const bool modified = fabs(fma_rn(d11, d22, -(d12 * d12))) < 1e-8;
     if (modified) { d11 = T(1e-6); d22 = T(1e-6); }
-    const T a1 = (l < row) ? T(0) : Tt[row * kTileStride + l];
-    const T a2 = (l < row) ? T(0) : ((l == row) ? d12 : Tt[(row + 1) * kTileStride + l]);
-    const T gr = sqrt(fma_rn(d11, d11, d12 * d12));
-    const T gc = d11 / gr, gs = d12 / gr;
-    T x1 = fma_rn(gc, a1, gs * a2);
-    T x2 = fma_rn(gc, a2, -(gs * a1));
-    const T td11 = fma_rn(gc, d11, gs * d12);
-    const T td12 = fma_rn(gc, d12, gs * d22);
-    const T td22 = fma_rn(gc, d22, -(gs * d12));
-    x2 = x2 / td22;
-    x1 = fma_rn(-td12, x2, x1) / td11;
-    __syncwarp();
-    Tt[row * kTileStride + l] = (l < row) ? T(0) : x1;
-    Tt[(row + 1) * kTileStride + l] = (l < row) ? T(0) : x2;
-    const T r1 = fma_rn(x1, d11, x2 * d12);
-    const T r2 = fma_rn(x1, d12, x2 * d22);
-    for (int i = row + 2; i < len; ++i) {
-        const T l1 = shfl(r1, i), l2 = shfl(r2, i);
-        Tt[i * kTileStride + l] -= fma_rn(l1, x1, l2 * x2);
-    }
-    __syncwarp();
+    if (wide_2x2(d11, d12, d22, piv64))
+        step_2x2_in<T, double>(Tt, row, len, d11, d12, d22);
+    else
+        step_2x2_in<T, T>(Tt, row, len, d11, d12, d22);
     if (modified && l == 0) {
         Tt[row * kTileStride + row] = T(1);
         Tt[row * kTileStride + row + 1] = T(0);
@@ -226,7 +240,8 @@ __device__ __forceinline__ void step_2x2(T* Tt, T* D, int row, int len)
 }
 
 template <class T>
-__device__ __forceinline__ void factorize_tile(T* Tt, int len, int* is_piv, T* D, int* perm, int method)
+__device__ __forceinline__ void factorize_tile(T* Tt, int len, int* is_piv, T* D, int* perm, int method,
+                                               double piv64)
 {
     const bool use_piv = method != CULIPX_PIV_STATIC;
     int p = 0;
@@ -256,7 +271,7 @@ __device__ __forceinline__ void factorize_tile(T* Tt, int len, int* is_piv, T* D
                 if (p0 != p) pivot_swap(Tt, perm, p, p0, len);
                 pivot_swap(Tt, perm, p + 1, p1, len);
             }
-            step_2x2(Tt, D, p, len);
+            step_2x2(Tt, D, p, len, piv64);
             if (use_piv && lane_id() == 0) { is_piv[p] = 1; is_piv[p + 1] = 0; }
         }
         __syncwarp();

@@ -48,26 +48,27 @@ __global__ void k_to_f32(const double* __restrict__ in, float* __restrict__ out,
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += stride) out[i] = (float)in[i];
 }
 
-// one right-hand side of a refinement round: x += d (if d), r = b - K x, ||r||^2
+// one right-hand side of a refinement round: v += a (if a), r = b - K v, ||r||^2
 struct ResJob {
     const int* rowptr;
     const int* colidx;
     const double* val;
     const double* b;
-    const double* d;
-    double* x;
+    const double* a;
+    double* v;
     double* r;
     long long n;
 };
 
 constexpr int kResT = 256;
+constexpr int kRefinePatience = 2;  // corrections in a row without a smaller residual that stop a right-hand side
 
 __global__ void k_add_corrections(const ResJob* __restrict__ jobs, int num)
 {
     for (int j = blockIdx.x; j < num; j += gridDim.x) {
         const ResJob J = jobs[j];
-        if (J.d)
-            for (long long i = threadIdx.x; i < J.n; i += kResT) J.x[i] += J.d[i];
+        if (J.a)
+            for (long long i = threadIdx.x; i < J.n; i += kResT) J.v[i] += J.a[i];
     }
 }
 
@@ -81,7 +82,7 @@ __global__ void k_residuals(const ResJob* __restrict__ jobs, int num, double* __
         for (long long i = threadIdx.x; i < J.n; i += kResT) {
             double acc = 0.0;
             for (int k = __ldg(J.rowptr + i); k < __ldg(J.rowptr + i + 1); ++k)
-                acc = fma_rn(__ldg(J.val + k), J.x[__ldg(J.colidx + k)], acc);
+                acc = fma_rn(__ldg(J.val + k), J.v[__ldg(J.colidx + k)], acc);
             const double ri = J.b[i] - acc;
             J.r[i] = ri;
             t = fma_rn(ri, ri, t);
@@ -108,7 +109,7 @@ long long request_bytes(const ServerPattern& sp, int nrhs, bool refine)
 {
     const long long n = sp.n;
     long long b = sp.nnz * 8 + 2 * n * nrhs * 8 + (long long)(7 * n + 8) * nrhs * 8 + 4096;
-    if (refine) b += 2 * n * nrhs * 8;
+    if (refine) b += 3 * n * nrhs * 8;
     if (sp.precision == CULIPX_F32) b += sp.nnz * 4;
     return b;
 }
@@ -170,7 +171,8 @@ Server::~Server()
         if (sl.h && sl.h->stream) cudaStreamSynchronize(sl.h->stream);
     }
     for (auto& r : requests)
-        for (void* p : {r.second.d_vals, r.second.d_vals32, r.second.d_b, r.second.d_x, r.second.d_r, r.second.d_d})
+        for (void* p : {r.second.d_vals, r.second.d_vals32, r.second.d_b, r.second.d_x, r.second.d_r, r.second.d_d,
+                        r.second.d_best})
             if (p) cudaFree(p);
     for (auto& sp : patterns) {
         for (Factor* f : sp.free_factors) delete static_cast<culipx_factor_t*>(f);
@@ -296,7 +298,10 @@ int finish_slot(Server* s, ServerSlot& sl)
         if (s->max_refine > 0 && (int)r.its_acc.size() == r.nrhs) {
             for (int c = 0; c < r.nrhs; ++c) {
                 r.its[c] = r.its_acc[c];
-                r.status[c] = r.broke[c] ? CULIPX_BREAKDOWN : (r.rel[c] <= s->tol ? CULIPX_OK : CULIPX_MAXIT);
+                r.status[c] = r.broke[c]           ? CULIPX_BREAKDOWN
+                              : r.rel[c] <= s->tol ? CULIPX_OK
+                              : r.stalled[c]       ? CULIPX_STALLED
+                                                   : CULIPX_MAXIT;
             }
         } else {
             many_results(r.nrhs, s->max_it, sl.out_host + (size_t)k * 8, nullptr, r.its.data(), r.status.data());
@@ -330,9 +335,11 @@ int enqueue_end(Server* s, ServerSlot& sl)
     for (int id : sl.reqs) {
         ServerRequest& r = s->requests.at(id);
         const size_t nb = (size_t)s->patterns[r.pid].n * r.nrhs;
-        CULIPX_CUDA(cudaMemcpyAsync(sl.x_host + xo, r.d_x, nb * sizeof(double), cudaMemcpyDeviceToHost, st));
+        // refined requests return their best iterates
+        const void* src = r.d_best ? r.d_best : r.d_x;
+        CULIPX_CUDA(cudaMemcpyAsync(sl.x_host + xo, src, nb * sizeof(double), cudaMemcpyDeviceToHost, st));
         xo += nb;
-        for (void** p : {&r.d_vals, &r.d_vals32, &r.d_b, &r.d_x, &r.d_r, &r.d_d})
+        for (void** p : {&r.d_vals, &r.d_vals32, &r.d_b, &r.d_x, &r.d_r, &r.d_d, &r.d_best})
             if (*p) {
                 CULIPX_CUDA(cudaFreeAsync(*p, st));
                 *p = nullptr;
@@ -382,21 +389,35 @@ int enqueue_residuals(Server* s, ServerSlot& sl, bool add)
 }
 
 // A refinement round finished: take the last solves' iterations and the new
-// residuals; right-hand sides still above tol (and below max_refine
-// corrections, without breakdown) get a correction d = SQMR(K, M, r,
-// inner_tol), then x += d and new residuals; otherwise the batch ends.
+// residuals (the first round's is the plain solve's).  An iterate with the
+// smallest residual so far is copied to best; kRefinePatience corrections in
+// a row without a new smallest residual stop the right-hand side (stalled).
+// Right-hand sides still above tol (and below max_refine corrections, not
+// stalled, without breakdown) get a correction d = SQMR(K, M, r, inner_tol),
+// x += d and a new residual; otherwise the batch ends, returning the best
+// iterates.
 int refine_step(Server* s, ServerSlot& sl)
 {
     std::vector<std::pair<int, int>> next;
     for (size_t i = 0; i < sl.cols.size(); ++i) {
         ServerRequest& r = s->requests.at(sl.cols[i].first);
         const int c = sl.cols[i].second;
+        const size_t n = s->patterns[r.pid].n;
         const double* o = sl.out_host + 8 * i;
         r.its_acc[c] += (int)o[1];
         if (o[2] != 0.0) r.broke[c] = 1;
-        r.rel[c] = r.bnorm[c] > 0.0 ? std::sqrt(sl.res_host[i]) / r.bnorm[c] : 0.0;
-        if (!std::isfinite(r.rel[c])) r.broke[c] = 1;
-        if (!r.broke[c] && r.rel[c] > s->tol && r.steps[c] < s->max_refine) next.push_back(sl.cols[i]);
+        const double rel = r.bnorm[c] > 0.0 ? std::sqrt(sl.res_host[i]) / r.bnorm[c] : 0.0;
+        if (!std::isfinite(rel)) r.broke[c] = 1;
+        if (r.steps[c] == 0 || (!r.broke[c] && rel < r.rel[c])) {
+            r.rel[c] = rel;
+            r.fails[c] = 0;
+            CULIPX_CUDA(cudaMemcpyAsync(static_cast<double*>(r.d_best) + c * n, static_cast<double*>(r.d_x) + c * n,
+                                        n * sizeof(double), cudaMemcpyDeviceToDevice, sl.h->stream));
+        } else if (!r.broke[c] && ++r.fails[c] >= kRefinePatience) {
+            r.stalled[c] = 1;
+        }
+        if (!r.broke[c] && !r.stalled[c] && r.rel[c] > s->tol && r.steps[c] < s->max_refine)
+            next.push_back(sl.cols[i]);
     }
     if (next.empty()) {
         sl.phase = 0;
@@ -510,6 +531,7 @@ int launch_slot(Server* s, ServerSlot& sl)
         if (s->max_refine > 0) {
             CULIPX_CUDA(cudaMallocAsync(&r.d_r, nb * sizeof(double), st));
             CULIPX_CUDA(cudaMallocAsync(&r.d_d, nb * sizeof(double), st));
+            CULIPX_CUDA(cudaMallocAsync(&r.d_best, nb * sizeof(double), st));
             r.bnorm.assign(r.nrhs, 0.0);
             for (int c = 0; c < r.nrhs; ++c) {
                 double t = 0.0;
@@ -520,6 +542,8 @@ int launch_slot(Server* s, ServerSlot& sl)
             r.steps.assign(r.nrhs, 0);
             r.its_acc.assign(r.nrhs, 0);
             r.broke.assign(r.nrhs, 0);
+            r.stalled.assign(r.nrhs, 0);
+            r.fails.assign(r.nrhs, 0);
         }
         r.q = (int)(sl.csrs.size());
         CULIPX_CUDA(cudaMemcpyAsync(r.d_vals, r.vals.data(), nv * sizeof(double), cudaMemcpyHostToDevice, st));

@@ -35,14 +35,15 @@ struct ServerRequest {
     long long bytes = 0;                   // device bytes while running
     Factor* F = nullptr;
     void *d_vals = nullptr, *d_vals32 = nullptr, *d_b = nullptr, *d_x = nullptr;
-    // FP64 refinement (Server::max_refine > 0): residuals, corrections, and
-    // per right-hand side ||b||, the last relative residual, corrections taken,
-    // SQMR iterations summed, breakdown seen
-    void *d_r = nullptr, *d_d = nullptr;
+    // FP64 refinement (Server::max_refine > 0): residuals, corrections, best
+    // iterates, and per right-hand side ||b||, the smallest relative residual,
+    // corrections computed, corrections in a row without a smaller residual,
+    // SQMR iterations summed, breakdown seen, stalled
+    void *d_r = nullptr, *d_d = nullptr, *d_best = nullptr;
     int q = -1;                            // position in the running batch
     std::vector<double> bnorm, rel;
-    std::vector<int> steps, its_acc;
-    std::vector<char> broke;
+    std::vector<int> steps, fails, its_acc;
+    std::vector<char> broke, stalled;
 };
 
 struct ServerSlot {

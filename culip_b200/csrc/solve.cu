@@ -585,9 +585,25 @@ __global__ void __launch_bounds__(32 * kSweepWarps)
     if (lane < h) x_out[fr + lane] = acc;
 }
 
-// k_solve_D: Givens-based 1x1 / 2x2 block-diagonal solve (out may equal in)
+// the Givens-form solve of one 1x1 / 2x2 pivot in C
+template <class C>
+__device__ __forceinline__ void givens_solve(C p11, C p12, C p22, C r1, C r2, C& g1, C& g2)
+{
+    const C gr = sqrt(fma_rn(p11, p11, p12 * p12));
+    const C gc = p11 / gr, gs = p12 / gr;
+    g1 = fma_rn(gc, r1, gs * r2);
+    g2 = fma_rn(gc, r2, -(gs * r1));
+    const C tp12 = fma_rn(gc, p12, gs * p22);
+    const C tp22 = fma_rn(gc, p22, -(gs * p12));
+    g2 = g2 / tp22;
+    g1 = fma_rn(-tp12, g2, g1) / gr;
+}
+
+// k_solve_D: Givens-based 1x1 / 2x2 block-diagonal solve (out may equal in);
+// an FP32 factor's ill-conditioned 2x2 pivots (wide_2x2) are solved in FP64
 template <class T>
-__global__ void k_solve_D(const T* __restrict__ tri, const int* __restrict__ is_piv, const T* in, T* out, int n)
+__global__ void k_solve_D(const T* __restrict__ tri, const int* __restrict__ is_piv, const T* in, T* out, int n,
+                          double piv64)
 {
     for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < n; g += gridDim.x * blockDim.x) {
         const int this_piv = is_piv[g];
@@ -595,14 +611,15 @@ __global__ void k_solve_D(const T* __restrict__ tri, const int* __restrict__ is_
         const T p11 = tri[3 * (size_t)g + 1], p12 = tri[3 * (size_t)g + 2];
         const T p22 = !next_piv ? tri[3 * (size_t)(g + 1) + 1] : T(1);
         const T r1 = in[g], r2 = (g < n - 1) ? in[g + 1] : T(0);
-        const T gr = sqrt(fma_rn(p11, p11, p12 * p12));
-        const T gc = p11 / gr, gs = p12 / gr;
-        T g1 = fma_rn(gc, r1, gs * r2);
-        T g2 = fma_rn(gc, r2, -(gs * r1));
-        const T tp12 = fma_rn(gc, p12, gs * p22);
-        const T tp22 = fma_rn(gc, p22, -(gs * p12));
-        g2 = g2 / tp22;
-        g1 = fma_rn(-tp12, g2, g1) / gr;
+        T g1, g2;
+        if (!next_piv && wide_2x2(p11, p12, p22, piv64)) {
+            double w1, w2;
+            givens_solve<double>(p11, p12, p22, r1, r2, w1, w2);
+            g1 = T(w1);
+            g2 = T(w2);
+        } else {
+            givens_solve<T>(p11, p12, p22, r1, r2, g1, g2);
+        }
         if (this_piv) out[g] = g1;
         if (!next_piv) out[g + 1] = g2;
     }
@@ -679,7 +696,7 @@ int apply_t(Factor* f, int stage, const void* d_b, void* d_x, cudaStream_t s)
     T* x = static_cast<T*>(d_x);
     const int grid_n = (n + 255) / 256 < 148 * 8 ? (n + 255) / 256 : 148 * 8;
     if (stage == CULIPX_MIDDLE) {
-        k_solve_D<T><<<grid_n, 256, 0, s>>>(f->tri.as<T>(), f->is_piv.as<int>(), b, x, n);
+        k_solve_D<T><<<grid_n, 256, 0, s>>>(f->tri.as<T>(), f->is_piv.as<int>(), b, x, n, f->pivot_fp64);
         return launch_check("k_solve_D");
     }
     const T* fval = f->val.as<T>();

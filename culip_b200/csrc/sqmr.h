@@ -18,6 +18,7 @@ struct Sqmr {
     DeviceBuffer ts;                  // 64 iterations x 8 phase stamps (ns, %globaltimer)
     DeviceBuffer vecs, partials, scal;
     DeviceBuffer ref_r, ref_d, ref_part;  // iterative refinement: residual, correction, norm partials
+    DeviceBuffer ref_best;                // its best iterate so far
     DeviceBuffer many;                    // sqmr_solve_many: vectors, argument blocks, counter
     void* host_flags = nullptr;  // pinned
     ~Sqmr()

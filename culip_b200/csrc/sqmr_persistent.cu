@@ -78,6 +78,7 @@ constexpr unsigned kFull = 0xffffffffu;
 template <class TF>
 struct PArgs {
     int n, nl, max_it;
+    int fuse_l0;               // level-0 simple rows compute (K ev) in the U sweep
     double tol;
     const int* rowptr;
     const int* colidx;
@@ -1414,6 +1415,7 @@ PArgs<TF> make_args(Csr* A, Factor* M, double* base, double* partials, const dou
     a.n = n;
     a.nl = p.num_levels;
     a.max_it = max_it;
+    a.fuse_l0 = (p.l0_diagonal && A->nnz == p.nnz && A->m == p.n) ? 1 : 0;
     a.tol = tol;
     a.rowptr = A->rowptr;
     a.colidx = A->colidx;

@@ -219,6 +219,13 @@ int analyze_pattern(culipx_handle_t* h, int n, const int* rowptr, const int* col
     }
     p.num_levels = 0;
     for (int c = 0; c < cm; ++c) p.num_levels = std::max(p.num_levels, p.row_level[c] + 1);
+    p.l0_diagonal = true;
+    for (int c = 0; c < cm && p.l0_diagonal; ++c) {
+        if (p.row_level[c] != 0) continue;
+        for (int i = p.bs[c]; i < p.bs[c + 1]; ++i)
+            for (int q = rowptr[i]; q < rowptr[i + 1]; ++q)
+                if (colidx[q] != i && p.row_block[colidx[q]] == c) p.l0_diagonal = false;
+    }
     const int nl = p.num_levels;
     p.lvl_off.assign(nl + 1, 0);
     for (int c = 0; c < cm; ++c) p.lvl_off[p.row_level[c] + 1]++;

@@ -38,6 +38,8 @@ extern "C" {
 #define CULIPX_CUDA_ERROR    6
 #define CULIPX_NOT_SUPPORTED 7
 #define CULIPX_PENDING       8  /* a server request has not finished yet */
+#define CULIPX_STALLED       9  /* refinement: corrections stopped lowering the
+                                   true residual; x is the best iterate reached */
 
 /* ---- value precision (the reference's T = double / float) ---- */
 #define CULIPX_F64 0
@@ -202,6 +204,16 @@ int culipx_factor_info(culipx_factor f, long long *info8);
  * culipx_sqmr_solve follow it; SQMR with JACOBI needs an FP64 factor. */
 int culipx_factor_set_solve_algorithm(culipx_factor f, int algorithm, int sweeps);
 
+/* FP32 factors (no counterpart in the reference, whose float factor inverts
+ * every pivot in float): a 2x2 pivot whose ratio
+ * |d11 d22 - d12^2| / (|d11 d22| + d12^2) is below bound is inverted in FP64,
+ * in the pivot-tile step (d_ldlt_2x2_step), the off-diagonal solve
+ * (d_left_solve_with_D_Ut) and the D apply (k_solve_D); results are rounded
+ * to FP32 once.  Default 1e-3; 0 keeps the reference's FP32 arithmetic.
+ * Bunch-Kaufman and rook pivots have a ratio above 0.42, so the bound acts on
+ * given (static) pivots.  No effect on FP64 factors; the next compute uses it. */
+int culipx_factor_set_pivot_fp64(culipx_factor f, double bound);
+
 /* Preconditioner applies; b and x are device vectors of n values in the
  * factor's precision (b == x allowed for MIDDLE). */
 int culipx_prec_apply(culipx_factor f, int stage, const void *d_b, void *d_x);
@@ -241,6 +253,19 @@ int culipx_csr_create(culipx_handle h, int m, int n, long long nnz, const int *d
 int culipx_csr_destroy(culipx_csr A);
 /* y = alpha op(A) x + beta y (beta == 0: y is not read) */
 int culipx_spmv(culipx_csr A, const void *d_x, void *d_y, double alpha, double beta, int transpose);
+/* Storage the non-transposed product reads (no counterpart in the
+ * reference, which hands the CSR arrays to cuSPARSE each call).
+ * CULIPX_FMT_CSR (default): the borrowed arrays.  CULIPX_FMT_SELL: a
+ * SELL-32-sigma copy built now (rows of up to 64 entries in slices of 32,
+ * sorted by length inside windows of 256 rows, entry j of a slice's rows
+ * contiguous), so a warp's index and value loads coalesce; every row is
+ * still summed serially in column order, so y is bit for bit the CSR
+ * kernel's.  The copy holds the values of the time it was built: after
+ * changing d_val call culipx_csr_refresh (one gather on the stream). */
+#define CULIPX_FMT_CSR  0
+#define CULIPX_FMT_SELL 1
+int culipx_csr_set_format(culipx_csr A, int format);
+int culipx_csr_refresh(culipx_csr A);
 
 /* ------------------------------------------------------------------------ */
 /* Vector operations on device vectors of n values in `precision`, on the
@@ -303,7 +328,8 @@ int culipx_sqmr_solve_multi(culipx_handle h, culipx_csr A, culipx_factor M, int 
  * stopping test; every step solves the corrections of the right-hand sides
  * still above tol together (culipx_sqmr_solve_multi).  Per right-hand side:
  * relres = ||b - K x|| / ||b||, SQMR iterations summed, corrections, status
- * (OK, MAXIT, BREAKDOWN); any output array may be NULL. */
+ * (OK, MAXIT, STALLED, BREAKDOWN), each as culipx_sqmr_refine defines them;
+ * any output array may be NULL. */
 int culipx_sqmr_refine_multi(culipx_handle h, culipx_csr A, culipx_factor M, int nrhs, const double *d_B,
                              double *d_X, double tol, double inner_tol, int inner_max_it, int max_refine,
                              double *h_relres, int *h_iterations, int *h_steps, int *h_status);
@@ -419,10 +445,13 @@ int culipx_tune_kkt_block(culipx_handle h, int n, int m, const int *h_rowptr, co
 /* FP64 iterative refinement of every request (the mixed-precision serving
  * path, meant for FP32 patterns; no counterpart in the reference): after the
  * solve, r = b - K x in FP64 per right-hand side; while ||r|| > tol ||b|| and
- * fewer than max_refine corrections: d = SQMR(K, M, r, inner_tol), x += d, new
- * r.  Corrections of a batch's right-hand sides run together.  Then the
+ * fewer than max_refine corrections: d = SQMR(K, M, r, inner_tol), x += d,
+ * new r; two corrections in a row without a new smallest ||r|| stop the
+ * right-hand side (STALLED).  Corrections of a batch's right-hand sides run
+ * together.  Every right-hand side returns its iterate of smallest ||r||, the
  * request's iterations are the SQMR iterations summed and its status OK when
- * ||b - K x|| <= tol ||b||, else MAXIT (BREAKDOWN if a solve broke down).
+ * ||b - K x|| <= tol ||b||, else STALLED or MAXIT (BREAKDOWN if a solve broke
+ * down).
  * max_refine 0 (the default) turns it off; applies to batches admitted
  * afterwards. */
 int culipx_server_set_refine(culipx_server s, int max_refine, double inner_tol);
@@ -432,7 +461,8 @@ int culipx_server_launch_count(culipx_server s, long long *count);
 /* culipx_sqmr_refine per system of a batch: every step solves all systems
  * still above tol in one batched launch (the others get a zero right-hand
  * side); per system the true relative residual, the SQMR iterations summed,
- * the corrections taken and a status (OK, MAXIT, BREAKDOWN). */
+ * the corrections computed and a status (OK, MAXIT, STALLED, BREAKDOWN), as
+ * culipx_sqmr_refine defines them. */
 int culipx_batch_sqmr_refine(culipx_batch b, culipx_csr A, culipx_factor M, const double *d_b, double *d_x,
                              double tol, double inner_tol, int inner_max_it, int max_refine, double *h_relres,
                              int *h_iterations, int *h_steps, int *h_status);
@@ -442,8 +472,12 @@ int culipx_batch_sqmr_refine(culipx_batch b, culipx_csr A, culipx_factor M, cons
  * ||r|| > tol ||b|| and fewer than max_refine corrections: d = SQMR(K, M, r,
  * inner_tol, inner_max_it), x += d, r = b - K x (FP64).  With an FP32 factor
  * the preconditioner applies are single precision and everything else FP64.
- * relres = ||b - K x|| / ||b||, iterations = SQMR iterations summed, steps =
- * corrections.  Returns CULIPX_MAXIT if tol was not reached. */
+ * The iterate of smallest ||r|| is kept and returned; two corrections in a
+ * row that do not lower it end the loop with CULIPX_STALLED (the inner solves
+ * no longer help: raise inner_max_it or use an FP64 factor).  relres =
+ * ||b - K x|| / ||b|| of the returned x, iterations = SQMR iterations summed,
+ * steps = corrections computed.  Returns CULIPX_MAXIT if tol was not reached
+ * in max_refine corrections. */
 int culipx_sqmr_refine(culipx_handle h, culipx_csr A, culipx_factor M, const double *d_b, double *d_x,
                        double tol, double inner_tol, int inner_max_it, int max_refine, double *relres,
                        int *iterations, int *steps);

@@ -14,6 +14,9 @@ import numpy as np
 
 from . import build as _build
 
+# the FP32 factor's FP64 2x2-pivot bound (ORC_PIVOT_FP64_DEFAULT)
+PIVOT_FP64_DEFAULT = 1e-3
+
 _lib = None
 
 _i32p = ctypes.POINTER(ctypes.c_int)
@@ -51,7 +54,7 @@ def lib():
             f.argtypes = [vp, vp, vp, ctypes.c_int, real, ctypes.c_int]
             ff = getattr(L, "orc_factor_forced" + sfx)
             ff.restype = vp
-            ff.argtypes = [vp, vp, vp, ctypes.c_int, real, ctypes.c_int, vp]
+            ff.argtypes = [vp, vp, vp, ctypes.c_int, real, ctypes.c_int, vp, ctypes.c_double]
             getattr(L, "orc_fac_free" + sfx).argtypes = [vp]
             g = getattr(L, "orc_fac_export_size" + sfx)
             g.restype = ctypes.c_long
@@ -133,30 +136,33 @@ class Sym:
             _lib.orc_sym_free(ctypes.cast(h, ctypes.c_void_p))
             self._h = None
 
-    def factor(self, vals, is_piv=None, pivot=1, threshold=0.0, literal=False, forced_grants=None) -> "Fac":
+    def factor(self, vals, is_piv=None, pivot=1, threshold=0.0, literal=False, forced_grants=None,
+               pivot_fp64=PIVOT_FP64_DEFAULT) -> "Fac":
         """forced_grants: per block (block-id order) the extra slots a block
-        that outgrows its capacity receives, as another run decided them."""
-        return Fac(self, vals, is_piv, pivot, threshold, literal, forced_grants)
+        that outgrows its capacity receives, as another run decided them.
+        pivot_fp64: a float factor inverts 2x2 pivots whose ratio
+        |d11 d22 - d12^2| / (|d11 d22| + d12^2) is below it in FP64 (0: float
+        throughout, the reference's arithmetic)."""
+        return Fac(self, vals, is_piv, pivot, threshold, literal, forced_grants, pivot_fp64)
 
 
 class Fac:
     """Numeric factor (BlockiLDLt::factorize) and its applies."""
 
-    def __init__(self, sym: Sym, vals, is_piv, pivot, threshold, literal, forced_grants=None):
+    def __init__(self, sym: Sym, vals, is_piv, pivot, threshold, literal, forced_grants=None,
+                 pivot_fp64=None):
         self.sym = sym
         self.sfx = "_d" if sym.dtype == np.float64 else "_s"
         self.vals = np.ascontiguousarray(vals, dtype=sym.dtype)
         ip = np.ones(sym.n, np.int32) if is_piv is None else np.ascontiguousarray(is_piv, dtype=np.int32)
-        if forced_grants is None:
-            f = getattr(lib(), "orc_factor" + self.sfx)
-            self._h = f(ctypes.cast(sym._h, ctypes.c_void_p), _p(self.vals), _p(ip), int(pivot), float(threshold),
-                        1 if literal else 0)
-        else:
+        self._forced = None
+        if forced_grants is not None:
             self._forced = np.ascontiguousarray(forced_grants, dtype=np.int32)
             assert len(self._forced) == sym.coarse_nnz
-            f = getattr(lib(), "orc_factor_forced" + self.sfx)
-            self._h = f(ctypes.cast(sym._h, ctypes.c_void_p), _p(self.vals), _p(ip), int(pivot), float(threshold),
-                        1 if literal else 0, _p(self._forced))
+        piv64 = PIVOT_FP64_DEFAULT if pivot_fp64 is None else float(pivot_fp64)
+        f = getattr(lib(), "orc_factor_forced" + self.sfx)
+        self._h = f(ctypes.cast(sym._h, ctypes.c_void_p), _p(self.vals), _p(ip), int(pivot), float(threshold),
+                    1 if literal else 0, None if self._forced is None else _p(self._forced), piv64)
 
     def __del__(self):
         h = getattr(self, "_h", None)

@@ -46,11 +46,16 @@ orc_fac_d *orc_factor_d(const orc_sym *s, const double *vals, const int *is_piv_
                         int pivot, double threshold, int literal);
 orc_fac_s *orc_factor_s(const orc_sym *s, const float *vals, const int *is_piv_init,
                         int pivot, float threshold, int literal);
-/* the same with each outgrowing block's extra slots given (coarse_nnz ints) */
+/* the same with each outgrowing block's extra slots given (coarse_nnz ints,
+ * or NULL for the pool) and the FP32 factor's FP64 2x2-pivot bound (the
+ * plain entry points use ORC_PIVOT_FP64_DEFAULT; 0 = float throughout) */
+#define ORC_PIVOT_FP64_DEFAULT 1e-3
 orc_fac_d *orc_factor_forced_d(const orc_sym *s, const double *vals, const int *is_piv_init,
-                               int pivot, double threshold, int literal, const int *forced_grants);
+                               int pivot, double threshold, int literal, const int *forced_grants,
+                               double piv64);
 orc_fac_s *orc_factor_forced_s(const orc_sym *s, const float *vals, const int *is_piv_init,
-                               int pivot, float threshold, int literal, const int *forced_grants);
+                               int pivot, float threshold, int literal, const int *forced_grants,
+                               double piv64);
 void orc_fac_free_d(orc_fac_d *f);
 void orc_fac_free_s(orc_fac_s *f);
 

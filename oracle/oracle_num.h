@@ -55,6 +55,20 @@
 
 #define NZ_EPS 1e-10
 
+/* An FP32 factor inverts a 2x2 pivot in FP64 when
+ * |d11 d22 - d12^2| < bound (|d11 d22| + d12^2) (the library's
+ * kPivotFp64Default rule; not in the reference, whose float factor inverts
+ * every pivot in float).  The products of two floats are exact in double. */
+#ifndef ORC_WIDE_2X2
+#define ORC_WIDE_2X2
+static int orc_wide_2x2(int is_float, double d11, double d12, double d22, double bound)
+{
+    if (!is_float) return 0;
+    const double p = d11 * d22, q = d12 * d12;
+    return fabs(p - q) < bound * (fabs(p) + q);
+}
+#endif
+
 /* per fine row: (global col, value) lists of the strictly off-diagonal
  * block part of U, and of U' (its columns), sorted by column */
 typedef struct {
@@ -75,6 +89,7 @@ typedef struct CAT(orc_fac, SUFFIX) {
     int *is_piv, *perm;
     REAL *row_norm;
     const int *forced_grants; /* per block: grants taken from another run, or NULL */
+    double piv64;             /* FP32: 2x2 pivots below this ratio inverted in FP64 */
     long leftover;        /* pool the blocks of the current level draw from */
 } F(fac_t);
 
@@ -169,12 +184,45 @@ static void F(step_1x1)(REAL T[32][32], REAL *D, int row, int len)
 }
 
 /* d_ldlt_2x2_step (Givens-based 2x2 solve) */
-static void F(step_2x2)(REAL T[32][32], REAL *D, int row, int len)
+static void F(step_2x2)(REAL T[32][32], REAL *D, int row, int len, double piv64)
 {
     int modified = 0;
     REAL d11 = T[row][row], d12 = T[row][row + 1], d22 = T[row + 1][row + 1];
     if (FABS(FMA(d11, d22, -(d12 * d12))) < 1e-8) {
         d11 = (REAL)1e-6; d22 = (REAL)1e-6; modified = 1;
+    }
+    if (orc_wide_2x2(sizeof(REAL) == 4, d11, d12, d22, piv64)) {
+        /* the same steps in double, each result rounded to REAL once */
+        const double e11 = d11, e12 = d12, e22 = d22;
+        const double gr = sqrt(fma(e11, e11, e12 * e12));
+        const double gc = e11 / gr, gs = e12 / gr;
+        const double td11 = fma(gc, e11, gs * e12);
+        const double td12 = fma(gc, e12, gs * e22);
+        const double td22 = fma(gc, e22, -(gs * e12));
+        double u1[32], u2[32], r1[32], r2[32];
+        for (int l = 0; l < 32; ++l) {
+            const double a1 = (l < row) ? 0.0 : (double)T[row][l];
+            const double a2 = (l < row) ? 0.0 : ((l == row) ? e12 : (double)T[row + 1][l]);
+            double x1 = fma(gc, a1, gs * a2);
+            double x2 = fma(gc, a2, -(gs * a1));
+            x2 = x2 / td22;
+            x1 = fma(-td12, x2, x1) / td11;
+            u1[l] = x1; u2[l] = x2;
+        }
+        for (int l = 0; l < 32; ++l) {
+            T[row][l] = (l < row) ? (REAL)0 : (REAL)u1[l];
+            T[row + 1][l] = (l < row) ? (REAL)0 : (REAL)u2[l];
+            r1[l] = fma(u1[l], e11, u2[l] * e12);
+            r2[l] = fma(u1[l], e12, u2[l] * e22);
+        }
+        for (int i = row + 2; i < len; ++i) {
+            const double l1 = r1[i], l2 = r2[i];
+            for (int l = 0; l < 32; ++l) T[i][l] = (REAL)((double)T[i][l] - fma(l1, u1[l], l2 * u2[l]));
+        }
+        if (modified) { T[row][row] = 1; T[row][row + 1] = 0; T[row + 1][row + 1] = 1; }
+        D[3 * row] = 0; D[3 * row + 1] = d11; D[3 * row + 2] = d12;
+        D[3 * (row + 1)] = d12; D[3 * (row + 1) + 1] = d22; D[3 * (row + 1) + 2] = 0;
+        return;
     }
     const REAL gr = SQRT(FMA(d11, d11, d12 * d12));
     const REAL gc = d11 / gr, gs = d12 / gr;
@@ -288,7 +336,8 @@ static void F(select_rook)(REAL T[32][32], int p, int len, int *order, int *p0, 
 }
 
 /* d_factor_pivot_factorize */
-static void F(factorize_tile)(REAL T[32][32], int len, int *is_piv, REAL *D, int *perm, int method)
+static void F(factorize_tile)(REAL T[32][32], int len, int *is_piv, REAL *D, int *perm, int method,
+                              double piv64)
 {
     const int use_piv = (method != ORC_PIV_STATIC);
     int p = 0;
@@ -306,7 +355,7 @@ static void F(factorize_tile)(REAL T[32][32], int len, int *is_piv, REAL *D, int
                 if (p0 != p) F(pivot_swap)(T, perm, p, p0, len);
                 F(pivot_swap)(T, perm, p + 1, p1, len);
             }
-            F(step_2x2)(T, D, p, len);
+            F(step_2x2)(T, D, p, len, piv64);
             if (use_piv) { is_piv[p] = 1; is_piv[p + 1] = 0; }
         }
         p += order;
@@ -316,7 +365,7 @@ static void F(factorize_tile)(REAL T[32][32], int len, int *is_piv, REAL *D, int
 /* d_left_solve_with_D_Ut: A <- D^-1 U^-T A for an h x w block; U is the
  * factored pivot tile (row-major, unit upper with stored diagonal). */
 static void F(left_solve_D_Ut)(REAL U[32][32], const REAL *D, REAL A[32][32],
-                               const int *is_piv, int h, int w, int literal)
+                               const int *is_piv, int h, int w, int literal, double piv64)
 {
     /* an identity pivot tile makes the substitution a sequence of exact
      * no-ops (divide by 1, subtract 0 * x); an all-zero column stays zero */
@@ -349,6 +398,20 @@ static void F(left_solve_D_Ut)(REAL U[32][32], const REAL *D, REAL A[32][32],
             if (l == h) d22 = 0;
             const int two = (l + 1) < h && !is_piv[l + 1];
             if (l >= h) { x1v[l] = 0; x2v[l] = 0; continue; }
+            if (two && orc_wide_2x2(sizeof(REAL) == 4, d11, d12, d22, piv64)) {
+                const double e11 = d11, e12 = d12, e22 = d22;
+                const double wr = sqrt(fma(e11, e11, e12 * e12));
+                const double wc = e11 / wr, ws = e12 / wr;
+                double y1 = fma(wc, (double)rhs[l], ws * (double)right);
+                double y2 = fma(wc, (double)right, -(ws * (double)rhs[l]));
+                const double w11 = fma(wc, e11, ws * e12);
+                const double w12 = fma(wc, e12, ws * e22);
+                const double w22 = fma(wc, e22, -(ws * e12));
+                y2 = y2 / w22;
+                y1 = fma(-w12, y2, y1) / w11;
+                x1v[l] = (REAL)y1; x2v[l] = (REAL)y2;
+                continue;
+            }
             const REAL gr = SQRT(FMA(d11, d11, d12 * d12));
             const REAL gc = d11 / gr, gs = d12 / gr;
             REAL x1 = FMA(gc, rhs[l], gs * right);
@@ -445,19 +508,20 @@ typedef struct {
 F(fac_t) *F(orc_factor)(const orc_sym *s, const REAL *vals, const int *is_piv_init,
                         int pivot, REAL threshold, int literal)
 {
-    return F(orc_factor_forced)(s, vals, is_piv_init, pivot, threshold, literal, NULL);
+    return F(orc_factor_forced)(s, vals, is_piv_init, pivot, threshold, literal, NULL, ORC_PIVOT_FP64_DEFAULT);
 }
 
 /* forced_grants (coarse_nnz entries, or NULL): the extra slots each block that
  * outgrows its capacity receives, taken from another run (the reference's
  * own grants race between a level's CTAs); NULL follows the pool */
 F(fac_t) *F(orc_factor_forced)(const orc_sym *s, const REAL *vals, const int *is_piv_init,
-                               int pivot, REAL threshold, int literal, const int *forced_grants)
+                               int pivot, REAL threshold, int literal, const int *forced_grants, double piv64)
 {
     F(fac_t) *f = (F(fac_t) *)calloc(1, sizeof(F(fac_t)));
     const int n = s->n, cnz = s->coarse_nnz;
     f->s = s; f->pivot = pivot; f->threshold = threshold; f->literal = literal;
     f->forced_grants = forced_grants;
+    f->piv64 = piv64;
     f->nnz = (int *)calloc(cnz, sizeof(int));
     f->maxnnz = (int *)malloc(sizeof(int) * cnz);
     f->got_extra = (int *)calloc(cnz, sizeof(int));
@@ -520,7 +584,8 @@ F(fac_t) *F(orc_factor_forced)(const orc_sym *s, const REAL *vals, const int *is
                 F(mult_tridiag)(Lt, f->tri + 3 * (size_t)s->bs[K], len, bw);
                 F(left_right_update)(f, T, Lt, R, len, bw, len);
             }
-            F(factorize_tile)(T, len, f->is_piv + from, f->tri + 3 * (size_t)from, f->perm + from, pivot);
+            F(factorize_tile)(T, len, f->is_piv + from, f->tri + 3 * (size_t)from, f->perm + from, pivot,
+                              f->piv64);
             for (int l = 0; l < len; ++l) {
                 REAL rs = 0;
                 for (int j = 0; j < len; ++j) rs = FMA(T[l][j], T[l][j], rs);
@@ -591,7 +656,8 @@ F(fac_t) *F(orc_factor_forced)(const orc_sym *s, const REAL *vals, const int *is
                         for (int l = 0; l < 32; ++l) A[i][l] = tmp[pi][l];
                     }
                 }
-                F(left_solve_D_Ut)(U, f->tri + 3 * (size_t)from, A, f->is_piv + from, h, w, f->literal);
+                F(left_solve_D_Ut)(U, f->tri + 3 * (size_t)from, A, f->is_piv + from, h, w, f->literal,
+                                   f->piv64);
                 if (f->threshold > 0 || f->literal)
                     for (int l = 0; l < h; ++l) {
                         REAL rs = 0;
@@ -853,7 +919,7 @@ static void F(solve_Ut)(const F(fac_t) *f, const F(rowlist_t) *Ut, REAL *x)
 }
 
 /* k_solve_D (Givens-based 1x1 / 2x2 block-diagonal solve), from a copy */
-static void F(solve_D)(int n, const REAL *tri, const int *is_piv, const REAL *in, REAL *out)
+static void F(solve_D)(int n, const REAL *tri, const int *is_piv, const REAL *in, REAL *out, double piv64)
 {
     /* every out entry is written by one g only, from the copy in */
 #pragma omp parallel for schedule(static) if (n > 16384)
@@ -863,6 +929,20 @@ static void F(solve_D)(int n, const REAL *tri, const int *is_piv, const REAL *in
         const REAL p11 = tri[3 * g + 1], p12 = tri[3 * g + 2];
         const REAL p22 = !next_piv ? tri[3 * (g + 1) + 1] : (REAL)1;
         const REAL r1 = in[g], r2 = (g < n - 1) ? in[g + 1] : (REAL)0;
+        if (!next_piv && orc_wide_2x2(sizeof(REAL) == 4, p11, p12, p22, piv64)) {
+            const double e11 = p11, e12 = p12, e22 = p22;
+            const double wr = sqrt(fma(e11, e11, e12 * e12));
+            const double wc = e11 / wr, ws = e12 / wr;
+            double y1 = fma(wc, (double)r1, ws * (double)r2);
+            double y2 = fma(wc, (double)r2, -(ws * (double)r1));
+            const double t12 = fma(wc, e12, ws * e22);
+            const double t22 = fma(wc, e22, -(ws * e12));
+            y2 = y2 / t22;
+            y1 = fma(-t12, y2, y1) / wr;
+            if (this_piv) out[g] = (REAL)y1;
+            out[g + 1] = (REAL)y2;
+            continue;
+        }
         const REAL gr = SQRT(FMA(p11, p11, p12 * p12));
         const REAL gc = p11 / gr, gs = p12 / gr;
         REAL g1 = FMA(gc, r1, gs * r2);
@@ -960,7 +1040,7 @@ void F(orc_prec_apply)(const F(fac_t) *f, int stage, const REAL *b, REAL *x)
         REAL *t = (REAL *)malloc(sizeof(REAL) * (n ? n : 1));
 #pragma omp parallel for schedule(static) if (n > 16384)
         for (int g = 0; g < n; ++g) { t[g] = b[g]; x[g] = b[g]; }
-        F(solve_D)(n, f->tri, f->is_piv, t, x);
+        F(solve_D)(n, f->tri, f->is_piv, t, x, f->piv64);
         free(t);
         return;
     }

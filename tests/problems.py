@@ -58,3 +58,42 @@ def random_spd_ish(n=200, density=0.03, seed=3, indefinite=True):
     A = (A + sp.diags(d * (1 + abs(A).sum(axis=1).A1))).tocsr()
     A.sort_indices()
     return A.indptr.astype(np.int32), A.indices.astype(np.int32), A.data.astype(np.float64)
+
+
+def planted_pairs(nblocks=20, block=8, eps=1e-5, coupling=1e-3, density=0.05, seed=17):
+    """A symmetric matrix whose first nblocks diagonal blocks hold 2x2 pairs
+    with d11 d22 = d12^2 (1 - eps) (ratio |det| / (|d11 d22| + d12^2) about
+    eps / 2), coupled (entries of size coupling) only to nblocks further
+    blocks with a dominant diagonal of 10; is_piv marks the pairs for static
+    pivoting.  The paired blocks are level 0 (their pivots see the planted
+    values), the others level 1.  Float32-representable values, so an FP32 and
+    an FP64 factor see the same matrix."""
+    import scipy.sparse as sp
+
+    rng = np.random.default_rng(seed)
+    half = nblocks * block
+    n = 2 * half
+    rows, cols, vals = [], [], []
+    for p in range(0, half, 2):
+        a = rng.uniform(0.5, 2.0) * rng.choice([-1.0, 1.0])
+        b = rng.uniform(0.5, 2.0) * np.sign(a)
+        c = np.sqrt(a * b * (1.0 - eps * rng.uniform(0.5, 1.5))) * rng.choice([-1.0, 1.0])
+        rows += [p, p, p + 1, p + 1]
+        cols += [p, p + 1, p, p + 1]
+        vals += [a, c, c, b]
+    for p in range(half, n):
+        rows.append(p)
+        cols.append(p)
+        vals.append(10.0 * rng.choice([-1.0, 1.0]))
+    C = sp.random(half, half, density=density, random_state=seed, format="coo")
+    r, c, v = C.row, C.col + half, coupling * (2 * C.data - 1)
+    rows += list(r) + list(c)
+    cols += list(c) + list(r)
+    vals += list(v) + list(v)
+    K = sp.csr_matrix((np.array(vals, np.float32).astype(np.float64), (rows, cols)), shape=(n, n))
+    K.sum_duplicates()
+    K.sort_indices()
+    bs = np.arange(0, n + 1, block, dtype=np.int32)
+    is_piv = np.ones(n, np.int32)
+    is_piv[1:half:2] = 0
+    return K.indptr.astype(np.int32), K.indices.astype(np.int32), K.data, bs, is_piv

@@ -197,6 +197,69 @@ def test_spmv_bit_exact(handle, case):
             assert np.array_equal(yg.cpu().numpy(), ref)
 
 
+@pytest.mark.parametrize("case", ["kkt_small", "kkt_scale_rows", "ragged_empty", "rows_to_64", "long_row", "wide_rows"])
+@pytest.mark.parametrize("precision", [cb.F64, cb.F32])
+def test_spmv_sell_bit_exact(handle, case, precision):
+    """The SELL-32 copy (culipx_csr_set_format): every row of at most 64
+    entries is summed serially in column order, so y equals the serial CSR
+    loop bit for bit at any average row length (the CSR kernel's wide rows
+    are group-reduced); the one longer row keeps the warp sum.  The copy
+    holds the values it was built with until culipx_csr_refresh."""
+    if case == "kkt_small":
+        rp, ci, v, _ = kkt("small")
+    elif case == "kkt_scale_rows":
+        rp, ci, v = cb.kkt_generate(20000, 10000, 6, 32, 1e-6, 1e6, seed=11)
+    elif case == "ragged_empty":
+        rng = np.random.default_rng(4)
+        rp, ci, v = _rows_matrix(rng.integers(0, 3, 1000) * rng.integers(0, 12, 1000), 1000, 5)
+    elif case == "rows_to_64":
+        lengths = np.full(2000, 6)
+        lengths[::97] = 64
+        rp, ci, v = _rows_matrix(lengths, 2000, 3)
+    elif case == "long_row":
+        lengths = np.full(3000, 5)
+        lengths[1234] = 2900
+        rp, ci, v = _rows_matrix(lengths, 3000, 6)
+    else:
+        rp, ci, v = _rows_matrix(np.full(700, 40), 3000, 7)
+    m = len(rp) - 1
+    n_cols = int(ci.max()) + 1 if len(ci) else 1
+    dt = np.float64 if precision == cb.F64 else np.float32
+    x = cb.normal_vector(8, max(n_cols, m)).astype(dt)
+    y0 = cb.normal_vector(9, m).astype(dt)
+    vt = torch.from_numpy(v.astype(dt)).cuda()
+    A = cb.CsrOperator(handle, torch.from_numpy(rp).cuda(), torch.from_numpy(ci).cuda(), vt, ncols=len(x))
+    A.set_format(cb.FMT_SELL)
+
+    def check(vals):
+        for alpha, beta in ((1.0, 0.0), (-1.0, 1.0), (0.5, -2.0)):
+            yg = torch.from_numpy(y0.copy()).cuda()
+            A.spmv(torch.from_numpy(x).cuda(), yg, alpha, beta)
+            y = yg.cpu().numpy()
+            if precision == cb.F64:
+                ref = oracle.spmv(rp, ci, vals, x, alpha, beta, y0)
+                if case == "long_row":
+                    assert np.allclose(y, ref, rtol=1e-13, atol=1e-13)
+                else:
+                    assert np.array_equal(y, ref)
+            else:
+                A.set_format(cb.FMT_CSR)
+                yc = torch.from_numpy(y0.copy()).cuda()
+                A.spmv(torch.from_numpy(x).cuda(), yc, alpha, beta)
+                A.set_format(cb.FMT_SELL)
+                if case in ("kkt_small", "kkt_scale_rows", "ragged_empty", "rows_to_64"):
+                    assert np.array_equal(y, yc.cpu().numpy())
+                else:
+                    assert np.allclose(y, yc.cpu().numpy(), rtol=1e-4, atol=1e-4)
+
+    check(v.astype(dt).astype(np.float64))
+    if precision == cb.F64:
+        vt.mul_(-3.0)
+        check(v)  # the copy still holds the old values
+        A.refresh()
+        check(-3.0 * v)
+
+
 def test_sqmr_small_kkt(handle):
     rp, ci, v, bs = kkt("small")
     S, OF, P, F = _factor_both(handle, rp, ci, v, bs)

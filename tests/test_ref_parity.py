@@ -5,8 +5,11 @@ oracle/_ref/ref_dump), run on the same inputs as the culipx path.
 * The factor -- every block's values and sparsity, D, the pivot flags and the
   pivoting permutation -- must equal the reference's bit for bit, on the
   benchmarked scale workload (n = 200000, m = 100000, 32-row blocks, BK)
-  included; on scrambled systems (2x2 pivots, swaps, deep level schedules,
-  fill levels 1-2) with the reference's racy leftover grants replayed.
+  included, and on scrambled systems (2x2 pivots, swaps, deep level
+  schedules).  With fill levels 1-2 the reference's leftover grants race
+  (replayed into the oracle) and its own runs also differ in the last bits
+  of a few blocks: there the sparsity, pivots and permutation are exact and
+  the values within 1e-9 of each block's largest entry (D^-1 b within 1e-7).
 * D^-1 b is a per-row formula: bit for bit.  The triangular sweeps: the
   reference sums each row's terms with atomicAdd (block_ildlt_kernels.impl.cuh
   k_solve_blocks_*), so its own results vary in the last bits; within 1e-14
@@ -55,13 +58,19 @@ def _gpu_factor(handle, rp, ci, v, bs, pivot, precision, fill_level=0, is_piv=No
     return P, F, ref.canonical_export(F.export(), rows, pe["coarse_col"], pe["fmt"])
 
 
-def _assert_blocks_equal(mine, theirs):
+def _assert_blocks_equal(mine, theirs, rtol=0.0):
+    """Same blocks, formats and sparsity; values bit for bit (rtol 0) or
+    within rtol of each block's largest entry."""
     assert set(mine) == set(theirs)
     for key, (fr, nr, _gr, ir, vr) in theirs.items():
         fm, nm, _gm, im, vm = mine[key]
         assert fm == fr, key
         assert np.array_equal(im, ir), key
-        assert np.array_equal(vm, vr), key
+        if rtol == 0.0:
+            assert np.array_equal(vm, vr), key
+        else:
+            scale = float(np.max(np.abs(vr))) if len(vr) else 0.0
+            assert np.max(np.abs(vm - vr), initial=0.0) <= rtol * scale, key
 
 
 CASES = {
@@ -111,7 +120,7 @@ def _backward_error(U, perm, b, y, stage):
     return np.max(np.abs(r)) / np.max(abs(T) @ np.abs(t))
 
 
-def _assert_applies(apply, R, b, dt, direct, U=None, perm=None):
+def _assert_applies(apply, R, b, dt, direct, U=None, perm=None, mtol=0.0):
     """D^-1 b bit for bit; the sweeps within 1e-14 (FP32: 1e-6) of the
     reference's on natural-order systems.  On scrambled systems (entries up to
     1e8, long cancelling sums) the reference's atomicAdd order moves its result
@@ -123,7 +132,10 @@ def _assert_applies(apply, R, b, dt, direct, U=None, perm=None):
         y = apply(stage)
         yr = R[key]
         if stage == cb.MIDDLE:
-            assert np.array_equal(y, yr), key
+            if mtol:
+                assert np.linalg.norm(y.astype(float) - yr) <= mtol * np.linalg.norm(yr), key
+            else:
+                assert np.array_equal(y, yr), key
         elif direct:
             assert np.linalg.norm(y.astype(float) - yr) <= tol * np.linalg.norm(yr), key
         else:
@@ -143,6 +155,9 @@ def test_factor_and_applies_match_reference(handle, case):
     rp, ci, v, bs = make()
     n = len(rp) - 1
     dt = np.float64 if precision == cb.F64 else np.float32
+    # with fill, the reference varies between its own runs: up to 30 of its
+    # grants, and (grants replayed) the last bits of a few blocks
+    rtol = 0.0 if fill == 0 else 1e-9
     b = cb.normal_vector(cb.SEED + 1, n)
     R = ref.run(rp, ci, v, bs, b, precision=1 if precision == cb.F64 else 0, pivot=pivot, fill_level=fill,
                 max_it=0)
@@ -154,12 +169,13 @@ def test_factor_and_applies_match_reference(handle, case):
     # the reference's own numerics, its grant decisions given
     OFr = S.factor(v.astype(dt), pivot=pivot, forced_grants=ref_grants)
     Er = OFr.export()
-    _assert_blocks_equal(ref.canonical_export(Er, S.blk_row, S.blk_col, S.fmt), theirs)
-    for k in ("tri", "is_piv", "perm"):
+    _assert_blocks_equal(ref.canonical_export(Er, S.blk_row, S.blk_col, S.fmt), theirs, rtol)
+    for k in ("is_piv", "perm"):
         assert np.array_equal(Er[k], R[k]), k
+    assert np.allclose(Er["tri"], R["tri"], rtol=rtol, atol=0.0) if rtol else np.array_equal(Er["tri"], R["tri"])
     direct = not case.startswith("scrambled")
     U = None if direct else _u_matrix(Er, S, bs, n)
-    _assert_applies(lambda st: OFr.apply(st, b.astype(dt)), R, b, dt, direct, U, Er["perm"])
+    _assert_applies(lambda st: OFr.apply(st, b.astype(dt)), R, b, dt, direct, U, Er["perm"], 1e2 * rtol)
     # the GPU path against the oracle with its own grants, bit for bit
     E = F.export()
     Eo = S.factor(v.astype(dt), pivot=pivot).export()
@@ -168,10 +184,11 @@ def test_factor_and_applies_match_reference(handle, case):
     bt = torch.from_numpy(b.astype(dt)).cuda()
     if np.array_equal(E["got_extra"], ref_grants):
         # the same decisions: the GPU factor and applies against the reference directly
-        _assert_blocks_equal(mine, theirs)
-        for k in ("tri", "is_piv", "perm"):
+        _assert_blocks_equal(mine, theirs, rtol)
+        for k in ("is_piv", "perm"):
             assert np.array_equal(E[k], R[k]), k
-        _assert_applies(lambda st: F.apply(st, bt).cpu().numpy(), R, b, dt, direct, U, Er["perm"])
+        assert np.allclose(E["tri"], R["tri"], rtol=rtol, atol=0.0) if rtol else np.array_equal(E["tri"], R["tri"])
+        _assert_applies(lambda st: F.apply(st, bt).cpu().numpy(), R, b, dt, direct, U, Er["perm"], 1e2 * rtol)
 
 
 @pytest.mark.parametrize("name,its_tol,rtol,restol", [("small", 2, 5e-2, 0.2), ("scale", 8, 1e-2, 5e-2)])

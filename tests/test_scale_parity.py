@@ -30,6 +30,7 @@ import pytest
 import scipy.sparse as sp
 
 import culip_b200 as cb
+from culip_b200 import _capi as capi
 import oracle
 from problems import kkt
 
@@ -97,6 +98,26 @@ def test_scale_sqmr_1000_true_relres(scale):
     rg = np.linalg.norm(s["b"] - K @ x.cpu().numpy()) / nb
     ro = np.linalg.norm(s["b"] - K @ xo) / nb
     assert abs(rg - ro) <= 5e-3 * ro
+
+
+def test_scale_refine_never_worse_than_start(scale):
+    """Refinement on the scale workload: its 1000-iteration correction leaves
+    a true relative residual near 1.45, above the 1.0 of x = 0.  The
+    refinement returns its best iterate, so its relres is at most 1.0 and is
+    the true residual of the returned x, and it stops (STALLED) once
+    corrections stop helping instead of running to max_refine."""
+    s = scale
+    x = torch.full((s["n"],), 7.0, dtype=torch.float64, device="cuda")
+    rel, its, steps, st = cb.sqmr_refine(s["h"], s["A"], s["F"], torch.from_numpy(s["b"]).cuda(), x, 1e-8, 1e-8, 1000,
+                                         6)
+    assert st in (capi.STALLED, capi.MAXIT) and steps >= 2 and its <= 1000 * steps
+    assert rel <= 1.0
+    K = sp.csr_matrix((s["v"], s["ci"], s["rp"]), shape=(s["n"], s["n"]))
+    xh = x.cpu().numpy()
+    true_rel = np.linalg.norm(s["b"] - K @ xh) / np.linalg.norm(s["b"])
+    assert abs(true_rel - rel) <= 1e-9 * rel
+    if rel == 1.0:
+        assert not xh.any()
 
 
 def test_mixed_construction_tenth_fp32_factor_exact():
