@@ -248,10 +248,13 @@ struct DBlock {
 // acc[j] - sum_k val[k] x[col[k] NR + j] in increasing k for the NR
 // interleaved right-hand sides (x is written during the kernel: plain loads);
 // index / value loads of a batch, then its gathers (the NR values of one
-// column are adjacent: 16-byte loads for even NR)
-template <class TF, int NR>
+// column are adjacent: 16-byte loads for even NR).  SC: the gathered values
+// are stored unscaled and enter as (TF)(x * xs[j]), the value an earlier
+// phase would have stored after scaling.
+template <class TF, int NR, bool SC = false>
 __device__ __forceinline__ void row_sub(TF (&acc)[NR], int k0, int k1, const int* __restrict__ col,
-                                        const TF* __restrict__ val, const double* x)
+                                        const TF* __restrict__ val, const double* x,
+                                        const double* xs = nullptr)
 {
     constexpr int B = (NR == 1) ? kBatch : (NR == 2 ? 4 : 2);
     for (int k = k0; k < k1; k += B) {
@@ -282,7 +285,8 @@ __device__ __forceinline__ void row_sub(TF (&acc)[NR], int k0, int k1, const int
         for (int j = 0; j < B; ++j)
             if (k + j < k1)
 #pragma unroll
-                for (int r = 0; r < NR; ++r) acc[r] = fma_rn(-v[j], (TF)xv[j][r], acc[r]);
+                for (int r = 0; r < NR; ++r)
+                    acc[r] = fma_rn(-v[j], SC ? (TF)(xv[j][r] * xs[r]) : (TF)xv[j][r], acc[r]);
     }
 }
 
@@ -580,7 +584,7 @@ enum RhsFrom {
 // One U'-sweep work item: dst[row] = U_II'^-1 (rhs - U'_I* dst) (interleaved)
 // with the lane's right-hand sides taken as FROM says.  t receives the
 // lane's results (0 for lanes >= h).
-template <class TF, int NR, int FROM>
+template <class TF, int NR, int FROM, bool SCG = false>
 __device__ __forceinline__ void ut_item(const PArgs<TF>& a, const ItemMeta& m, const double* src,
                                         const double (&sc)[NR], double* dst, double (&t)[NR])
 {
@@ -605,7 +609,8 @@ __device__ __forceinline__ void ut_item(const PArgs<TF>& a, const ItemMeta& m, c
         TF acc[NR];
 #pragma unroll
         for (int r = 0; r < NR; ++r) acc[r] = (TF)y[r];
-        row_sub<TF, NR>(acc, __ldg(a.ut_off + fr + lane), __ldg(a.ut_off + fr + lane + 1), a.ut_col, a.ut_val, dst);
+        row_sub<TF, NR, SCG>(acc, __ldg(a.ut_off + fr + lane), __ldg(a.ut_off + fr + lane + 1), a.ut_col, a.ut_val,
+                             dst, sc);
 #pragma unroll
         for (int r = 0; r < NR; ++r) t[r] = (double)acc[r];
     }
@@ -646,7 +651,7 @@ __device__ __forceinline__ void u_item_res(const PArgs<TF>& a, const ResSlot<TF>
     }
 }
 
-template <class TF, int NR, int FROM>
+template <class TF, int NR, int FROM, bool SCG = false>
 __device__ __forceinline__ void ut_item_res(const PArgs<TF>& a, const ResSlot<TF>& rs, const double* src,
                                             const double (&sc)[NR], double* dst, double (&t)[NR])
 {
@@ -671,7 +676,7 @@ __device__ __forceinline__ void ut_item_res(const PArgs<TF>& a, const ResSlot<TF
         TF acc[NR];
 #pragma unroll
         for (int r = 0; r < NR; ++r) acc[r] = (TF)y[r];
-        row_sub<TF, NR>(acc, rs.ut0[lane], rs.ut1[lane], a.ut_col, a.ut_val, dst);
+        row_sub<TF, NR, SCG>(acc, rs.ut0[lane], rs.ut1[lane], a.ut_col, a.ut_val, dst, sc);
 #pragma unroll
         for (int r = 0; r < NR; ++r) t[r] = (double)acc[r];
     }
@@ -840,6 +845,7 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal 
         for (int j = 0; j < NR; ++j) {
             memset(&S[j], 0, sizeof(Scal));
             S[j].c[0] = -1.0;
+            cfs.sc[j] = 1.0;  // the scale of the Av that the initial phase leaves
         }
         long long np = 0;
         for (int L = 1; L < a.nl; ++L) {
@@ -850,6 +856,15 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal 
     }
     __syncthreads();
     auto lvl = [&](int L) -> LvlBounds { return L < kLvlCache ? lvb[L] : level_bounds(a, sv, L); };
+    // Two levels, level 0 all simple block rows whose K rows reach only
+    // themselves and level-1 rows (a natural-order KKT system): each level-0
+    // row computes its (K ev) in the U sweep, right after its ev, and the U'
+    // sweep's level-0 phase and its barrier go away.  Level-0 Av is then kept
+    // unscaled (the 1/delta it needs is known only after the U sweep's
+    // reduction); every reader applies the scale of the iteration that wrote
+    // it, at the point where the unfused path rounded it, so the results are
+    // the unfused path's bit for bit.
+    const bool fused = a.fuse_l0 && a.nl == 2 && lvb[0].c1 == lvb[0].c0;
 
     // the level with the most pivot-tile items keeps its first kResSlots x
     // (grid) items in the warps' shared-memory slots
@@ -1044,6 +1059,7 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal 
                 // rows of simple block rows: thread per row (u_item with D = d,
                 // an identity tile and no swaps)
                 const int s1 = lb.s1;
+                const bool fz = fused && L == 0;
                 for (int i = lb.s0 + ctx.g0; i < s1; i += ctx.gstride) {
                     const int g = __ldg(a.simple_rows + i);
                     const double dd = (double)__ldg(a.dg + g);
@@ -1051,7 +1067,8 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal 
 #pragma unroll
                     for (int j = 0; j < NR; ++j) {
                         const size_t o = (size_t)g * NR + j;
-                        double v = a.Av[o];
+                        // fused level 0: Av holds the last iteration's unscaled (K ev)
+                        double v = fz ? (double)(TF)(a.Av[o] * cv.sc[j]) : a.Av[o];
                         double* const vk1 = cv.vk1;
                         v = fma_rn(na[j], cv.vk[o], v);
                         v = fma_rn(nb[j], vk1[o], v);
@@ -1062,6 +1079,14 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal 
                     row_sub<TF, NR>(acc, __ldg(a.u_off + g), __ldg(a.u_off + g + 1), a.u_colp, a.u_val, a.ev);
 #pragma unroll
                     for (int j = 0; j < NR; ++j) a.ev[(size_t)g * NR + j] = (double)acc[j];
+                    if (fz) {
+                        // K row g reaches only ev[g] (written just above) and level-1
+                        // rows (final since the last barrier)
+                        double y[NR];
+                        spmv_row<TF, NR>(a, g, a.ev, y);
+#pragma unroll
+                        for (int j = 0; j < NR; ++j) a.Av[(size_t)g * NR + j] = y[j];
+                    }
                 }
                 if (L > 0) {
                     ctx.sync();
@@ -1116,6 +1141,8 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal 
             for (int j = 0; j < 4 * NR; ++j) r[j] = 0.0;
             const volatile Coef<NR>& cf = cfs;
             for (int L = 0; L < a.nl; ++L) {
+                // fused: level 0 has no items and its rows' products are done
+                if (fused && L == 0) continue;
                 const LvlBounds lb = lvl(L);
                 const int c1 = lb.c1;
                 for (int t = lb.c0 + wid; t < c1; t += nwarps) {
@@ -1128,11 +1155,13 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal 
                     for (int j = 0; j < NR; ++j) scv[j] = cf.sc[j];
                     DBlock<TF> D;
                     if (res) {
-                        if (L == 0) ut_item_res<TF, NR, kRhsSpmv>(a, *rs, a.ev, scv, a.Av, av);
+                        if (fused) ut_item_res<TF, NR, kRhsSpmv, true>(a, *rs, a.ev, scv, a.Av, av);
+                        else if (L == 0) ut_item_res<TF, NR, kRhsSpmv>(a, *rs, a.ev, scv, a.Av, av);
                         else ut_item_res<TF, NR, kRhsPre>(a, *rs, a.ev, scv, a.Av, av);
                         D = dblock_res(a, *rs);
                     } else {
-                        if (L == 0) ut_item<TF, NR, kRhsSpmv>(a, m, a.ev, scv, a.Av, av);
+                        if (fused) ut_item<TF, NR, kRhsSpmv, true>(a, m, a.ev, scv, a.Av, av);
+                        else if (L == 0) ut_item<TF, NR, kRhsSpmv>(a, m, a.ev, scv, a.Av, av);
                         else ut_item<TF, NR, kRhsPre>(a, m, a.ev, scv, a.Av, av);
                         D.load(a, fr, h, flags);
                     }
@@ -1204,9 +1233,17 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal 
                     double y[NR];
                     spmv_row<TF, NR>(a, g, a.ev, y);
                     TF acc[NR];
+                    double scv[NR];
 #pragma unroll
-                    for (int j = 0; j < NR; ++j) acc[j] = (TF)(y[j] * cf.sc[j]);
-                    row_sub<TF, NR>(acc, __ldg(a.ut_off + g), __ldg(a.ut_off + g + 1), a.ut_col, a.ut_val, a.Av);
+                    for (int j = 0; j < NR; ++j) {
+                        scv[j] = cf.sc[j];
+                        acc[j] = (TF)(y[j] * scv[j]);
+                    }
+                    if (fused)  // level 1: its U' rows gather the unscaled level-0 Av
+                        row_sub<TF, NR, true>(acc, __ldg(a.ut_off + g), __ldg(a.ut_off + g + 1), a.ut_col, a.ut_val,
+                                              a.Av, scv);
+                    else
+                        row_sub<TF, NR>(acc, __ldg(a.ut_off + g), __ldg(a.ut_off + g + 1), a.ut_col, a.ut_val, a.Av);
                     double av[NR];
 #pragma unroll
                     for (int j = 0; j < NR; ++j) {
@@ -1229,7 +1266,10 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal 
                             const int g = __ldg(a.simple_rows + i);
                             double av[NR];
 #pragma unroll
-                            for (int j = 0; j < NR; ++j) av[j] = a.Av[(size_t)g * NR + j];
+                            for (int j = 0; j < NR; ++j) {
+                                const double w = a.Av[(size_t)g * NR + j];
+                                av[j] = (fused && L == 1) ? (double)(TF)(w * cf.sc[j]) : w;
+                            }
                             simple_epilogue<TF, NR>(a, g, av, cv.vk, cv.vk1, cv.pkm1, cv.pk, cv.pk, cf, r);
                         }
                     }
