@@ -56,9 +56,11 @@ def _parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="culipx", choices=["culipx", "reference"])
-    ap.add_argument("--config", default="scale", choices=["small", "scale", "mixed", "batch", "served", "spmv"])
+    ap.add_argument("--config", default="scale", choices=["small", "scale", "mixed", "batch", "served", "spmv", "schur"])
     ap.add_argument("--spmv-workload", default="mixed", choices=["small", "scale", "mixed"],
                     help="--config spmv: the KKT matrix whose product is timed")
+    ap.add_argument("--spmv-format", default="sell", choices=["csr", "sell"],
+                    help="--config spmv: the CSR arrays or the SELL-32 copy (culipx_csr_set_format)")
     ap.add_argument("--rate", type=float, default=2000.0, help="--config served: arrivals per second")
     ap.add_argument("--duration", type=float, default=0.25, help="--config served: seconds of arrivals")
     ap.add_argument("--patterns", type=int, default=64, help="--config served: sparsity patterns")
@@ -329,7 +331,8 @@ def run_culipx(args):
         "e2e": {"value": job_rate(world, e2e_steps, e2e_total / 1e3), "unit": UNIT,
                 "h2d_bytes_per_step": int(nnz * 8 + N * 8), "d2h_bytes_per_step": int(N * 8)},
         "roofline": roof,
-        "spmv": spmv_roofline(A, N, nnz, flush, stream),
+        "spmv": spmv_formats(h, d_rp, d_ci, d_v, N, nnz, flush, stream),
+        "sweeps": sweep_roofline(F, N, flush, stream),
     }
     if rank == 0 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(args.config, rp, ci, v, bs, b, args.max_it)
@@ -376,7 +379,71 @@ def sqmr_roofline(info, N, nnz, its, launch_ms, nr=1, kernel="k_sqmr_persistent<
             "avg_launch_ms": launch_ms, "us_per_iteration": launch_ms * 1e3 / max(its, 1)}
 
 
-def spmv_roofline(A, N, nnz, flush, stream, reps=20):
+def sweep_roofline(F, N, flush, stream, reps=10, precision_bytes=8):
+    """The standalone triangular solves (culipx_prec_apply; the reference's
+    solve_left / solve_right), L2 flushed before every call (outside the
+    events): LEFT = the pivot permutation gather + the U' level sweeps,
+    RIGHT = a copy + the U level sweeps + the permutation scatter.
+    Algorithmic bytes: B_tri = nnz_U (s + 4) + 4 (N + 1) + s * (upper-triangle
+    entries of the non-identity pivot tiles) + 2 s N for the sweeps, plus the
+    permutation pass (read b, the permutation, write x: 2 s N + 4 N) and for
+    RIGHT the copy (2 s N).  One launch per level plus the permutation."""
+    import torch
+
+    import culip_b200 as cb
+
+    info = F.info()
+    s = info["value_bytes"]
+    dt = torch.float64 if s == 8 else torch.float32
+    b = torch.linspace(-1.0, 1.0, N, dtype=dt, device="cuda")
+    x = torch.zeros_like(b)
+    b_tri = info["u_nnz"] * (s + 4) + 4 * (N + 1) + s * info["tile_entries"] + 2 * s * N
+    peak = _peak_hbm()
+    out = {}
+    for name, stage, extra in (("u_transpose_sweep (LEFT)", cb.LEFT, 2 * s * N + 4 * N),
+                               ("u_sweep (RIGHT)", cb.RIGHT, 2 * s * N + 4 * N + 2 * s * N)):
+        for _ in range(3):
+            F.apply(stage, b, x)
+        ms = []
+        for i in range(reps):
+            flush.fill_(float(i))
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            F.apply(stage, b, x)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        t = float(np.mean(ms))
+        byt = b_tri + extra
+        out[name] = {"achieved": byt / (t * 1e-3) / 1e9, "frac": byt / (t * 1e-3) / 1e9 / peak,
+                     "avg_us": t * 1e3, "algorithmic_bytes": int(byt)}
+    out.update({"unit": "GB/s", "peak": peak, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
+                "kernels": "k_perm_gather / cudaMemcpyAsync + k_sweep_level per level + k_perm_scatter",
+                "l2": "flushed before every call"})
+    return out
+
+
+def spmv_formats(h, d_rp, d_ci, d_v, N, nnz, flush, stream, reps=20):
+    """spmv_roofline for the CSR arrays and for the SELL-32 copy
+    (culipx_csr_set_format), each on its own operator."""
+    import culip_b200 as cb
+
+    out = {}
+    for name, fmt in (("csr", cb.FMT_CSR), ("sell", cb.FMT_SELL)):
+        B = cb.CsrOperator(h, d_rp, d_ci, d_v)
+        if fmt != cb.FMT_CSR:
+            B.set_format(fmt)
+        out[name] = spmv_roofline(B, N, nnz, flush, stream, reps,
+                                  kernel="k_sell_spmv<double>" if fmt == cb.FMT_SELL else "k_csr_spmv_rows<double>")
+    best = max(out, key=lambda k: out[k]["achieved"])
+    res = dict(out[best])
+    res["format"] = best
+    res["formats"] = {k: {"achieved": o["achieved"], "frac": o["frac"], "avg_launch_us": o["avg_launch_us"]}
+                      for k, o in out.items()}
+    return res
+
+
+def spmv_roofline(A, N, nnz, flush, stream, reps=20, kernel="k_csr_spmv_rows<double>"):
     """Standalone y = K x (culipx_spmv, FP64, beta = 0) with L2 flushed before
     every launch (outside the events): algorithmic bytes
     B_spmv = nnz_K (8 + 4) + 4 (N + 1) + 8 N (x) + 8 N (y) over the mean
@@ -399,7 +466,7 @@ def spmv_roofline(A, N, nnz, flush, stream, reps=20):
     t = float(np.mean(ms))
     b = nnz * 12 + 4 * (N + 1) + 16 * N
     peak = _peak_hbm()
-    return {"kernel": "k_csr_spmv_rows<double> (culipx_spmv, L2 flushed before each launch)", "achieved": b / (t * 1e-3) / 1e9,
+    return {"kernel": f"{kernel} (culipx_spmv, L2 flushed before each launch)", "achieved": b / (t * 1e-3) / 1e9,
             "peak": peak, "unit": "GB/s", "frac": b / (t * 1e-3) / 1e9 / peak, "algorithmic_bytes": int(b),
             "avg_launch_us": t * 1e3, "launches": reps}
 
@@ -741,7 +808,8 @@ def run_mixed(args):
         "e2e": {"value": nr * len(e_ms) / (float(np.sum(e_ms)) / 1e3), "unit": "solves/s",
                 "h2d_bytes_per_step": int(nnz * 8 + nr * N * 8), "d2h_bytes_per_step": int(nr * N * 8)},
         "roofline": roof,
-        "spmv": spmv_roofline(A, N, nnz, flush, stream),
+        "spmv": spmv_formats(h, d_rp, d_ci, d_v, N, nnz, flush, stream),
+        "sweeps": sweep_roofline(F, N, flush, stream),
     }
     if rank == 0:
         print(json.dumps(out), flush=True)
@@ -762,6 +830,10 @@ def run_spmv(args):
     stream = torch.cuda.current_stream()
     h = cb.Handle(local, stream)
     A = cb.CsrOperator(h, torch.from_numpy(rp).cuda(), torch.from_numpy(ci).cuda(), torch.from_numpy(v).cuda())
+    kname = "k_csr_spmv_rows<double>"
+    if args.spmv_format == "sell":
+        A.set_format(cb.FMT_SELL)
+        kname = "k_sell_spmv<double>"
     flush = L2Flush()
     x = torch.linspace(-1.0, 1.0, N, dtype=torch.float64, device="cuda")
     y = torch.zeros(N, dtype=torch.float64, device="cuda")
@@ -809,14 +881,14 @@ def run_spmv(args):
             if ln.startswith("dram_bytes_per_launch"):
                 traffic = float(ln.split("=")[1])
     out = {
-        "metric": "SpMV HBM GB/s (culipx_spmv, FP64 CSR, y = K x)", "value": gbs, "unit": "GB/s", "n_gpus": world,
+        "metric": "SpMV HBM GB/s (culipx_spmv, FP64, y = K x)", "value": gbs, "format": args.spmv_format, "unit": "GB/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded KKT generator)",
         "config": _config_dict(args.spmv_workload, cfg, nnz, {"parallelism": "one GPU"}, solve="y = K x only"),
         "gpu_launches": int(launches), "clocks": ck,
         "e2e": {"value": b / (float(np.mean(e_ms)) * 1e-3) / 1e9, "unit": "GB/s", "h2d_bytes_per_step": int(8 * N),
                 "d2h_bytes_per_step": int(8 * N)},
-        "roofline": {"kernel": "k_csr_spmv_rows<double>", "bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s",
+        "roofline": {"kernel": kname, "bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s",
                      "frac": gbs / peak, "traffic": traffic, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
                      "algorithmic_bytes": int(b), "avg_launch_us": t * 1e3},
     }
@@ -1100,10 +1172,104 @@ def run_served(args):
         print(json.dumps(out), flush=True)
 
 
+def schur_update_stats(P, F, bs):
+    """Sparsity of the block Schur updates of a computed factor, from its
+    export: for every pivot block row k and every pair of its off-diagonal
+    blocks (k, i), (k, j), i <= j, whose target block (i, j) exists in the
+    pattern (level-based fill drops the rest), the update U_ki' D_k U_kj.
+    F_alg counts 2 flops per product of a nonzero of U_ki and a nonzero of
+    U_kj in the same row of block row k (1x1 pivots; the sparse work the
+    update needs), F_tile 2 h_k h_i h_j (the dense tile product a tensor-core
+    MMA would issue).  Returns the totals and histograms of nonzeros per
+    off-diagonal block and of F_alg / F_tile per update."""
+    pe = P.export()
+    E = F.export()
+    bs = np.asarray(bs, np.int64)
+    off, col = pe["coarse_off"].astype(np.int64), pe["coarse_col"].astype(np.int64)
+    cm = len(off) - 1
+    rows = np.repeat(np.arange(cm), np.diff(off))
+    exists = set(zip(rows.tolist(), col.tolist()))
+    bo = E["blk_off"]
+    nnz_blk, dens = [], []
+    f_alg = f_tile = 0.0
+    n_upd = 0
+    for k in range(cm):
+        hk = int(bs[k + 1] - bs[k])
+        qs = [q for q in range(off[k], off[k + 1]) if col[q] > k]
+        if not qs:
+            continue
+        rn = {}
+        for q in qs:
+            J = int(col[q])
+            w = int(bs[J + 1] - bs[J])
+            s0, s1 = int(bo[q]), int(bo[q + 1])
+            idx, val = E["idx"][s0:s1], E["val"][s0:s1]
+            keep = val != 0
+            r = np.bincount(idx[keep] // w, minlength=hk)[:hk].astype(np.float64)
+            rn[J] = r
+            nnz_blk.append(int(keep.sum()))
+        cols = sorted(rn)
+        for a, i in enumerate(cols):
+            for j in cols[a:]:
+                if (i, j) not in exists:
+                    continue
+                fa = 2.0 * float(rn[i] @ rn[j])
+                ft = 2.0 * hk * float(bs[i + 1] - bs[i]) * float(bs[j + 1] - bs[j])
+                f_alg += fa
+                f_tile += ft
+                dens.append(fa / ft)
+                n_upd += 1
+    nnz_blk = np.array(nnz_blk)
+    dens = np.array(dens) if dens else np.zeros(1)
+    hist_edges = [0, 1, 2, 4, 8, 16, 32, 64, 128, 256, 512, 1025]
+    h_nnz, _ = np.histogram(nnz_blk, bins=hist_edges)
+    d_edges = [0, 1e-3, 3e-3, 1e-2, 3e-2, 0.1, 0.3, 1.0001]
+    h_den, _ = np.histogram(dens, bins=d_edges)
+    return {"updates": n_upd, "F_alg": f_alg, "F_tile": f_tile, "F_alg_over_F_tile": f_alg / max(f_tile, 1.0),
+            "offdiag_blocks": int(len(nnz_blk)),
+            "nnz_per_offdiag_block": {"median": float(np.median(nnz_blk)) if len(nnz_blk) else 0.0,
+                                      "max": int(nnz_blk.max()) if len(nnz_blk) else 0,
+                                      "histogram": {f"[{a},{b})": int(c) for a, b, c in
+                                                    zip(hist_edges[:-1], hist_edges[1:], h_nnz)}},
+            "update_density": {"median": float(np.median(dens)), "max": float(dens.max()),
+                               "updates_at_least_0.1": int((dens >= 0.1).sum()),
+                               "histogram": {f"[{a:g},{b:g})": int(c) for a, b, c in
+                                             zip(d_edges[:-1], d_edges[1:], h_den)}}}
+
+
+def run_schur(args):
+    """The tensor-core question for the factorization: F_alg vs F_tile of the
+    block Schur updates (schur_update_stats) of the FP32 factor of the
+    mixed-precision workload (n = 1e6, m = 5e5) and of the FP64 factor of the
+    scale workload, on their BK factors as the GPU computes them."""
+    import torch
+
+    import culip_b200 as cb
+
+    torch.cuda.set_device(0)
+    h = cb.Handle(0)
+    res = {}
+    for name, prec in (("mixed", cb.F32), ("scale", cb.F64)):
+        cfg, rp, ci, v, bs, _ = _workload(name)
+        P = cb.Pattern(h, rp, ci, bs, 0, 1.0, prec)
+        F = cb.Factor(P)
+        F.compute(torch.from_numpy(v).to(torch.float32 if prec == cb.F32 else torch.float64).cuda(), None,
+                  cb.PIV_BK, 0.0)
+        t0 = time.perf_counter()
+        st = schur_update_stats(P, F, bs)
+        st["analysis_s"] = time.perf_counter() - t0
+        st["workload"] = _config_dict(name, cfg, len(ci))["workload"]
+        res[name] = st
+    print(json.dumps({"metric": "block Schur updates: F_alg / F_tile (tensor-core candidate work)", "configs": res}),
+          flush=True)
+
+
 if __name__ == "__main__":
     a = _parse()
     if a.impl == "reference":
         run_reference(a)
+    elif a.config == "schur":
+        run_schur(a)
     elif a.config == "mixed":
         run_mixed(a)
     elif a.config == "spmv":

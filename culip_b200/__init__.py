@@ -336,6 +336,47 @@ class PermutePlan:
             pass
 
 
+class KktAssembly:
+    """K = [[diag(d) + delta I, A'], [A, -gamma I]] of an interior-point
+    iteration, d = s / x (or given), as full symmetric CSR: the structure is
+    planned once per pattern of A (m x n CSR, torch int32 CUDA tensors),
+    assemble() writes one iteration's values on the device."""
+
+    def __init__(self, handle: Handle, m: int, n: int, d_rowptr, d_colidx):
+        self.handle = handle
+        self.m, self.n = int(m), int(n)
+        self._keep = (d_rowptr, d_colidx)
+        h = ctypes.c_void_p()
+        capi.call("culipx_kkt_assembly_create", handle._h, self.m, self.n, int(d_colidx.numel()), _dptr(d_rowptr),
+                  _dptr(d_colidx), ctypes.byref(h))
+        self._h = h
+        N = ctypes.c_int()
+        nnz = ctypes.c_longlong()
+        capi.call("culipx_kkt_assembly_size", self._h, ctypes.byref(N), ctypes.byref(nnz))
+        self.N, self.nnz = N.value, nnz.value
+
+    def structure(self):
+        """(rowptr, colidx) of K as host numpy int32 arrays."""
+        rowptr = np.zeros(self.N + 1, np.int32)
+        colidx = np.zeros(max(self.nnz, 1), np.int32)
+        capi.call("culipx_kkt_assembly_export", self._h, _p(rowptr), _p(colidx))
+        return rowptr, colidx[: self.nnz]
+
+    def assemble(self, d_aval, d_kval, x=None, s=None, d=None, delta=1e-8, gamma=1e-8):
+        """K's values into d_kval (float64 or float32 CUDA tensor of nnz
+        entries) from A's values and the iterate (x, s) or the diagonal d."""
+        prec = F64 if d_kval.dtype.itemsize == 8 else F32
+        capi.call("culipx_kkt_assemble", self._h, _dptr(d_aval), _dptr(x), _dptr(s), _dptr(d), float(delta),
+                  float(gamma), prec, _dptr(d_kval))
+        return d_kval
+
+    def __del__(self):
+        try:
+            _release(self, "culipx_kkt_assembly_destroy")
+        except Exception:  # interpreter shutdown
+            pass
+
+
 class CsrOperator:
     """CSR operator over torch CUDA tensors (kept alive by this object)."""
 

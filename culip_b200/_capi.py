@@ -79,6 +79,12 @@ _SIGS = {
     "culipx_csr_create": [vp, i32, i32, i64, vp, vp, vp, i32, i32, ctypes.POINTER(vp)],
     "culipx_csr_destroy": [vp],
     "culipx_spmv": [vp, vp, vp, f64, f64, i32],
+    "culipx_kkt_assembly_create": [vp, i32, i32, i64, vp, vp, ctypes.POINTER(vp)],
+    "culipx_kkt_assembly_destroy": [vp],
+    "culipx_kkt_assembly_size": [vp, ctypes.POINTER(i32), ctypes.POINTER(i64)],
+    "culipx_kkt_assembly_structure": [vp, ctypes.POINTER(vp), ctypes.POINTER(vp)],
+    "culipx_kkt_assembly_export": [vp, vp, vp],
+    "culipx_kkt_assemble": [vp, vp, vp, vp, vp, f64, f64, i32, vp],
     "culipx_csr_set_format": [vp, i32],
     "culipx_csr_refresh": [vp],
     "culipx_sqmr_solve": [vp, vp, vp, vp, vp, f64, i32, ctypes.POINTER(f64), ctypes.POINTER(i32)],

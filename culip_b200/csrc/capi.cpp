@@ -1,5 +1,6 @@
 // extern "C" entry points of libculipx (declared in include/culipx.h).
 #include "factor.h"
+#include "kkt_assembly.h"
 #include "ldu.h"
 #include "operators.h"
 #include "pattern.h"
@@ -421,6 +422,70 @@ CULIPX_API int culipx_csr_create(culipx_handle h, int m, int n, long long nnz, c
     handle_retain(h);
     *out = A;
     return CULIPX_OK;
+    GUARD_END
+}
+
+CULIPX_API int culipx_kkt_assembly_create(culipx_handle h, int m, int n, long long nnz_a, const int* d_rowptr,
+                                          const int* d_colidx, culipx_kkt_assembly* out)
+{
+    if (!h || !out) return fail(CULIPX_INVALID_ARG, "culipx_kkt_assembly_create: null argument");
+    GUARD_BEGIN
+    CULIPX_TRY(use_device(h));
+    KktAssembly* K = nullptr;
+    CULIPX_TRY(kkt_assembly_create(h, m, n, nnz_a, d_rowptr, d_colidx, &K));
+    handle_retain(h);
+    *out = static_cast<culipx_kkt_assembly>(K);
+    return CULIPX_OK;
+    GUARD_END
+}
+
+CULIPX_API int culipx_kkt_assembly_destroy(culipx_kkt_assembly K)
+{
+    if (K) {
+        culipx_handle_t* h = K->handle;
+        set_device_of(h);
+        delete static_cast<KktAssembly*>(K);
+        handle_release(h);
+    }
+    return CULIPX_OK;
+}
+
+CULIPX_API int culipx_kkt_assembly_size(culipx_kkt_assembly K, int* N, long long* nnz_k)
+{
+    if (!K) return fail(CULIPX_INVALID_ARG, "null plan");
+    if (N) *N = K->n + K->m;
+    if (nnz_k) *nnz_k = K->nnz_k;
+    return CULIPX_OK;
+}
+
+CULIPX_API int culipx_kkt_assembly_structure(culipx_kkt_assembly K, const int** d_rowptr, const int** d_colidx)
+{
+    if (!K) return fail(CULIPX_INVALID_ARG, "null plan");
+    if (d_rowptr) *d_rowptr = K->rowptr.as<int>();
+    if (d_colidx) *d_colidx = K->colidx.as<int>();
+    return CULIPX_OK;
+}
+
+CULIPX_API int culipx_kkt_assembly_export(culipx_kkt_assembly K, int* h_rowptr, int* h_colidx)
+{
+    if (!K || !h_rowptr || !h_colidx) return fail(CULIPX_INVALID_ARG, "culipx_kkt_assembly_export: null argument");
+    GUARD_BEGIN
+    CULIPX_TRY(use_device(K->handle));
+    const size_t N = (size_t)K->n + K->m;
+    CULIPX_CUDA(cudaMemcpy(h_rowptr, K->rowptr.get(), (N + 1) * sizeof(int), cudaMemcpyDeviceToHost));
+    if (K->nnz_k > 0)
+        CULIPX_CUDA(cudaMemcpy(h_colidx, K->colidx.get(), K->nnz_k * sizeof(int), cudaMemcpyDeviceToHost));
+    return CULIPX_OK;
+    GUARD_END
+}
+
+CULIPX_API int culipx_kkt_assemble(culipx_kkt_assembly K, const double* d_aval, const double* d_x, const double* d_s,
+                                   const double* d_d, double delta, double gamma, int precision, void* d_kval)
+{
+    if (!K) return fail(CULIPX_INVALID_ARG, "culipx_kkt_assemble: null plan");
+    GUARD_BEGIN
+    CULIPX_TRY(use_device(K->handle));
+    return kkt_assembly_values(K, d_aval, d_x, d_s, d_d, delta, gamma, precision, d_kval);
     GUARD_END
 }
 

@@ -219,6 +219,31 @@ int culipx_factor_set_pivot_fp64(culipx_factor f, double bound);
 int culipx_prec_apply(culipx_factor f, int stage, const void *d_b, void *d_x);
 
 /* ------------------------------------------------------------------------ */
+/* KKT assembly for an interior-point iteration (no counterpart in culip's
+ * libs/la, whose IPM caller forms K on the host): the explicit
+ *   K = [[diag(d) + delta I, A'], [A, -gamma I]],  d_j = s_j / x_j
+ * (the LP barrier Hessian X^-1 S; or d given directly), i.e. the matrix of
+ * AugmentedMatrixSPMV<T> (libs/la/spmv.cuh:104-149) with the dual shift on
+ * every row, as full symmetric CSR with sorted columns and an explicit
+ * diagonal (N = n + m rows, nnz_K = 2 nnz_A + N).  create() plans K's
+ * structure once per pattern of A (m x n CSR on the device, rows sorted, no
+ * duplicates; invalid structure is rejected with CULIPX_INVALID_ARG);
+ * assemble() writes one iteration's values with one gather on the handle's
+ * stream (precision CULIPX_F64 or CULIPX_F32 output).  Pass d_d = NULL to
+ * use x and s (all n entries > 0), else d_x / d_s may be NULL. */
+typedef struct culipx_kkt_assembly_t *culipx_kkt_assembly;
+int culipx_kkt_assembly_create(culipx_handle h, int m, int n, long long nnz_a, const int *d_rowptr,
+                               const int *d_colidx, culipx_kkt_assembly *out);
+int culipx_kkt_assembly_destroy(culipx_kkt_assembly K);
+/* K's size and its device structure (owned by the plan) */
+int culipx_kkt_assembly_size(culipx_kkt_assembly K, int *N, long long *nnz_k);
+int culipx_kkt_assembly_structure(culipx_kkt_assembly K, const int **d_rowptr, const int **d_colidx);
+/* K's structure copied to host arrays of N + 1 and nnz_k ints (culipx_pattern_analyze's input) */
+int culipx_kkt_assembly_export(culipx_kkt_assembly K, int *h_rowptr, int *h_colidx);
+int culipx_kkt_assemble(culipx_kkt_assembly K, const double *d_aval, const double *d_x, const double *d_s,
+                        const double *d_d, double delta, double gamma, int precision, void *d_kval);
+
+/* ------------------------------------------------------------------------ */
 /* Permutation and scaling of K before the factorization: B = diag(1/r)
  * P_r K P_c' diag(1/c) with sorted rows and columns, as T_matrix_permute_scale
  * (libs/la/sparse_la.impl.cuh:599-657) called by the driver's host_permute

@@ -251,6 +251,26 @@ def ldu_apply(L_rowptr, L_colidx, L_val, tri, is_piv, perm, scale, stage, b):
     return x
 
 
+def kkt_assemble(m, n, a_rowptr, a_colidx, a_val, x=None, s=None, d=None, delta=1e-8, gamma=1e-8):
+    """K = [[diag(d) + delta I, A'], [A, -gamma I]] with d = s / x (or given)
+    as full symmetric CSR with sorted columns and an explicit diagonal (numpy
+    restatement of the augmented system whose product AugmentedMatrixSPMV<T>
+    computes, libs/la/spmv.cuh:104-149, with the dual shift on every row).
+    Returns (rowptr, colidx, val)."""
+    a_rowptr = np.asarray(a_rowptr, np.int64)
+    a_colidx = np.asarray(a_colidx, np.int64)
+    a_val = np.asarray(a_val, np.float64)
+    dd = np.asarray(d, np.float64) if d is not None else np.asarray(s, np.float64) / np.asarray(x, np.float64)
+    arow = np.repeat(np.arange(m), np.diff(a_rowptr))
+    rows = np.concatenate([np.arange(n), a_colidx, n + arow, n + np.arange(m)])
+    cols = np.concatenate([np.arange(n), n + arow, a_colidx, n + np.arange(m)])
+    vals = np.concatenate([dd + delta, a_val, a_val, np.full(m, -gamma)])
+    order = np.lexsort((cols, rows))
+    rowptr = np.zeros(n + m + 1, np.int64)
+    np.add.at(rowptr, rows + 1, 1)
+    return np.cumsum(rowptr).astype(np.int32), cols[order].astype(np.int32), vals[order]
+
+
 def permute_scale(rowptr, colidx, val, row_perm, col_perm=None, row_scale=None, col_scale=None,
                   scale_before_match=False, perm_is_old_to_new=True):
     """B = diag(1/r) P_r A P_c' diag(1/c) as sorted CSR (numpy restatement of
