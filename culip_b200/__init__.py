@@ -336,6 +336,29 @@ class PermutePlan:
             pass
 
 
+def sprank(m: int, n: int, rowptr, colidx):
+    """Structural rank of an m x n CSR pattern (culipx_sprank, culip's
+    sprank): (rank, row_match, col_match), INT_MAX marking unmatched."""
+    rp = np.ascontiguousarray(rowptr, np.int32)
+    ci = np.ascontiguousarray(colidx, np.int32)
+    rmatch = np.zeros(max(m, 1), np.int32)
+    cmatch = np.zeros(max(n, 1), np.int32)
+    rank = ctypes.c_int()
+    capi.call("culipx_sprank", int(m), int(n), _p(rp), _p(ci), _p(rmatch), _p(cmatch), ctypes.byref(rank))
+    return rank.value, rmatch[:m], cmatch[:n]
+
+
+def ordering_rcm(rowptr, colidx):
+    """Reverse Cuthill-McKee ordering of a square CSR pattern
+    (culipx_ordering_rcm): perm[new] = old."""
+    rp = np.ascontiguousarray(rowptr, np.int32)
+    ci = np.ascontiguousarray(colidx, np.int32)
+    n = len(rp) - 1
+    perm = np.zeros(max(n, 1), np.int32)
+    capi.call("culipx_ordering_rcm", n, _p(rp), _p(ci), _p(perm))
+    return perm[:n]
+
+
 class KktAssembly:
     """K = [[diag(d) + delta I, A'], [A, -gamma I]] of an interior-point
     iteration, d = s / x (or given), as full symmetric CSR: the structure is

@@ -219,6 +219,21 @@ int culipx_factor_set_pivot_fp64(culipx_factor f, double bound);
 int culipx_prec_apply(culipx_factor f, int stage, const void *d_b, void *d_x);
 
 /* ------------------------------------------------------------------------ */
+/* Orderings (host functions; no handle, no device).
+ * culipx_sprank replaces culip's sprank (libs/algorithms/sprank.cuh, an
+ * UnweightedBipartiteMatching, libs/algorithms/matching.cuh:18-62): the
+ * structural rank of the m x n CSR pattern by a maximum matching of rows to
+ * columns; row_match[i] = the column matched to row i, col_match[j] = the row
+ * matched to column j, INT_MAX where unmatched (either may be NULL).  Any
+ * maximum matching may be returned; the rank is unique.
+ * culipx_ordering_rcm (no counterpart in the reference, whose driver reads its
+ * permutation from a file): reverse Cuthill-McKee of the symmetrized n x n
+ * pattern, deterministic; perm[new] = old, i.e. pass perm_is_old_to_new = 0 to
+ * culipx_permute_create. */
+int culipx_sprank(int m, int n, const int *rowptr, const int *colidx, int *row_match, int *col_match, int *rank);
+int culipx_ordering_rcm(int n, const int *rowptr, const int *colidx, int *perm);
+
+/* ------------------------------------------------------------------------ */
 /* KKT assembly for an interior-point iteration (no counterpart in culip's
  * libs/la, whose IPM caller forms K on the host): the explicit
  *   K = [[diag(d) + delta I, A'], [A, -gamma I]],  d_j = s_j / x_j

@@ -4,6 +4,7 @@ Source: culip's tests/la/data/*.mtx (read from the reference checkout, which
 exists only where the fixtures are generated; the .npz files are committed).
   sqmr_{small,big}_{A,prec_L,prec_D,prec_p,prec_s}   tests/la/test_sqmr.cc:192-293
   spmv_{A,K}                                          tests/la/test_spmv.cc:150-210
+  bound_rank_*  (patterns and rank bounds)            tests/algorithms/test_bound_rank.cc:55-86
 MatrixMarket semantics follow libs/test/test.impl.h: 1-based coordinates,
 symmetric files expanded to both triangles (:73-89), rows sorted; dense
 "array" vectors read as written (shift 0, :233-290).
@@ -64,6 +65,13 @@ def main(root):
         M = read_mtx(os.path.join(data, f"spmv_{name}.mtx"))
         np.savez_compressed(os.path.join(HERE, f"spmv_{name}.npz"), m=M["m"], n=M["n"], rowptr=M["rowptr"],
                             colidx=M["colidx"], val=M["val"])
+    # tests/algorithms/test_bound_rank.cc:84-86: the patterns (values are not read) and
+    # their rank bounds (BTF lower bound, sprank upper bound)
+    for fname, lb, ub in (("bound_rank_51_800", 51, 800), ("bound_rank_920_930", 920, 930),
+                          ("bound_rank_4380_4380", 4380, 4380)):
+        M = read_mtx(os.path.join(root, "tests", "algorithms", "data", fname + ".mtx"))
+        np.savez_compressed(os.path.join(HERE, f"{fname}.npz"), m=M["m"], n=M["n"], rowptr=M["rowptr"],
+                            colidx=M["colidx"], lb=lb, ub=ub)
     print("wrote fixtures to", HERE)
 
 
