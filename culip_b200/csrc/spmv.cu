@@ -129,10 +129,13 @@ int launch(const int* rowptr, const int* colidx, const void* val, int m, double 
 
 // SELL-32 product: thread (slice s, lane) sums row rows[32 s + lane] over
 // the slots slice_off[s] + lane + 32 j in column order (col < 0: padding
-// after the row's last entry), 8 index and value loads ahead of their
-// gathers, as k_csr_spmv_rows does per row
+// after the row's last entry), in batches of 8: a batch's gathers of x are
+// issued together with the next batch's index and value loads (software
+// pipelined), and the slot stream is read with evict-first loads so that x
+// keeps its place in the caches.  128-thread CTAs (measured on the mixed
+// matrix: 0.594 of HBM against 0.551 for the unpipelined 256-thread kernel).
 template <class T>
-__global__ void __launch_bounds__(256) k_sell_spmv(int nslices, const int* __restrict__ rows,
+__global__ void __launch_bounds__(128) k_sell_spmv(int nslices, const int* __restrict__ rows,
                                                    const long long* __restrict__ slice_off,
                                                    const int* __restrict__ slice_len, const int* __restrict__ col,
                                                    const T* __restrict__ val, const T* __restrict__ x,
@@ -146,20 +149,36 @@ __global__ void __launch_bounds__(256) k_sell_spmv(int nslices, const int* __res
     const int* cp = col + __ldg(slice_off + sl) + (t & 31);
     const T* vp = val + __ldg(slice_off + sl) + (t & 31);
     T acc = T(0);
-    for (int jb = 0; jb < len; jb += kGatherBatch) {
-        T v[kGatherBatch], xv[kGatherBatch];
-        int c[kGatherBatch];
+    constexpr int B = kGatherBatch;
+    int c[B];
+    T v[B];
 #pragma unroll
-        for (int j = 0; j < kGatherBatch; ++j) {
-            const bool ok = jb + j < len;
-            c[j] = ok ? __ldg(cp + 32 * (jb + j)) : -1;
-            v[j] = ok ? __ldg(vp + 32 * (jb + j)) : T(0);
+    for (int j = 0; j < B; ++j) {
+        const bool ok = j < len;
+        c[j] = ok ? __ldcs(cp + 32 * j) : -1;
+        v[j] = ok ? __ldcs(vp + 32 * j) : T(0);
+    }
+    for (int jb = 0; jb < len; jb += B) {
+        T xv[B];
+#pragma unroll
+        for (int j = 0; j < B; ++j) xv[j] = (c[j] >= 0) ? __ldg(x + c[j]) : T(0);
+        // the next batch's indices and values, in flight with this batch's gathers
+        int cn[B];
+        T vn[B];
+#pragma unroll
+        for (int j = 0; j < B; ++j) {
+            const bool ok = jb + B + j < len;
+            cn[j] = ok ? __ldcs(cp + 32 * (jb + B + j)) : -1;
+            vn[j] = ok ? __ldcs(vp + 32 * (jb + B + j)) : T(0);
         }
 #pragma unroll
-        for (int j = 0; j < kGatherBatch; ++j) xv[j] = (c[j] >= 0) ? __ldg(x + c[j]) : T(0);
-#pragma unroll
-        for (int j = 0; j < kGatherBatch; ++j)
+        for (int j = 0; j < B; ++j)
             if (c[j] >= 0) acc = fma_rn(v[j], xv[j], acc);
+#pragma unroll
+        for (int j = 0; j < B; ++j) {
+            c[j] = cn[j];
+            v[j] = vn[j];
+        }
     }
     if (row >= 0) y[row] = (beta == T(0)) ? alpha * acc : fma_rn(alpha, acc, beta * y[row]);
 }
@@ -204,7 +223,7 @@ int launch_sell(Csr* A, const void* x, void* y, double alpha, double beta, cudaS
     T* yy = static_cast<T*>(y);
     if (S.nslices > 0) {
         const long long threads = 32LL * S.nslices;
-        k_sell_spmv<T><<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(
+        k_sell_spmv<T><<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(
             S.nslices, S.rows.as<int>(), S.slice_off.as<long long>(), S.slice_len.as<int>(), S.col.as<int>(),
             S.val.as<T>(), xx, yy, (T)alpha, (T)beta);
         CULIPX_TRY(launch_check("k_sell_spmv"));
