@@ -494,6 +494,20 @@ def batch_sqmr_solve(batch: Batch, A: CsrOperator, M: Factor, b, x, tol=1e-8, ma
     return res, its, st
 
 
+def batch_factor_solve_graph(batch: Batch, A: CsrOperator, M: Factor, vals, b, x, tol=1e-8, max_it=1000,
+                             pivot=PIV_BK, threshold=0.0):
+    """Factor the union (values `vals`, a CUDA tensor in M's precision) and
+    solve all systems, as one CUDA-graph launch after the first call for the
+    same buffers (culipx_batch_factor_solve_graph).  Returns per-system
+    (residual, iterations, status) numpy arrays."""
+    res = np.zeros(batch.num)
+    its = np.zeros(batch.num, np.int32)
+    st = np.zeros(batch.num, np.int32)
+    capi.call("culipx_batch_factor_solve_graph", batch._h, A._h, M._h, _dptr(vals), int(pivot), float(threshold),
+              _dptr(b), _dptr(x), float(tol), int(max_it), _p(res), _p(its), _p(st))
+    return res, its, st
+
+
 class Server:
     """Continuous-batching request server (culipx_server_*): patterns analysed
     once, requests (K's values + right-hand sides, host numpy) admitted by

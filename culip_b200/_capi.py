@@ -79,6 +79,7 @@ _SIGS = {
     "culipx_csr_create": [vp, i32, i32, i64, vp, vp, vp, i32, i32, ctypes.POINTER(vp)],
     "culipx_csr_destroy": [vp],
     "culipx_spmv": [vp, vp, vp, f64, f64, i32],
+    "culipx_batch_factor_solve_graph": [vp, vp, vp, vp, i32, f64, vp, vp, f64, i32, vp, vp, vp],
     "culipx_sprank": [i32, i32, vp, vp, vp, vp, ctypes.POINTER(i32)],
     "culipx_ordering_rcm": [i32, vp, vp, vp],
     "culipx_kkt_assembly_create": [vp, i32, i32, i64, vp, vp, ctypes.POINTER(vp)],

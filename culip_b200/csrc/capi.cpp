@@ -671,6 +671,18 @@ CULIPX_API int culipx_batch_sqmr_solve(culipx_batch b, culipx_csr A, culipx_fact
     GUARD_END
 }
 
+CULIPX_API int culipx_batch_factor_solve_graph(culipx_batch b, culipx_csr A, culipx_factor M, const void* d_vals,
+                                               int pivot, double threshold, const double* d_b, double* d_x, double tol,
+                                               int max_it, double* h_residual, int* h_iterations, int* h_status)
+{
+    if (!b) return fail(CULIPX_INVALID_ARG, "null batch");
+    GUARD_BEGIN
+    CULIPX_TRY(use_device(b->h));
+    return batch_factor_solve_graph(b, A, M, d_vals, pivot, threshold, d_b, d_x, tol, max_it, h_residual,
+                                    h_iterations, h_status);
+    GUARD_END
+}
+
 CULIPX_API int culipx_sqmr_solve_multi(culipx_handle h, culipx_csr A, culipx_factor M, int nrhs, const double* d_B,
                                        double* d_X, double tol, int max_it, double* h_residual, int* h_iterations,
                                        int* h_status)

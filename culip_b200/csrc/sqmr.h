@@ -38,11 +38,38 @@ struct Batch {
     std::vector<int> row_off;                 // num + 1
     DeviceBuffer d_row_off, d_qb, d_qe;       // num + 1, num x nl, num x nl
     DeviceBuffer d_out, d_next;               // num x 8 results, system counter
+    // batch_factor_solve_graph: the factorization and the batched solve as one
+    // CUDA graph, its own workspace (the graph holds its addresses), and what
+    // the graph was captured for
+    Sqmr* gw = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    cudaStream_t capture_stream = nullptr;
+    struct Key {
+        const void* vals = nullptr;
+        const void* A = nullptr;
+        const void* M = nullptr;
+        const double* b = nullptr;
+        double* x = nullptr;
+        int pivot = -1, max_it = -1;
+        double threshold = -1.0, tol = -1.0, piv64 = -1.0;
+        bool operator==(const Key& o) const
+        {
+            return vals == o.vals && A == o.A && M == o.M && b == o.b && x == o.x && pivot == o.pivot &&
+                   max_it == o.max_it && threshold == o.threshold && tol == o.tol && piv64 == o.piv64;
+        }
+    } graph_key;
+    int graph_launches = 0;
+    ~Batch();
 };
 
 int batch_create(culipx_handle_t* h, const Pattern* p, int num, const int* h_row_off, Batch** out);
 int batch_sqmr_solve(Batch* bt, Csr* A, Factor* M, const double* b, double* x, double tol, int max_it,
                      double* h_res, int* h_its, int* h_status, Sqmr* w);
+
+int batch_factor_solve_graph(Batch* bt, Csr* A, Factor* M, const void* d_vals, int pivot, double threshold,
+                             const double* b, double* x, double tol, int max_it, double* h_res, int* h_its,
+                             int* h_status);
 
 int batch_sqmr_refine(Batch* bt, Csr* A, Factor* M, const double* b, double* x, double tol, double inner_tol,
                       int inner_max_it, int max_refine, double* h_relres, int* h_its, int* h_steps, int* h_status,

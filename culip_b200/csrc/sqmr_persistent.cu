@@ -1800,6 +1800,127 @@ int batch_create(culipx_handle_t* h, const Pattern* p, int num, const int* h_row
     return CULIPX_OK;
 }
 
+namespace {
+
+// the batch's results (8 values per system) to per-system residual, iterations, status
+int batch_results(Batch* bt, int max_it, double* h_res, int* h_its, int* h_status)
+{
+    std::vector<double> out((size_t)bt->num * 8);
+    CULIPX_CUDA(cudaMemcpyAsync(out.data(), bt->d_out.get(), out.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                                bt->h->stream));
+    CULIPX_CUDA(cudaStreamSynchronize(bt->h->stream));
+    for (int k = 0; k < bt->num; ++k) {
+        const double* o = out.data() + (size_t)k * 8;
+        if (h_res) h_res[k] = o[0];
+        if (h_its) h_its[k] = (int)o[1];
+        if (h_status)
+            h_status[k] = (o[2] != 0.0) ? CULIPX_BREAKDOWN
+                          : (o[3] == 0.0 && max_it > 0 && (int)o[1] >= max_it) ? CULIPX_MAXIT
+                                                                               : CULIPX_OK;
+    }
+    return CULIPX_OK;
+}
+
+int batch_check(Batch* bt, Csr* A, Factor* M, const double* b, double* x, int max_it, const char* what)
+{
+    if (!bt || !A || !M || !b || !x) return fail(CULIPX_INVALID_ARG, "%s: null argument", what);
+    if (A->precision != CULIPX_F64 || A->m != A->n || A->m != bt->pat->n)
+        return fail(CULIPX_INVALID_ARG, "%s: A must be the FP64 union matrix of the batch", what);
+    if (M->pat != bt->pat) return fail(CULIPX_INVALID_ARG, "%s: M must be a factor of the batch's pattern", what);
+    if (M->solve_algorithm == CULIPX_SOLVE_JACOBI) return fail(CULIPX_NOT_SUPPORTED, "%s: SOLVE_JACOBI is not batched", what);
+    if (max_it < 0) return fail(CULIPX_INVALID_ARG, "%s: max_it < 0", what);
+    return CULIPX_OK;
+}
+
+}  // namespace
+
+Batch::~Batch()
+{
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (capture_stream) cudaStreamDestroy(capture_stream);
+    delete gw;
+}
+
+// The numeric factorization of the union and the batched solve as one CUDA
+// graph launch.  The first call for a given set of buffers (values, A, M, b,
+// x) and settings factors and solves by ordinary launches -- which sizes
+// every buffer, the batch's own solver workspace included -- and captures
+// the same sequence on a stream of the batch's own; later calls replay it
+// (the contents of the buffers may change in between).
+int batch_factor_solve_graph(Batch* bt, Csr* A, Factor* M, const void* d_vals, int pivot, double threshold,
+                             const double* b, double* x, double tol, int max_it, double* h_res, int* h_its,
+                             int* h_status)
+{
+    CULIPX_TRY(batch_check(bt, A, M, b, x, max_it, "culipx_batch_factor_solve_graph"));
+    if (!d_vals) return fail(CULIPX_INVALID_ARG, "culipx_batch_factor_solve_graph: null values");
+    if (pivot < CULIPX_PIV_STATIC || pivot > CULIPX_PIV_ROOK)
+        return fail(CULIPX_INVALID_ARG, "culipx_batch_factor_solve_graph: bad pivot method %d", pivot);
+    culipx_handle_t* h = bt->h;
+    if (!bt->gw) bt->gw = new Sqmr();
+    Batch::Key key;
+    key.vals = d_vals;
+    key.A = A;
+    key.M = M;
+    key.b = b;
+    key.x = x;
+    key.pivot = pivot;
+    key.max_it = max_it;
+    key.threshold = threshold;
+    key.tol = tol;
+    key.piv64 = M->pivot_fp64;
+    auto solve = [&]() -> int {
+        return (M->precision == CULIPX_F64) ? launch_batched<double>(bt, A, M, b, x, tol, max_it, bt->gw)
+                                            : launch_batched<float>(bt, A, M, b, x, tol, max_it, bt->gw);
+    };
+    if (!bt->graph_exec || !(bt->graph_key == key)) {
+        CULIPX_TRY(factor_compute(M, d_vals, nullptr, pivot, threshold));
+        CULIPX_TRY(solve());
+        CULIPX_TRY(batch_results(bt, max_it, h_res, h_its, h_status));
+        if (bt->graph_exec) cudaGraphExecDestroy(bt->graph_exec);
+        if (bt->graph) cudaGraphDestroy(bt->graph);
+        bt->graph_exec = nullptr;
+        bt->graph = nullptr;
+        if (!bt->capture_stream) CULIPX_CUDA(cudaStreamCreateWithFlags(&bt->capture_stream, cudaStreamNonBlocking));
+        cudaStream_t s = h->stream;
+        const long long launches0 = h->launches;
+        CULIPX_CUDA(cudaStreamBeginCapture(bt->capture_stream, cudaStreamCaptureModeThreadLocal));
+        h->stream = bt->capture_stream;
+        M->capturing = true;
+        int st = factor_compute(M, d_vals, nullptr, pivot, threshold);
+        if (st == CULIPX_OK) st = solve();
+        M->capturing = false;
+        h->stream = s;
+        bt->graph_launches = (int)(h->launches - launches0);
+        h->launches = launches0;  // captured, not launched
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(bt->capture_stream, &g);
+        if (st != CULIPX_OK || e != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();
+            return st != CULIPX_OK ? st
+                                   : fail(CULIPX_CUDA_ERROR, "culipx_batch_factor_solve_graph: capture failed: %s",
+                                          cudaGetErrorString(e));
+        }
+        cudaGraphExec_t ge = nullptr;
+        if (cudaGraphInstantiate(&ge, g, 0) != cudaSuccess) {
+            cudaGraphDestroy(g);
+            cudaGetLastError();
+            return fail(CULIPX_CUDA_ERROR, "culipx_batch_factor_solve_graph: graph instantiation failed");
+        }
+        bt->graph = g;
+        bt->graph_exec = ge;
+        bt->graph_key = key;
+        return CULIPX_OK;  // the ordinary run above factored and solved
+    }
+    CULIPX_CUDA(cudaGraphLaunch(bt->graph_exec, h->stream));
+    h->launches += bt->graph_launches;
+    M->pivot = pivot;
+    M->threshold = threshold;
+    M->computed = true;
+    return batch_results(bt, max_it, h_res, h_its, h_status);
+}
+
 int batch_sqmr_solve(Batch* bt, Csr* A, Factor* M, const double* b, double* x, double tol, int max_it,
                      double* h_res, int* h_its, int* h_status, Sqmr* w)
 {

@@ -351,6 +351,17 @@ int culipx_batch_create(culipx_pattern p, int num_systems, const int *h_row_offs
 int culipx_batch_destroy(culipx_batch b);
 int culipx_batch_sqmr_solve(culipx_batch b, culipx_csr A, culipx_factor M, const double *d_b, double *d_x,
                             double tol, int max_it, double *h_residual, int *h_iterations, int *h_status);
+/* The numeric factorization of the batch's union (values d_vals, in M's
+ * precision) and the batched SQMR solve of all its systems as ONE CUDA-graph
+ * launch (no counterpart in the reference).  The first call for a set of
+ * buffers (d_vals, A, M, d_b, d_x) and settings runs both as ordinary launches,
+ * which sizes every buffer (the batch keeps its own solver workspace), and
+ * captures them; later calls replay the graph, so the buffers' contents may
+ * change between calls but not their addresses.  Results as
+ * culipx_batch_sqmr_solve. */
+int culipx_batch_factor_solve_graph(culipx_batch b, culipx_csr A, culipx_factor M, const void *d_vals, int pivot,
+                                    double threshold, const double *d_b, double *d_x, double tol, int max_it,
+                                    double *h_residual, int *h_iterations, int *h_status);
 
 /* Several right-hand sides of one system (no counterpart in the reference,
  * whose SQMR takes one): d_B and d_X are n x nrhs column-major.  Up to four

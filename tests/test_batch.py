@@ -202,3 +202,40 @@ def test_union_analysis_formats_equal_separate_analyses():
     with pytest.raises(cb.CulipxError):
         cb.Pattern(hh, rp, ci, bs, 0, 1.0, cb.F32, system_row_offsets=[0, off[1] + 1, off[-1]])
     capi.load().culipx_handle_destroy(hh._h)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [cb.F64, cb.F32])
+def test_batch_factor_solve_graph_replays_bit_for_bit(precision):
+    """culipx_batch_factor_solve_graph: the factorization of the union and the
+    batched solve as one graph launch.  The capturing call and two replays
+    (the second after the values changed) each equal an ordinary factor +
+    batch_sqmr_solve of the same values, bit for bit."""
+    import torch
+
+    handle = cb.Handle(0)
+    syst = _systems(5, seed=321)
+    rp, ci, v, bs, off = cb.union_systems(syst)
+    dt = torch.float64 if precision == cb.F64 else torch.float32
+    P = cb.Pattern(handle, rp, ci, bs, 0, 1.0, precision, system_row_offsets=off)
+    F, F2 = cb.Factor(P), cb.Factor(P)
+    B = cb.Batch(P, off)
+    d_v = torch.from_numpy(v).cuda()
+    d_vals = d_v.to(dt)
+    A = cb.CsrOperator(handle, torch.from_numpy(rp).cuda(), torch.from_numpy(ci).cuda(), d_v)
+    b = torch.from_numpy(np.concatenate(_rhs(syst, range(len(syst))))).cuda()
+    x = torch.zeros_like(b)
+    x2 = torch.zeros_like(b)
+    rows = np.repeat(np.arange(len(rp) - 1), np.diff(rp))
+    diag = torch.from_numpy(np.nonzero(rows == ci)[0]).cuda()
+    for call in range(3):
+        if call == 2:  # new values behind the same buffers: the replay must pick them up
+            d_v[diag] *= 1.5
+            d_vals.copy_(d_v.to(dt))
+        res, its, st = cb.batch_factor_solve_graph(B, A, F, d_vals, b, x, 1e-8, 300)
+        F2.compute(d_vals.clone())
+        res2, its2, st2 = cb.batch_sqmr_solve(B, A, F2, b, x2, 1e-8, 300)
+        assert np.array_equal(its, its2) and np.array_equal(st, st2) and np.array_equal(res, res2), call
+        assert torch.equal(x, x2), call
+        for k in ("val", "tri", "perm"):
+            assert np.array_equal(F.export()[k], F2.export()[k]), (call, k)
