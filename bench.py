@@ -382,12 +382,11 @@ def sqmr_roofline(info, N, nnz, its, launch_ms, nr=1, kernel="k_sqmr_persistent<
 def sweep_roofline(F, N, flush, stream, reps=10, precision_bytes=8):
     """The standalone triangular solves (culipx_prec_apply; the reference's
     solve_left / solve_right), L2 flushed before every call (outside the
-    events): LEFT = the pivot permutation gather + the U' level sweeps,
-    RIGHT = a copy + the U level sweeps + the permutation scatter.
+    events): LEFT = x = U'^-1 P' b, RIGHT = x = P U^-1 b, one launch per level
+    with the pivot permutation folded into the sweeps.
     Algorithmic bytes: B_tri = nnz_U (s + 4) + 4 (N + 1) + s * (upper-triangle
-    entries of the non-identity pivot tiles) + 2 s N for the sweeps, plus the
-    permutation pass (read b, the permutation, write x: 2 s N + 4 N) and for
-    RIGHT the copy (2 s N).  One launch per level plus the permutation."""
+    entries of the non-identity pivot tiles) + 2 s N (read b, write x), plus
+    the permutation (4 N)."""
     import torch
 
     import culip_b200 as cb
@@ -400,8 +399,7 @@ def sweep_roofline(F, N, flush, stream, reps=10, precision_bytes=8):
     b_tri = info["u_nnz"] * (s + 4) + 4 * (N + 1) + s * info["tile_entries"] + 2 * s * N
     peak = _peak_hbm()
     out = {}
-    for name, stage, extra in (("u_transpose_sweep (LEFT)", cb.LEFT, 2 * s * N + 4 * N),
-                               ("u_sweep (RIGHT)", cb.RIGHT, 2 * s * N + 4 * N + 2 * s * N)):
+    for name, stage, extra in (("u_transpose_sweep (LEFT)", cb.LEFT, 4 * N), ("u_sweep (RIGHT)", cb.RIGHT, 4 * N)):
         for _ in range(3):
             F.apply(stage, b, x)
         ms = []
@@ -418,7 +416,7 @@ def sweep_roofline(F, N, flush, stream, reps=10, precision_bytes=8):
         out[name] = {"achieved": byt / (t * 1e-3) / 1e9, "frac": byt / (t * 1e-3) / 1e9 / peak,
                      "avg_us": t * 1e3, "algorithmic_bytes": int(byt)}
     out.update({"unit": "GB/s", "peak": peak, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
-                "kernels": "k_perm_gather / cudaMemcpyAsync + k_sweep_level per level + k_perm_scatter",
+                "kernels": "k_sweep_level per level (permutation folded in)",
                 "l2": "flushed before every call"})
     return out
 
@@ -1026,7 +1024,26 @@ def run_batch(args):
         e1.record(stream)
         torch.cuda.synchronize()
         e_ms.append(e0.elapsed_time(e1))
+    # the factorization and one batched solve of every system as ONE graph
+    # launch (culipx_batch_factor_solve_graph): first call captures, then timed replays
+    xg = torch.zeros_like(d_x)
+    cb.batch_factor_solve_graph(B, A, F, d_v32, d_b, xg, inner_tol, inner_it)
+    g_ms, g_st = [], None
+    for i in range(3):
+        flush.fill_(float(i))
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        _, g_its, g_st = cb.batch_factor_solve_graph(B, A, F, d_v32, d_b, xg, inner_tol, inner_it)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        g_ms.append(e0.elapsed_time(e1))
     num = len(syst)
+    single_graph = {"what": "factor + one batched SQMR solve of all systems (tol 1e-6, no refinement) as one CUDA "
+                            "graph launch", "ms": float(np.mean(g_ms)),
+                    "systems_per_s": num / (float(np.mean(g_ms)) / 1e3),
+                    "quasi_residual_converged_fraction": float(np.mean(g_st == 0)),
+                    "median_iterations": int(np.median(g_its))}
     out = {
         "metric": "KKT solves/s (batched uneven instances, FP32 factor + FP64 refinement to relres 1e-8)",
         "value": num * args.steps / (total_ms / 1e3), "unit": "solves/s", "n_gpus": world, "steps": args.steps,
@@ -1048,6 +1065,7 @@ def run_batch(args):
         "factor_ms": fac_ms, "analysis_s_once": analysis_s, "gpu_launches": int(launches), "clocks": ck,
         "e2e": {"value": num * len(e_ms) / (float(np.sum(e_ms)) / 1e3), "unit": "solves/s",
                 "h2d_bytes_per_step": int(nnz * 8 + N * 8), "d2h_bytes_per_step": int(N * 8)},
+        "single_graph": single_graph,
     }
     if rank == 0:
         print(json.dumps(out), flush=True)

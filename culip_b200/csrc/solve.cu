@@ -496,48 +496,88 @@ __global__ void k_sweep_extras(const int* __restrict__ u_off, const int* __restr
 }
 
 // ---------------------------------------------------------------------------
-// one level of the U (UPPER) or U' sweep, in place on x
+// one level of the U (UPPER) or U' sweep, warp per block row, lane per fine
+// row, each row's terms in increasing column order.
+//   U' (solve_left): row r starts from (P' b)_r = src[perm[r]] (src == NULL:
+//   from x[r], the permuted right-hand side already there), subtracts the
+//   earlier levels' x, and writes x[r].
+//   U (solve_right): row r starts from src[r], subtracts the later levels'
+//   values, read at their permuted places through ucol = perm[col], and
+//   writes x[perm[r]]: x = P U^-1 b with the permutation folded in (src may
+//   equal x: a block row writes only its own places, after reading them).
+// The non-identity pivot tile's upper triangle comes packed (column by
+// column for U, row by row for U', as the persistent solver reads it) and is
+// staged in shared memory for the serial substitution.
 template <class T, bool UPPER>
 __global__ void __launch_bounds__(32 * kSweepWarps)
     k_sweep_level(const int* __restrict__ rows, int nrows, const int* __restrict__ bs,
                   const int* __restrict__ off, const int* __restrict__ col, const T* __restrict__ vals,
-                  const long long* __restrict__ piv_off, const int* __restrict__ rowflags,
-                  const T* __restrict__ fval, T* __restrict__ x)
+                  const long long* __restrict__ pk_off, const int* __restrict__ rowflags,
+                  const T* __restrict__ pk, const int* __restrict__ perm, const T* src, T* x)
 {
-    __shared__ T tiles[kSweepWarps][kTileElems];
+    constexpr int kTri = 32 * 33 / 2;
+    __shared__ T tiles[kSweepWarps][kTri];
     const int warp = threadIdx.x >> 5;
     const int t = blockIdx.x * kSweepWarps + warp;
     if (t >= nrows) return;
     const int lane = lane_id();
     const int I = rows[t];
     const int fr = bs[I], h = bs[I + 1] - fr;
+    const int flags = rowflags[I];
+    const bool pid = (flags & kRowPermIdentity) != 0;
     T acc = T(0);
     if (lane < h) {
-        acc = x[fr + lane];
-        const int e1 = off[fr + lane + 1];
-        for (int k = off[fr + lane]; k < e1; ++k) acc = fma_rn(-vals[k], x[col[k]], acc);
+        const int g = fr + lane;
+        if (UPPER) acc = src[g];
+        else acc = src ? src[pid ? g : perm[g]] : x[g];
+        // the row's terms in batches of 8: index and value loads, then the
+        // gathers, then the fmas in column order
+        constexpr int B = 8;
+        const int e1 = off[g + 1];
+        for (int k = off[g]; k < e1; k += B) {
+            int c[B];
+            T v[B], xv[B];
+#pragma unroll
+            for (int j = 0; j < B; ++j) {
+                c[j] = (k + j < e1) ? col[k + j] : -1;
+                v[j] = (k + j < e1) ? vals[k + j] : T(0);
+            }
+#pragma unroll
+            for (int j = 0; j < B; ++j) xv[j] = (c[j] >= 0) ? x[c[j]] : T(0);
+#pragma unroll
+            for (int j = 0; j < B; ++j)
+                if (c[j] >= 0) acc = fma_rn(-v[j], xv[j], acc);
+        }
     }
-    if (!(rowflags[I] & 1)) {
+    if (!(flags & kRowIdentity)) {
         T* tile = tiles[warp];
-        const T* P = fval + piv_off[I];
-        if (lane < h)
-            for (int i = 0; i < h; ++i) tile[i * kTileStride + lane] = P[i * h + lane];
+        const T* P = pk + pk_off[I];
+        for (int e = lane; e < h * (h + 1) / 2; e += 32) tile[e] = P[e];
         __syncwarp();
         if (UPPER) {
+            // column c of the triangle at c (c + 1) / 2: rows 0 .. c
             for (int c = h - 1; c >= 0; --c) {
-                if (lane == c) acc = acc / tile[c * kTileStride + c];
+                const int cb = c * (c + 1) / 2;
+                if (lane == c) acc = acc / tile[cb + c];
                 const T xc = shfl(acc, c);
-                if (lane < c) acc = fma_rn(-tile[lane * kTileStride + c], xc, acc);
+                if (lane < c) acc = fma_rn(-tile[cb + lane], xc, acc);
             }
         } else {
+            // row r of the triangle at r h - r (r - 1) / 2: columns r .. h - 1
             for (int r = 0; r < h; ++r) {
-                if (lane == r) acc = acc / tile[r * kTileStride + r];
+                const int rb = r * h - r * (r - 1) / 2 - r;
+                if (lane == r) acc = acc / tile[rb + r];
                 const T xr = shfl(acc, r);
-                if (lane > r && lane < h) acc = fma_rn(-tile[r * kTileStride + lane], xr, acc);
+                if (lane > r && lane < h) acc = fma_rn(-tile[rb + lane], xr, acc);
             }
         }
     }
-    if (lane < h) x[fr + lane] = acc;
+    __syncwarp();  // every lane has read its own place before any lane writes
+    if (lane < h) {
+        const int g = fr + lane;
+        if (UPPER) x[pid ? g : perm[g]] = acc;
+        else x[g] = acc;
+    }
 }
 
 // one block-Jacobi sweep over all block rows (SOLVE_JACOBI; the stripe
@@ -729,32 +769,31 @@ int apply_t(Factor* f, int stage, const void* d_b, void* d_x, cudaStream_t s)
         return launch_check("Jacobi sweeps");
     }
     if (stage == CULIPX_LEFT) {
-        T* t = x;
+        const T* src = b;
         if ((const void*)b == (void*)x) {
-            t = f->work.as<T>();
+            // in place: P' b into x first, the sweeps then start from x
+            T* t = f->work.as<T>();
             CULIPX_CUDA(cudaMemcpyAsync(t, b, n * sizeof(T), cudaMemcpyDeviceToDevice, s));
             k_perm_gather<T><<<grid_n, 256, 0, s>>>(t, x, f->perm.as<int>(), n);
-        } else {
-            k_perm_gather<T><<<grid_n, 256, 0, s>>>(b, x, f->perm.as<int>(), n);
+            src = nullptr;
         }
         for (int L = 0; L < p.num_levels; ++L) {
             const int nr = p.lvl_off[L + 1] - p.lvl_off[L];
             k_sweep_level<T, false><<<(nr + kSweepWarps - 1) / kSweepWarps, 32 * kSweepWarps, 0, s>>>(
                 p.d_lvl_rows.as<int>() + p.lvl_off[L], nr, p.d_bs.as<int>(), f->ut_off.as<int>(),
-                f->ut_col.as<int>(), f->ut_val.as<T>(), f->piv_off.as<long long>(), f->rowflags.as<int>(), fval, x);
+                f->ut_col.as<int>(), f->ut_val.as<T>(), f->pk_off.as<long long>(), f->rowflags.as<int>(),
+                f->pk_row.as<T>(), f->perm.as<int>(), src, x);
         }
         return launch_check("U' sweep");
     }
-    // RIGHT: t = U^-1 b, x = P t
-    T* t = f->work.as<T>();
-    CULIPX_CUDA(cudaMemcpyAsync(t, b, n * sizeof(T), cudaMemcpyDeviceToDevice, s));
+    // RIGHT: x = P U^-1 b, the permutation folded into the sweeps
     for (int L = p.num_levels - 1; L >= 0; --L) {
         const int nr = p.lvl_off[L + 1] - p.lvl_off[L];
         k_sweep_level<T, true><<<(nr + kSweepWarps - 1) / kSweepWarps, 32 * kSweepWarps, 0, s>>>(
-            p.d_lvl_rows.as<int>() + p.lvl_off[L], nr, p.d_bs.as<int>(), f->u_off.as<int>(), f->u_col.as<int>(),
-            f->u_val.as<T>(), f->piv_off.as<long long>(), f->rowflags.as<int>(), fval, t);
+            p.d_lvl_rows.as<int>() + p.lvl_off[L], nr, p.d_bs.as<int>(), f->u_off.as<int>(), f->u_colp.as<int>(),
+            f->u_val.as<T>(), f->pk_off.as<long long>(), f->rowflags.as<int>(), f->pk_col.as<T>(),
+            f->perm.as<int>(), b, x);
     }
-    k_perm_scatter<T><<<grid_n, 256, 0, s>>>(t, x, f->perm.as<int>(), n);
     return launch_check("U sweep");
 }
 
@@ -787,7 +826,7 @@ int prec_apply(Factor* f, int stage, const void* d_b, void* d_x, cudaStream_t s)
     Pattern& p = *f->pat;
     if (stage == CULIPX_MIDDLE) p.handle->launches += 1;
     else if (f->solve_algorithm == CULIPX_SOLVE_JACOBI) p.handle->launches += f->jacobi_sweeps + 1 + (stage == CULIPX_LEFT);
-    else p.handle->launches += p.num_levels + 1;
+    else p.handle->launches += p.num_levels + ((stage == CULIPX_LEFT && d_b == d_x) ? 1 : 0);
     if (f->precision == CULIPX_F64) return apply_t<double>(f, stage, d_b, d_x, s);
     return apply_t<float>(f, stage, d_b, d_x, s);
 }
