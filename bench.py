@@ -873,7 +873,7 @@ def run_spmv(args):
         torch.cuda.synchronize()
         e_ms.append(e0.elapsed_time(e1))
     traffic = None
-    prof = os.path.join(ROOT, "profiles", f"spmv_{args.spmv_workload}.txt")
+    prof = os.path.join(ROOT, "profiles", f"spmv_{'sell_' if args.spmv_format == 'sell' else ''}{args.spmv_workload}.txt")
     if os.path.exists(prof):
         for ln in open(prof):
             if ln.startswith("dram_bytes_per_launch"):
