@@ -127,6 +127,7 @@ _SIGS = {
     "culipx_sqmr_refine": [vp, vp, vp, vp, vp, f64, f64, i32, i32, ctypes.POINTER(f64), ctypes.POINTER(i32),
                            ctypes.POINTER(i32)],
     "culipx_sqmr_profile": [vp, i32],
+    "culipx_sqmr_set_wait_skew": [vp, ctypes.c_ulonglong],
     "culipx_sqmr_phase_times": [vp, vp, i32],
 }
 

@@ -609,6 +609,13 @@ CULIPX_API int culipx_sqmr_profile(culipx_handle h, int enable)
     return CULIPX_OK;
 }
 
+CULIPX_API int culipx_sqmr_set_wait_skew(culipx_handle h, unsigned long long skew)
+{
+    if (!h || !h->sqmr) return fail(CULIPX_INVALID_ARG, "null handle");
+    h->sqmr->wait_skew = skew;
+    return CULIPX_OK;
+}
+
 CULIPX_API int culipx_sqmr_phase_times(culipx_handle h, double* out_us, int iterations)
 {
     if (!h || !out_us || iterations < 0) return fail(CULIPX_INVALID_ARG, "bad argument");

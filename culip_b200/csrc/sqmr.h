@@ -15,6 +15,7 @@ struct Sqmr {
     int n = -1;
     bool force_multi_kernel = false;  // use the per-phase kernels instead of the persistent solver
     bool profile = false;             // record per-phase device timestamps of the persistent solver
+    unsigned long long wait_skew = 0; // added to the persistent solver's level-wait target (tests; 0)
     DeviceBuffer ts;                  // 64 iterations x 8 phase stamps (ns, %globaltimer)
     DeviceBuffer vecs, partials, scal;
     DeviceBuffer ref_r, ref_d, ref_part;  // iterative refinement: residual, correction, norm partials

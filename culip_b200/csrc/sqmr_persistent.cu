@@ -26,8 +26,14 @@
 //       v+' D^-1 Av and v+' D^-1 v+; the first level also updates p and x.
 //       Barrier + reduction: beta, the next alpha, ||x||, the tests.
 //
-// That is 2 x (number of levels) barriers per iteration: 4 for a KKT system
-// in natural order.  Re-associations against the reference, all exact in
+// That is 2 x (number of levels) barriers per iteration, fewer for a KKT
+// system in natural order (two levels, level 0 of simple rows): there the
+// level-0 rows also compute their (K ev) in the U sweep (the U' sweep's
+// level-0 phase goes away), and instead of a grid barrier between the U
+// sweep's two levels every CTA counts its finished level-1 rows on a device
+// counter that the level-0 rows wait for (one elected poller per CTA, a
+// bounded wait: a wait that gives up ends the solve with CULIPX_TIMEOUT) --
+// two grid synchronisations per iteration, both reductions.  Re-associations against the reference, all exact in
 // real arithmetic:
 //   * v+ is divided by delta after the U sweep instead of before it (the
 //     sweep is linear); the division is applied to the SpMV result.
@@ -116,7 +122,60 @@ struct PArgs {
     double* partials;  // 2 buffers x kMaxNV x gridDim
     double* out;       // [0] gamma/norm_pb, [1] iterations, [2] breakdown, [3] converged, [4] norm_pb, [5] it
     unsigned long long* ts;  // optional phase timestamps: [it * 8 + phase], it < kTsIters
+    // Level-completion counter of the fused two-level iteration (grid launches
+    // only; NULL: a grid synchronisation instead): every CTA adds 1 once its
+    // level-1 rows of an iteration are written, level-0 rows wait for
+    // G (it + 1) before they read them.  [1]: set when a wait gave up.
+    unsigned long long* lvl_done;
+    unsigned long long wait_skew;  // added to the wait's target (fault injection in tests; 0)
 };
+
+// Bound of one device wait on the level counter: well above any legitimate
+// wait (a few microseconds), far below a watchdog.
+constexpr unsigned long long kWaitLimitNs = 200ull * 1000 * 1000;
+
+// Shared state of a CTA's level waits: the iteration (+1) whose count the CTA
+// has seen, and the iteration (+1) whose poller was elected.
+struct LvlWait {
+    int seen;
+    int poll;
+};
+
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p)
+{
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void red_release_add_u64(unsigned long long* p, unsigned long long v)
+{
+    asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// One thread spins (acquire loads, backing off) until *ctr >= target; gives up
+// after kWaitLimitNs, or at once if an earlier wait gave up, and records that
+// in ctr[1].  Returns false when it gave up.
+__device__ bool wait_count(unsigned long long* ctr, unsigned long long target)
+{
+    if (ld_acquire_u64(ctr) >= target) return true;
+    volatile unsigned long long* failed = ctr + 1;
+    if (*failed) return false;
+    unsigned long long t0;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+    for (unsigned k = 0;; ++k) {
+        __nanosleep(k < 8 ? 32 : 256);
+        if (ld_acquire_u64(ctr) >= target) return true;
+        if ((k & 15) == 15) {
+            unsigned long long t;
+            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+            if (*failed || t - t0 > kWaitLimitNs) {
+                *failed = 1;
+                return false;
+            }
+        }
+    }
+}
 
 constexpr int kTsIters = 64;
 
@@ -865,6 +924,49 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal 
     // it, at the point where the unfused path rounded it, so the results are
     // the unfused path's bit for bit.
     const bool fused = a.fuse_l0 && a.nl == 2 && lvb[0].c1 == lvb[0].c0;
+    // fused grid launches hand level 1 to level 0 through the level counter
+    const bool counted = fused && a.lvl_done != nullptr;
+    if (counted && blockIdx.x == 0 && tid == 0) {
+        a.lvl_done[0] = 0;  // read only after the initial phases' grid synchronisations
+        a.lvl_done[1] = 0;
+    }
+    __shared__ LvlWait lw;
+    if (tid == 0) {
+        lw.seen = 0;
+        lw.poll = 0;
+    }
+    // the calling warp's active lanes wait until the count for iteration it is
+    // reached: the first warp of the CTA to get here polls global memory, the
+    // others watch the CTA's shared flag; then every lane does one acquire
+    // load of the counter, which orders its own later loads after the count
+    auto level_wait = [&](int it) {
+        const unsigned mask = __activemask();
+        const int want = it + 1;
+        const int leader = __ffs(mask) - 1;
+        if (*(volatile int*)&lw.seen < want && lane == leader) {
+            if (atomicMax(&lw.poll, want) < want) {
+                wait_count(a.lvl_done,
+                           (unsigned long long)gridDim.x * (unsigned long long)want + a.wait_skew);
+                __threadfence_block();
+                *(volatile int*)&lw.seen = want;
+            } else {
+                unsigned long long t0, t;
+                asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+                for (unsigned k = 0; *(volatile int*)&lw.seen < want; ++k) {
+                    __nanosleep(64);
+                    if ((k & 15) == 15) {
+                        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+                        if (t - t0 > 2 * kWaitLimitNs) {
+                            *(volatile unsigned long long*)(a.lvl_done + 1) = 1;
+                            break;
+                        }
+                    }
+                }
+            }
+        }
+        __syncwarp(mask);
+        (void)ld_acquire_u64(a.lvl_done);
+    };
 
     // the level with the most pivot-tile items keeps its first kResSlots x
     // (grid) items in the warps' shared-memory slots
@@ -1060,6 +1162,7 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal 
                 // an identity tile and no swaps)
                 const int s1 = lb.s1;
                 const bool fz = fused && L == 0;
+                bool ready = !(counted && L == 0);
                 for (int i = lb.s0 + ctx.g0; i < s1; i += ctx.gstride) {
                     const int g = __ldg(a.simple_rows + i);
                     const double dd = (double)__ldg(a.dg + g);
@@ -1076,6 +1179,11 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal 
                         r[j] = fma_rn(v, v, r[j]);
                         acc[j] = (TF)(v / dd);
                     }
+                    if (!ready) {
+                        // v+ and D^-1 v+ above need no level-1 value; the gathers below do
+                        level_wait(it);
+                        ready = true;
+                    }
                     row_sub<TF, NR>(acc, __ldg(a.u_off + g), __ldg(a.u_off + g + 1), a.u_colp, a.u_val, a.ev);
 #pragma unroll
                     for (int j = 0; j < NR; ++j) a.ev[(size_t)g * NR + j] = (double)acc[j];
@@ -1089,7 +1197,14 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal 
                     }
                 }
                 if (L > 0) {
-                    ctx.sync();
+                    if (counted) {
+                        // this CTA's level-1 rows are written: count it (release);
+                        // level-0 rows wait for every CTA's count before reading them
+                        __syncthreads();
+                        if (tid == 0) red_release_add_u64(a.lvl_done, 1ull);
+                    } else {
+                        ctx.sync();
+                    }
                     if (NR == 1 && L == a.nl - 1) stamp(a.ts, it, 1);
                 }
             }
@@ -1350,6 +1465,9 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal 
             o[3] = (Q.snap0 || Q.snap1) ? 1 : 0;
             o[4] = Q.norm_pb;
             o[5] = Q.done ? Q.stop_it : it;
+            // a level wait that gave up: the results are invalid
+            o[6] = (counted && *(volatile unsigned long long*)(a.lvl_done + 1)) ? 1.0 : 0.0;
+            if (o[6] != 0.0) o[2] = 1.0;
         }
     __syncthreads();
 }
@@ -1494,6 +1612,8 @@ PArgs<TF> make_args(Csr* A, Factor* M, double* base, double* partials, const dou
     a.out = base + (size_t)kVecs * vn;
     a.partials = partials;
     a.ts = nullptr;
+    a.lvl_done = nullptr;
+    a.wait_skew = 0;
     a.x = x;
     a.b = b;
     return a;
@@ -1591,6 +1711,9 @@ int launch_persistent(culipx_handle_t* h, Csr* A, Factor* M, const double* b, do
     if ((size_t)(2 * kMaxNV * G) * sizeof(double) > w->partials.bytes())
         CULIPX_TRY(w->partials.alloc(h, (size_t)2 * kMaxNV * G * sizeof(double)));
     PArgs<TF> a = make_args<TF>(A, M, w->vecs.as<double>(), w->partials.as<double>(), b, x, tol, max_it, NR);
+    // the level counter in the spare slots after the results (need: 8 NR + 64 values)
+    a.lvl_done = reinterpret_cast<unsigned long long*>(a.out + 8 * kMaxNR);
+    a.wait_skew = w->wait_skew;
     if (w->profile && NR == 1) {
         if (w->ts.bytes() < (size_t)kTsIters * 8 * sizeof(unsigned long long))
             CULIPX_TRY(w->ts.alloc(h, (size_t)kTsIters * 8 * sizeof(unsigned long long)));
@@ -1613,6 +1736,7 @@ int launch_nr(int nr, culipx_handle_t* h, Csr* A, Factor* M, const double* b, do
 
 int status_of(const double* o, int max_it)
 {
+    if (o[6] != 0.0) return fail(CULIPX_TIMEOUT, "persistent SQMR: a bounded device wait gave up (results invalid)");
     if (o[2] != 0.0) return CULIPX_BREAKDOWN;
     if (o[3] == 0.0 && max_it > 0 && (int)o[1] >= max_it) return CULIPX_MAXIT;
     return CULIPX_OK;
@@ -2111,6 +2235,7 @@ int sqmr_solve_persistent(culipx_handle_t* h, Csr* A, Factor* M, const double* b
     if (st != CULIPX_OK) return st;
     if (residual) *residual = out[0];
     if (iterations) *iterations = (int)out[1];
+    if (out[6] != 0.0) return fail(CULIPX_TIMEOUT, "culipx_sqmr_solve: a bounded device wait gave up (results invalid)");
     if (out[2] != 0.0) return fail(CULIPX_BREAKDOWN, "culipx_sqmr_solve: breakdown (non-finite scalar)");
     if (out[3] == 0.0 && max_it > 0 && (int)out[1] >= max_it) return CULIPX_MAXIT;
     return CULIPX_OK;
@@ -2181,6 +2306,9 @@ int launch_noalloc(culipx_handle_t* h, Csr* A, Factor* M, const double* b, doubl
     double* base = g_noalloc_ptr[dev].load(std::memory_order_acquire);
     // run_persistent clears the recurrence vectors the scratch kept from the last call
     PArgs<TF> a = make_args<TF>(A, M, base, base + kNoAllocVecs, b, x, tol, max_it);
+    // the level counter after the results (the vectors' region holds a spare row of kNoAllocMaxRows values)
+    a.lvl_done = reinterpret_cast<unsigned long long*>(a.out + 8 * kMaxNR);
+    a.wait_skew = h->sqmr ? h->sqmr->wait_skew : 0;
     return run_persistent<TF, 1>(h, a, G, out);
 }
 
@@ -2207,6 +2335,8 @@ int sqmr_solve_noalloc(culipx_handle_t* h, Csr* A, Factor* M, const double* b, d
     if (st != CULIPX_OK) return st;
     if (residual) *residual = out[0];
     if (iterations) *iterations = (int)out[1];
+    if (out[6] != 0.0)
+        return fail(CULIPX_TIMEOUT, "culipx_sqmr_solve_noalloc: a bounded device wait gave up (results invalid)");
     if (out[2] != 0.0) return fail(CULIPX_BREAKDOWN, "culipx_sqmr_solve_noalloc: breakdown (non-finite scalar)");
     return status_of(out, max_it);
 }

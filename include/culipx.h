@@ -542,6 +542,13 @@ int culipx_sqmr_refine(culipx_handle h, culipx_csr A, culipx_factor M, const dou
  * levels with the final reduction, an unused slot (0), and the whole
  * iteration. */
 int culipx_sqmr_profile(culipx_handle h, int enable);
+/* Fault injection for tests (no counterpart in the reference).  In the
+ * persistent solver's iteration the level-0 rows of a two-level system wait
+ * on a device counter for the level-1 rows of every CTA (a bounded wait:
+ * 200 ms); skew > 0 raises the count they wait for beyond reach, so the wait
+ * gives up and the solve returns CULIPX_TIMEOUT (results invalid) instead of
+ * hanging.  0 (the default) for normal operation. */
+int culipx_sqmr_set_wait_skew(culipx_handle h, unsigned long long skew);
 int culipx_sqmr_phase_times(culipx_handle h, double *out_us, int iterations);
 
 /* The same solve (same kernel, same results) without any device allocation;
