@@ -64,6 +64,9 @@ def _parse():
     ap.add_argument("--rate", type=float, default=2000.0, help="--config served: arrivals per second")
     ap.add_argument("--duration", type=float, default=0.25, help="--config served: seconds of arrivals")
     ap.add_argument("--patterns", type=int, default=64, help="--config served: sparsity patterns")
+    ap.add_argument("--plain", action="store_true",
+                    help="--config served: the same requests through the plain FP64 path, one after another (FP64 "
+                         "factor, one single-right-hand-side solve at a time, no server)")
     ap.add_argument("--precision", default="f32", choices=["f32", "f64"],
                     help="--config served: factor precision (f32: FP32 factor and applies, FP64 SQMR)")
     ap.add_argument("--refine", type=int, default=0,
@@ -1126,6 +1129,8 @@ def run_served(args):
         state[j][0] = v
         return v, rng.standard_normal((len(pats[j][0]) - 1, nrhs))
 
+    if args.plain:
+        return run_served_plain(args, pats, arrivals, make_request, local)
     srv = cb.Server(local, 0, 3, 512, 1e-8, args.max_it)
     srv.set_large_rows(args.large_rows)
     srv.set_refine(args.refine, 1e-6)
@@ -1280,6 +1285,67 @@ def run_schur(args):
         res[name] = st
     print(json.dumps({"metric": "block Schur updates: F_alg / F_tile (tensor-core candidate work)", "configs": res}),
           flush=True)
+
+
+def run_served_plain(args, pats, arrivals, make_request, local):
+    """The served trace's requests through the plain FP64 single-solve path,
+    back to back (throughput; arrival times ignored): per request the FP64
+    factor of its values (each pattern analysed once, before the timing) and
+    one culipx_sqmr_solve per right-hand side on the whole GPU.  value =
+    requests / the device time of the whole run; the ratio of the served
+    line's value to this one is the serving path's gain at the same iteration
+    cap."""
+    import torch
+
+    import culip_b200 as cb
+
+    h = cb.Handle(local)
+    stream = torch.cuda.current_stream()
+    fac = []
+    for rp, ci, v, bs, n in pats:
+        P = cb.Pattern(h, rp, ci, bs, 0, 1.0, cb.F64)
+        F = cb.Factor(P)
+        d_rp, d_ci = torch.from_numpy(rp).cuda(), torch.from_numpy(ci).cuda()
+        d_v = torch.from_numpy(v).cuda()
+        fac.append((P, F, cb.CsrOperator(h, d_rp, d_ci, d_v), d_v))
+    # warm-up: one solve per pattern
+    for (P, F, A, d_v), (rp, ci, v, bs, n) in zip(fac, pats):
+        F.compute(d_v)
+        x = torch.zeros(len(rp) - 1, dtype=torch.float64, device="cuda")
+        cb.sqmr_solve(h, A, F, torch.ones_like(x), x, 1e-8, args.max_it)
+    reqs = [make_request(j, nrhs) for _, j, nrhs in arrivals]
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    nrhs_tot, conv, its = 0, 0, []
+    for (_, j, nrhs), (v, B) in zip(arrivals, reqs):
+        P, F, A, d_v = fac[j]
+        d_v.copy_(torch.from_numpy(v))
+        F.compute(d_v)
+        for c in range(B.shape[1]):
+            b = torch.from_numpy(np.ascontiguousarray(B[:, c])).cuda()
+            x = torch.zeros_like(b)
+            res, it, st = cb.sqmr_solve(h, A, F, b, x, 1e-8, args.max_it)
+            its.append(it)
+            conv += int(st == 0)
+            nrhs_tot += 1
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ck = clocks.stop()
+    sec = e0.elapsed_time(e1) / 1e3
+    out = {"metric": "KKT solves/s (served IPM stream's requests through the plain FP64 single-solve path)",
+           "value": len(reqs) / sec, "unit": "requests/s", "n_gpus": 1, "steps": len(reqs), "warmup": len(pats),
+           "ms_per_step": 1e3 * sec / max(len(reqs), 1), "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded KKT generator, the served trace's requests)",
+           "config": {"workload": f"{len(pats)} patterns, {len(reqs)} requests, {nrhs_tot} right-hand sides "
+                                  f"(the trace of --config served --rate {args.rate:g} --duration {args.duration:g})",
+                      "solver": f"FP64 factor per request, culipx_sqmr_solve per right-hand side, tol 1e-8, max_it "
+                                f"{args.max_it}", "parallelism": "one GPU, one solve at a time"},
+           "right_hand_sides": nrhs_tot, "rhs_per_s": nrhs_tot / sec, "converged_fraction": conv / max(nrhs_tot, 1),
+           "median_iterations": int(np.median(its)) if its else None, "clocks": ck}
+    print(json.dumps(out), flush=True)
 
 
 if __name__ == "__main__":

@@ -49,6 +49,11 @@ namespace culipx {
 void handle_retain(culipx_handle_t* h);
 void handle_release(culipx_handle_t* h);
 
+// A process-wide serial number for objects whose device addresses a captured
+// CUDA graph holds: a new object never repeats an old one's number, even when
+// it reuses the old one's host address.
+unsigned long long next_serial();
+
 // Checks the last launch error on this thread.
 int launch_check(const char* what);
 

@@ -27,6 +27,7 @@ static_assert(sizeof(CItem) == 32, "CItem is two 16-byte words");
 
 struct Factor {
     Pattern* pat = nullptr;
+    unsigned long long serial = next_serial();
     int precision = CULIPX_F64;
     size_t vbytes = 8;
     bool computed = false;

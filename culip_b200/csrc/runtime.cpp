@@ -6,6 +6,12 @@
 
 namespace culipx {
 
+unsigned long long next_serial()
+{
+    static std::atomic<unsigned long long> n{0};
+    return ++n;
+}
+
 namespace {
 thread_local char g_last_error[1024] = "";
 }

@@ -33,6 +33,7 @@ constexpr int kSellWindow = 256;
 
 struct Csr {
     culipx_handle_t* h = nullptr;
+    unsigned long long serial = next_serial();
     int m = 0, n = 0;
     long long nnz = 0;
     const int* rowptr = nullptr;

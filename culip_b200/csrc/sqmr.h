@@ -48,8 +48,7 @@ struct Batch {
     cudaStream_t capture_stream = nullptr;
     struct Key {
         const void* vals = nullptr;
-        const void* A = nullptr;
-        const void* M = nullptr;
+        unsigned long long A = 0, M = 0;  // serial numbers: host addresses can be reused
         const double* b = nullptr;
         double* x = nullptr;
         int pivot = -1, max_it = -1;

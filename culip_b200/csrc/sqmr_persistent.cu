@@ -1984,8 +1984,8 @@ int batch_factor_solve_graph(Batch* bt, Csr* A, Factor* M, const void* d_vals, i
     if (!bt->gw) bt->gw = new Sqmr();
     Batch::Key key;
     key.vals = d_vals;
-    key.A = A;
-    key.M = M;
+    key.A = A->serial;
+    key.M = M->serial;
     key.b = b;
     key.x = x;
     key.pivot = pivot;
