@@ -135,6 +135,25 @@ def test_prec_apply(handle, stage, case):
     assert np.array_equal(xo, xg), np.max(np.abs(xo - xg) / (np.abs(xo) + 1e-300))
 
 
+@pytest.mark.parametrize("stage", [cb.LEFT, cb.MIDDLE, cb.RIGHT])
+@pytest.mark.parametrize("case", ["scrambled", "small_fill1"])
+def test_prec_apply_in_place(handle, stage, case):
+    """b == x: LEFT gathers P' b first, MIDDLE is per row, RIGHT writes each
+    block row's results at their permuted places after reading its own rows
+    (pivot swaps move values inside a block row): the same bits as out of
+    place, and as the oracle."""
+    fill = 1 if case.endswith("fill1") else 0
+    rp, ci, v, bs = kkt("small") if case.startswith("small") else scrambled_kkt(seed=7)
+    S, OF, P, F = _factor_both(handle, rp, ci, v, bs, fill_level=fill)
+    assert not np.array_equal(OF.export()["perm"], np.arange(len(rp) - 1)) or case != "scrambled"
+    b = cb.normal_vector(13, len(rp) - 1)
+    out = F.apply(stage, torch.from_numpy(b).cuda()).cpu().numpy()
+    xb = torch.from_numpy(b.copy()).cuda()
+    F.apply(stage, xb, xb)
+    assert np.array_equal(xb.cpu().numpy(), out)
+    assert np.array_equal(out, OF.apply(stage, b))
+
+
 @pytest.mark.parametrize("transpose", [False, True])
 def test_spmv(handle, transpose):
     rp, ci, v = random_spd_ish(500, 0.02)
