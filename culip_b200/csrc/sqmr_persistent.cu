@@ -937,16 +937,18 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal 
     }
     // the calling warp's active lanes wait until the count for iteration it is
     // reached: the first warp of the CTA to get here polls global memory, the
-    // others watch the CTA's shared flag; then every lane does one acquire
-    // load of the counter, which orders its own later loads after the count
+    // others watch the CTA's shared flag; then every lane reads the counter
+    // itself with an acquire load and checks it (at once satisfied, or at once
+    // given up after a timeout), which orders its own later loads after every
+    // CTA's release
     auto level_wait = [&](int it) {
         const unsigned mask = __activemask();
         const int want = it + 1;
+        const unsigned long long target = (unsigned long long)gridDim.x * (unsigned long long)want + a.wait_skew;
         const int leader = __ffs(mask) - 1;
         if (*(volatile int*)&lw.seen < want && lane == leader) {
             if (atomicMax(&lw.poll, want) < want) {
-                wait_count(a.lvl_done,
-                           (unsigned long long)gridDim.x * (unsigned long long)want + a.wait_skew);
+                wait_count(a.lvl_done, target);
                 __threadfence_block();
                 *(volatile int*)&lw.seen = want;
             } else {
@@ -965,7 +967,7 @@ __device__ void sqmr_body(const PArgs<TF>& a, Ctx& ctx, const SysView& sv, Scal 
             }
         }
         __syncwarp(mask);
-        (void)ld_acquire_u64(a.lvl_done);
+        wait_count(a.lvl_done, target);
     };
 
     // the level with the most pivot-tile items keeps its first kResSlots x
